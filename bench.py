@@ -1,0 +1,424 @@
+"""Benchmark: 30-qubit layered circuit, FP64 gate-by-gate apply throughput.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the layered random circuit on n=30 qubits, complex128, 16 GiB
+state): each layer applies Rx, Ry, Rz to every qubit (angles uniform in
+[0, 2 pi), seeded per layer) and then a CNOT brickwork on (2i, 2i+1) for
+even layers, (2i+1, 2i+2) for odd layers; 40 layers make the circuit
+(4180 gates), input |0...0>.  One step = one layer through the PLAIN
+(gate-by-gate, bit-exact) path; K = 40 steps is exactly one circuit.
+
+metric/value: algorithmic HBM GB/s of the plain path (every gate reads and
+writes the amplitudes it updates once: 2*16*2^30 bytes for an uncontrolled
+dense or diagonal gate, half that for a CNOT), whole job over N GPUs.
+Extra keys: seconds per circuit of the TILED (bit-exact) and FUSED k=5 forms
+(FP64 and complex64 with split coefficients) with 1 - fidelity against the
+FP64 result, and the VQE adjoint gradient rate (n=24, 384 parameters,
+transverse-field Ising model).
+
+Multi-GPU: replicas only (the simulation of one circuit does not shard
+here); every rank runs the same per-GPU workload, value = all ranks' bytes /
+max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "yao-rs_b200"))
+
+METRIC = "30q gate-apply HBM GB/s & s/circuit; VQE grads/s fused vs plain at 1-F<=1e-6"
+NQ = 30
+LAYERS = 40
+
+
+# --------------------------------------------------------------- workload
+def layer_elements(Y, n, layer, seed=2026):
+    rng = np.random.default_rng([seed, layer])
+    ang = rng.uniform(0.0, 2.0 * math.pi, size=(n, 3))
+    els = []
+    for q in range(n):
+        els.append(Y.put([q], Y.Gate.Rx(float(ang[q, 0]))))
+        els.append(Y.put([q], Y.Gate.Ry(float(ang[q, 1]))))
+        els.append(Y.put([q], Y.Gate.Rz(float(ang[q, 2]))))
+    start = 0 if layer % 2 == 0 else 1
+    for a in range(start, n - 1, 2):
+        els.append(Y.control([a], [a + 1], Y.Gate.X))
+    return els
+
+
+def layer_bytes(n, layer, amp_bytes=16):
+    """Algorithmic bytes of one layer: 3n full-state gates + CNOTs on half."""
+    full = 2 * amp_bytes * (1 << n)
+    ncnot = len(range(0 if layer % 2 == 0 else 1, n - 1, 2))
+    return 3 * n * full + ncnot * full // 2
+
+
+def vqe_circuit(Y, n, layers, params):
+    els, k = [], 0
+    for _ in range(layers):
+        for q in range(n):
+            els.append(Y.put([q], Y.Gate.Ry(float(params[k]))))
+            els.append(Y.put([q], Y.Gate.Rz(float(params[k + 1]))))
+            k += 2
+        for q in range(n):
+            els.append(Y.control([q], [(q + 1) % n], Y.Gate.X))
+    return Y.Circuit.qubits(n, els)
+
+
+def tfim(Y, n):
+    cs, ss = [], []
+    for i in range(n):
+        cs.append(-1.0)
+        ss.append(Y.OperatorString([(i, Y.Op.Z), ((i + 1) % n, Y.Op.Z)]))
+    for i in range(n):
+        cs.append(-1.0)
+        ss.append(Y.OperatorString([(i, Y.Op.X)]))
+    return Y.OperatorPolynomial(cs, ss)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = str(gpu_index)
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9 and f[0] == self.idx:
+                self.rows.append(f)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_baseline_sample(n, budget_s, layer=0):
+    """The oracle (C restatement of yao-rs's single-threaded CPU loops) on
+    the first gates of layer 0 at n qubits, until `budget_s` seconds pass."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    import yao_rs as Y
+
+    O.lib()
+    els = layer_elements(Y, n, layer)
+    st = np.empty(1 << n, dtype=np.complex128)
+    st.fill(0)  # touch every page before timing
+    st[0] = 1
+    arr, keep = Y.elements_array(els)
+    import ctypes as C
+    t_total, b_total, gates = 0.0, 0.0, 0
+    full = 2 * 16 * (1 << n)
+    for i, el in enumerate(els):
+        t0 = time.perf_counter()
+        O.lib().orc_apply_inplace(n, C.cast(C.addressof(arr[i]), C.c_void_p), 1,
+                                  st.ctypes.data_as(C.c_void_p))
+        t_total += time.perf_counter() - t0
+        b_total += full if not el.control_locs else full // 2
+        gates += 1
+        if t_total > budget_s:
+            break
+    return b_total / t_total / 1e9, gates, t_total
+
+
+def host_ram_gb():
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable"):
+                return int(line.split()[1]) / 1e6
+    except OSError:
+        pass
+    return 0.0
+
+
+# -------------------------------------------------------------- reference
+def run_reference(args, rank, world):
+    """yao-rs cannot run here (Rust; no toolchain): its CPU path is timed
+    through the oracle, the C restatement of its loops, single-threaded like
+    yao-rs.  One step = one gate of the layered circuit at n qubits."""
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import ctypes as C
+
+    import oracle as O
+    import yao_rs as Y
+
+    n = args.qubits if host_ram_gb() > 3 * 16 * (1 << args.qubits) / 1e9 else min(args.qubits, 28)
+    O.lib()
+    gates = []
+    for layer in range(LAYERS):
+        gates += layer_elements(Y, n, layer)
+    arr, keep = Y.elements_array(gates)
+    st = np.empty(1 << n, dtype=np.complex128)
+    st.fill(0)  # touch every page before timing
+    st[0] = 1
+    full = 2 * 16 * (1 << n)
+    times, nbytes = [], []
+    for s in range(args.warmup + args.steps):
+        i = s % len(gates)
+        t0 = time.perf_counter()
+        O.lib().orc_apply_inplace(n, C.cast(C.addressof(arr[i]), C.c_void_p), 1, st.ctypes.data_as(C.c_void_p))
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+            nbytes.append(full if not gates[i].control_locs else full // 2)
+    T = sum(times)
+    v = sum(nbytes) / T / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * T / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": f"layered random circuit n={n}, one gate per step (layer order)", "qubits": n,
+                   "l2": "state larger than L2"},
+        "cpu_baseline": {"value": v, "unit": "GB/s", "cores": 1, "kind": "port",
+                         "sample": f"{args.steps} gates of the layered circuit at n={n}, oracle (C restatement of "
+                                   "yao-rs instruct loops, -O3, 1 thread: yao-rs is single-threaded)"},
+        "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------- ours
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=LAYERS)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--qubits", type=int, default=NQ)
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+
+    import yao_rs as Y
+    from yao_rs import _abi as A
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    n = args.qubits
+    dev = local
+    circuits = [Y.Circuit.qubits(n, layer_elements(Y, n, l)) for l in range(LAYERS)]
+    stream = torch.cuda.ExternalStream(A.stream_ptr(dev), device=torch.device("cuda", dev))
+
+    def barrier():
+        A.synchronize(dev)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    reg = Y.ArrayReg.zero_state(n, device=dev)
+    for i in range(args.warmup):
+        Y.apply_inplace(circuits[i % LAYERS], reg)
+    # timed region starts from |0...0>: K = 40 steps is one full circuit
+    A.check(A.lib().yao_ctx_synchronize(A.context(dev)))
+    del reg
+    reg = Y.ArrayReg.zero_state(n, device=dev)
+    barrier()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    clocks = ClockSampler(vis.split(",")[dev] if vis else dev)
+    clocks.start()
+    time.sleep(0.3)
+    A.profile(True, dev)
+    launches0 = Y.launch_count(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.steps):
+        Y.apply_inplace(circuits[i % LAYERS], reg)
+    e1.record(stream)
+    e1.synchronize()
+    launches = Y.launch_count(dev) - launches0
+    prof = A.profile_report(dev)
+    A.profile(False, dev)
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    nbytes = sum(layer_bytes(n, i % LAYERS) for i in range(args.steps))
+    value = world * nbytes / (ms / 1e3) / 1e9
+    prof_bytes = sum(p["bytes"] for p in prof)
+
+    # roofline of the dominant kernel (largest share of device time)
+    peak, peak_kind = measured_peaks()
+    top = max(prof, key=lambda p: p["ms"])
+    achieved = top["bytes"] / (top["ms"] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": top["kernel"], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "bytes_per_launch": top["bytes"] / top["launches"], "launches": top["launches"],
+                "avg_launch_ms": top["ms"] / top["launches"], "traffic": None,
+                "share": top["ms"] / sum(p["ms"] for p in prof)}
+    kernels = [{"kernel": p["kernel"], "launches": p["launches"], "ms": round(p["ms"], 3),
+                "GBps": round(p["bytes"] / (p["ms"] / 1e3) / 1e9, 1)} for p in prof]
+
+    # e2e: host state in pinned memory -> upload, K layers, download, through the public API
+    host = torch.zeros(1 << n, dtype=torch.complex128, pin_memory=True)
+    host[0] = 1
+    hp = host.data_ptr()
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    A.check(A.lib().yao_reg_upload(reg.handle, A.C.c_void_p(hp)))
+    for i in range(args.steps):
+        Y.apply_inplace(circuits[i % LAYERS], reg)
+    A.check(A.lib().yao_reg_to_host(reg.handle, A.C.c_void_p(hp)))
+    f1.record(stream)
+    f1.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{dev}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t.item())
+    state_bytes = 16 * (1 << n)
+    e2e = {"value": world * nbytes / (e2e_ms / 1e3) / 1e9, "unit": "GB/s",
+           "h2d_bytes_per_step": state_bytes / args.steps, "d2h_bytes_per_step": state_bytes / args.steps,
+           "note": "one upload of the input state and one download of the final state per K steps"}
+    del host
+
+    extras = {}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras = run_extras(Y, A, torch, stream, circuits, n, dev)
+    if rank == 0 and world == 1:
+        nb = n if host_ram_gb() > 2.5 * 16 * (1 << n) / 1e9 else min(n, 28)
+        v, g, tt = cpu_baseline_sample(nb, args.cpu_budget)
+        cpu = {"value": v, "unit": "GB/s", "cores": 1, "kind": "port",
+               "sample": f"first {g} gates of layer 0 at n={nb} ({tt:.1f} s), oracle = C restatement of yao-rs's "
+                         "single-threaded instruct loops"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": f"layered random circuit n={n}, 40 layers (Rx,Ry,Rz per qubit + CNOT brickwork), "
+                                   "one layer per step, PLAIN gate-by-gate FP64",
+                       "qubits": n, "state_bytes": state_bytes, "l2": "state (16 GiB) larger than L2, no flush",
+                       "parallelism": f"replicas x{world}"},
+            "s_per_circuit_plain": ms / args.steps * LAYERS / 1e3,
+            "roofline": roofline, "kernels": kernels, "profiled_bytes": prof_bytes, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clk, "cpu_baseline": cpu,
+        }
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_extras(Y, A, torch, stream, circuits, n, dev):
+    """Full 40-layer circuit through the TILED and FUSED forms, 1 - F against
+    the FP64 result, and the VQE gradient rate."""
+    out = {}
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        A.synchronize(dev)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / 1e3
+
+    ref = Y.ArrayReg.zero_state(n, device=dev)
+    # warm the tiled path (plan + first launches) on a throwaway pass
+    Y.apply_inplace(circuits[0], ref, Y.MODE_TILED)
+    del ref
+    ref = Y.ArrayReg.zero_state(n, device=dev)
+    t_tiled = timed(lambda: [Y.apply_inplace(c, ref, Y.MODE_TILED) for c in circuits])
+    out["s_per_circuit_tiled"] = t_tiled
+    forms = {}
+    for name, prec, k in (("fused_f64_k5", Y.C128, 5), ("fused_c64_k5", Y.C64, 5)):
+        r = Y.ArrayReg.zero_state(n, prec, device=dev)
+        Y.apply_inplace(circuits[0], r, Y.MODE_FUSED, k)
+        del r
+        r = Y.ArrayReg.zero_state(n, prec, device=dev)
+        t = timed(lambda: [Y.apply_inplace(c, r, Y.MODE_FUSED, k) for c in circuits])
+        f = ref.fidelity(r)
+        forms[name] = {"s_per_circuit": t, "one_minus_fidelity": max(0.0, 1.0 - f),
+                       "max_abs_err": ref.max_abs_diff(r)}
+        del r
+    out["fused"] = forms
+    del ref
+    # VQE: n=24, 8 layers of Ry.Rz on every qubit + CNOT ring, TFIM
+    nv, lv = 24, 8
+    rng = np.random.default_rng(2024)
+    params = rng.uniform(-math.pi, math.pi, size=2 * nv * lv)
+    vc = vqe_circuit(Y, nv, lv, params)
+    op = tfim(Y, nv)
+    z = Y.ArrayReg.zero_state(nv, device=dev)
+    Y.expect_grad(op, vc, z)
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        val, g = Y.expect_grad(op, vc, z)
+    dt = (time.perf_counter() - t0) / reps
+    out["vqe"] = {"qubits": nv, "params": len(g), "gates": len(vc.elements), "grads_per_s": 1.0 / dt,
+                  "s_per_grad": dt, "energy": val}
+    return out
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,419 @@
+"""GPU parity: the CUDA library (through its C ABI) against the CPU oracle
+and yao-rs's golden vectors.
+
+Bars: PLAIN and TILED application, density-matrix evolution, partial
+trace, full probabilities, the lambda vector and measurement bookkeeping
+are bit-exact (max |diff| == 0); reductions (expectation values, norms,
+purity, marginal probabilities, gradients) agree to 1e-12 relative;
+FUSED (FP64) to 1e-10 with 1 - F <= 1e-12; FUSED on complex64 to
+1 - F <= 1e-6.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+import yao_rs as Y
+from helpers import (circuit_from_case, layered_circuit, matrix_pairs, matrix_reim, named_gate, noise_from_key, pairs,
+                     qft_circuit, random_circuit, random_state, state, tfim, vqe_ansatz)
+from yao_rs import Gate, NoiseChannel
+
+pytestmark = pytest.mark.gpu
+
+MODES = [Y.MODE_PLAIN, Y.MODE_TILED]
+
+
+def maxdiff(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b)))) if np.size(a) else 0.0
+
+
+def gpu_apply(c, psi, mode=Y.MODE_PLAIN, k=0):
+    r = Y.ArrayReg.from_vec(c.nbits, psi)
+    Y.apply_inplace(c, r, mode, k)
+    return r.state_vec()
+
+
+# ------------------------------------------------------------------ golden
+def test_instruct_cases_bit_exact(golden):
+    """instruct.json cases as one-gate circuits (Custom matrices follow the
+    same dispatch as the named gates)."""
+    tested = 0
+    for case in golden("instruct")["cases"]:
+        if "locs" not in case or "regression" in case["label"]:
+            continue
+        if "gate_matrix" in case:
+            g = Gate.Custom(matrix_pairs(case["gate_matrix"]))
+        elif case.get("gate_name") in (None, "PSWAP", "CPHASE"):
+            continue
+        else:
+            g = named_gate(case["gate_name"], case.get("theta", 0.0))
+        n, locs = case["nbits"], case["locs"]
+        ctrl, bits = case.get("ctrl_locs", []), case.get("ctrl_bits", [])
+        if g.num_sites() == 1 and len(locs) > 1:
+            els = [Y.put([l], g) for l in locs]
+        else:
+            els = [Y.PositionedGate(g, locs, ctrl, [bool(b) for b in bits])]
+        c = Y.Circuit.qubits(n, els)
+        inp = pairs(case["input_state"])
+        for mode in MODES:
+            out = gpu_apply(c, inp, mode)
+            assert maxdiff(out, O.apply_circuit(c, inp)) == 0.0, case["label"]
+            assert maxdiff(out, pairs(case["output_state"])) < 1e-10, case["label"]
+        tested += 1
+    assert tested >= 40
+
+
+def test_instruct_regression_2q(golden):
+    case = [c for c in golden("instruct")["cases"] if "regression" in c["label"]][0]
+    g = Gate.Custom(matrix_pairs(case["gate_matrix"]))
+    c = Y.Circuit.qubits(case["nbits"], [Y.put(list(p), g) for p in case["gate_pairs"]])
+    out = gpu_apply(c, pairs(case["input_state"]))
+    assert maxdiff(out, pairs(case["output_state"])) < 1e-10
+
+
+def test_apply_ground_truth(golden):
+    tested = 0
+    for case in golden("apply")["cases"]:
+        if not all(d == 2 for d in case["dims"]):
+            continue
+        c = circuit_from_case(case)
+        inp = state(case["input_state_re"], case["input_state_im"])
+        ref = O.apply_circuit(c, inp)
+        for mode in MODES:
+            out = gpu_apply(c, inp, mode)
+            assert maxdiff(out, ref) == 0.0, case["label"]
+        assert maxdiff(out, state(case["output_state_re"], case["output_state_im"])) < 1e-10, case["label"]
+        tested += 1
+    assert tested >= 60
+
+
+def test_apply_rejects_qudits(golden):
+    case = [c for c in golden("apply")["cases"] if not all(d == 2 for d in c["dims"])][0]
+    c = circuit_from_case(case)
+    r = Y.ArrayReg.zero_state(len(case["dims"]))
+    with pytest.raises(Y.YaoError, match="qubit-only"):
+        Y.apply_inplace(c, r)
+    with pytest.raises(Y.YaoError, match="mismatch"):
+        Y.apply_inplace(Y.Circuit.qubits(3, [Y.put([0], Gate.H)]), Y.ArrayReg.zero_state(2))
+
+
+def test_measure_ground_truth(golden):
+    for case in golden("measure")["cases"]:
+        c = circuit_from_case(dict(case, dims=[2] * case["num_qubits"]))
+        r = Y.apply(c, Y.ArrayReg.zero_state(case["num_qubits"]))
+        assert maxdiff(Y.probs(r), case["probabilities"]) < 1e-10, case["label"]
+
+
+def test_pysim_ground_truth(golden):
+    for case in golden("pysim")["cases"]:
+        circ = case["circuit"]
+        n = circ["num_qubits"]
+        els = []
+        for el in circ["elements"]:
+            g = named_gate(el["gate"], (el.get("params") or [0.0])[0])
+            cs = el.get("controls", [])
+            els.append(Y.PositionedGate(g, el["targets"], cs, el.get("control_configs", [True] * len(cs))))
+        c = Y.Circuit.qubits(n, els)
+        out = Y.apply(c, Y.ArrayReg.zero_state(n)).state_vec()
+        assert maxdiff(out, state(case["state_re"], case["state_im"])) < 1e-12, case["label"]
+
+
+# ------------------------------------------------------- random circuits
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 8, 11, 13, 15])
+def test_random_circuits_bit_exact(n):
+    rng = np.random.default_rng(100 + n)
+    for rep in range(3):
+        c = random_circuit(rng, n, 60, max_ctrl=min(3, n - 1) if n > 1 else 0)
+        psi = random_state(rng, n)
+        ref = O.apply_circuit(c, psi)
+        for mode in MODES:
+            out = gpu_apply(c, psi, mode)
+            assert maxdiff(out, ref) == 0.0, (n, rep, mode)
+
+
+@pytest.mark.parametrize("n", [4, 12, 16])
+def test_fused_fp64_and_c64(n):
+    rng = np.random.default_rng(7 + n)
+    c = random_circuit(rng, n, 120, max_ctrl=2)
+    psi = random_state(rng, n)
+    ref = O.apply_circuit(c, psi)
+    for k in (2, 4, 5, 6):
+        out = gpu_apply(c, psi, Y.MODE_FUSED, k)
+        assert maxdiff(out, ref) < 1e-10, k
+        assert 1 - abs(np.vdot(ref, out)) ** 2 < 1e-12, k
+    r = Y.ArrayReg.from_vec(n, psi).to_precision(Y.C64)
+    Y.apply_inplace(c, r, Y.MODE_FUSED, 5)
+    out = r.state_vec().astype(np.complex128)
+    assert 1 - abs(np.vdot(ref, out)) ** 2 < 1e-6
+
+
+def test_layered_circuit_exact_and_roundtrip():
+    """The layered workload (Rx, Ry, Rz per qubit + CNOT brickwork) at n=16
+    against the oracle, and apply -> dagger round trip at n=24."""
+    c = layered_circuit(16, 4, seed=11)
+    z = np.zeros(1 << 16, complex)
+    z[0] = 1
+    ref = O.apply_circuit(c, z)
+    for mode in MODES:
+        assert maxdiff(gpu_apply(c, z, mode), ref) == 0.0
+    big = layered_circuit(24, 3, seed=12)
+    r = Y.ArrayReg.zero_state(24)
+    Y.apply_inplace(big, r, Y.MODE_TILED)
+    n1 = r.norm()
+    Y.apply_inplace(big.dagger(), r, Y.MODE_TILED)
+    v = r.state_vec()
+    assert abs(n1 - 1) < 1e-12
+    assert abs(v[0] - 1) < 1e-11 and np.max(np.abs(v[1:])) < 1e-11
+
+
+def test_qft20_bit_exact():
+    """QFT on 20 qubits (H + 190 controlled phases + 10 SWAPs) on a seeded
+    Gaussian state, against the oracle (max-abs 0; the bar is 1e-12)."""
+    rng = np.random.default_rng(2026)
+    psi = random_state(rng, 20)
+    c = qft_circuit(20)
+    assert len(c.elements) == 220
+    ref = O.apply_circuit(c, psi)
+    for mode in MODES:
+        assert maxdiff(gpu_apply(c, psi, mode), ref) == 0.0
+
+
+def test_channels_ignored_in_pure_apply():
+    """src/apply.rs:139-143: channels are skipped on an ArrayReg."""
+    c = Y.Circuit.qubits(2, [Y.put([0], Gate.H), Y.channel([1], NoiseChannel.BitFlip(0.3)), Y.label(0, "x")])
+    z = np.array([1, 0, 0, 0], complex)
+    assert maxdiff(gpu_apply(c, z), O.apply_circuit(c, z)) == 0.0
+
+
+# ---------------------------------------------------------- registers
+def test_register_constructors_and_reductions():
+    n = 10
+    r = Y.ArrayReg.deterministic_state(n)
+    ref = O.deterministic_state(n)
+    assert maxdiff(r.state_vec(), ref) < 1e-15
+    assert abs(r.norm() - 1) < 1e-13
+    assert abs(Y.ArrayReg.zero_state(3).state_vec()[0] - 1) == 0
+    g = Y.ArrayReg.ghz_state(3).state_vec()
+    assert abs(g[0] - 1 / math.sqrt(2)) < 1e-15 and abs(g[7] - 1 / math.sqrt(2)) < 1e-15
+    u = Y.ArrayReg.uniform_state(2).state_vec()
+    assert np.allclose(u, 0.5)
+    p = Y.ArrayReg.product_state([1, 0, 1]).state_vec()
+    assert p[5] == 1 and np.sum(np.abs(p)) == 1
+    rng = np.random.default_rng(1)
+    a, b = random_state(rng, n), random_state(rng, n)
+    ra, rb = Y.ArrayReg.from_vec(n, a), Y.ArrayReg.from_vec(n, b)
+    f = ra.fidelity(rb)
+    assert abs(f - O.fidelity(a, b, n)) < 1e-14
+    ra2 = Y.ArrayReg.from_vec(n, a * 3.0)
+    ra2.normalize()
+    assert maxdiff(ra2.state_vec(), a) < 1e-15
+    # complex64 round trip
+    c64 = ra.to_precision(Y.C64)
+    assert maxdiff(c64.state_vec(), a) < 1e-7
+    assert abs(ra.fidelity(c64) - 1) < 1e-7
+
+
+# ------------------------------------------------------------ expectation
+OPS = [Y.Op.I, Y.Op.X, Y.Op.Y, Y.Op.Z, Y.Op.P0, Y.Op.P1, Y.Op.Pu, Y.Op.Pd]
+
+
+def random_polynomial(rng, n, nterms):
+    coeffs, strs = [], []
+    for _ in range(nterms):
+        k = int(rng.integers(0, min(4, n) + 1))
+        sites = [int(s) for s in rng.integers(0, n, size=k)]  # duplicates allowed
+        ops = [OPS[int(rng.integers(len(OPS)))] for _ in sites]
+        strs.append(Y.OperatorString(list(zip(sites, ops))))
+        coeffs.append(complex(rng.normal(), rng.normal()))
+    return Y.OperatorPolynomial(coeffs, strs)
+
+
+@pytest.mark.parametrize("n", [1, 3, 7, 12])
+def test_expect_arrayreg(n):
+    rng = np.random.default_rng(40 + n)
+    psi = random_state(rng, n)
+    r = Y.ArrayReg.from_vec(n, psi)
+    for _ in range(5):
+        op = random_polynomial(rng, n, 12)
+        got, ref = Y.expect_arrayreg(r, op), O.expect_arrayreg(psi, n, op)
+        assert abs(got - ref) <= 1e-12 * max(1.0, abs(ref)), (got, ref)
+    op = tfim(n)
+    assert abs(Y.expect_arrayreg(r, op) - O.expect_arrayreg(psi, n, op)) < 1e-12
+
+
+# ----------------------------------------------------------------------- AD
+def test_expect_grad_matches_oracle_and_fd():
+    rng = np.random.default_rng(9)
+    n = 6
+    els = []
+    for _ in range(3):
+        for q in range(n):
+            els.append(Y.put([q], Gate.Ry(float(rng.uniform(-3, 3)))))
+            els.append(Y.put([q], Gate.Rz(float(rng.uniform(-3, 3)))))
+            els.append(Y.put([q], Gate.Rx(float(rng.uniform(-3, 3)))))
+        els.append(Y.control([0], [3], Gate.Ry(float(rng.uniform(-3, 3)))))
+        els.append(Y.PositionedGate(Gate.Phase(float(rng.uniform(-3, 3))), [2], [4, 5], [True, False]))
+        els.append(Y.put([1, 4], Gate.FSim(float(rng.uniform(-3, 3)), float(rng.uniform(-3, 3)))))
+        els.append(Y.put([2], Gate.SqrtW))
+        els.append(Y.control([1], [2], Gate.X))
+        els.append(Y.put([0, 5], Gate.ISWAP))
+    c = Y.Circuit.qubits(n, els)
+    op = tfim(n, 0.8) + Y.OperatorPolynomial.single(2, Y.Op.Y, 0.3)
+    psi0 = random_state(rng, n)
+    r0 = Y.ArrayReg.from_vec(n, psi0)
+    v, g = Y.expect_grad(op, c, r0)
+    vo, go = O.expect_grad(op, c, psi0)
+    assert abs(v - vo) < 1e-12
+    assert np.max(np.abs(np.array(g) - np.array(go))) < 1e-11
+    p0 = c.parameters()
+    h = 1e-5
+    for i in range(0, len(p0), 3):
+        pp, pm = list(p0), list(p0)
+        pp[i] += h
+        pm[i] -= h
+        c.dispatch(pp)
+        fp = Y.expect_arrayreg(Y.apply(c, r0), op).real
+        c.dispatch(pm)
+        fm = Y.expect_arrayreg(Y.apply(c, r0), op).real
+        assert abs((fp - fm) / (2 * h) - g[i]) < 1e-6
+    c.dispatch(p0)
+
+
+def test_expect_grad_rejects_channels():
+    c = Y.Circuit.qubits(1, [Y.put([0], Gate.Rx(0.3)), Y.channel([0], NoiseChannel.BitFlip(0.1))])
+    with pytest.raises(Y.YaoError, match="noise channel"):
+        Y.expect_grad(Y.OperatorPolynomial.single(0, Y.Op.Z, 1.0), c, Y.ArrayReg.zero_state(1))
+
+
+def test_vqe_gradient_small():
+    """The VQE ansatz (Ry.Rz layers + CNOT ring) with the TFIM Hamiltonian at
+    n=10, against the oracle."""
+    n, layers = 10, 3
+    rng = np.random.default_rng(77)
+    params = rng.uniform(-math.pi, math.pi, size=2 * n * layers)
+    c = vqe_ansatz(n, layers, params)
+    op = tfim(n)
+    z = np.zeros(1 << n, complex)
+    z[0] = 1
+    v, g = Y.expect_grad(op, c, Y.ArrayReg.zero_state(n))
+    vo, go = O.expect_grad(op, c, z)
+    assert abs(v - vo) < 1e-12
+    assert np.max(np.abs(np.array(g) - go)) < 1e-11
+
+
+# -------------------------------------------------------------- measurement
+def test_probs_and_marginals():
+    rng = np.random.default_rng(5)
+    n = 9
+    psi = random_state(rng, n)
+    r = Y.ArrayReg.from_vec(n, psi)
+    assert maxdiff(Y.probs(r), O.probs(psi, n)) == 0.0
+    for locs in ([0], [8], [3, 1], [0, 4, 8], [7, 2, 5, 1], list(range(n)), []):
+        assert maxdiff(Y.probs(r, locs), O.probs(psi, n, locs)) < 1e-15, locs
+    with pytest.raises(Y.YaoError, match="out of range"):
+        Y.probs(r, [9])
+    with pytest.raises(Y.YaoError, match="duplicate"):
+        Y.probs(r, [1, 1])
+
+
+class FixedRng:
+    def __init__(self, r):
+        self.r = r
+
+    def random(self):
+        return self.r
+
+
+@pytest.mark.parametrize("post", ["none", "reset", "remove"])
+def test_measure_with_postprocess(post):
+    rng = np.random.default_rng(11)
+    n = 7
+    for trial in range(6):
+        psi = random_state(rng, n)
+        locs = [int(x) for x in rng.permutation(n)[: int(rng.integers(1, 4))]]
+        rr = float(rng.uniform(0.01, 0.99))
+        reset_val = int(rng.integers(0, 1 << len(locs)))
+        code = {"none": 0, "reset": 1, "remove": 2}[post]
+        pp = {"none": Y.PostProcess.NoPostProcess, "reset": Y.PostProcess.ResetTo(reset_val),
+              "remove": Y.PostProcess.RemoveMeasured}[post]
+        r = Y.ArrayReg.from_vec(n, psi)
+        res = Y.measure_with_postprocess(r, locs, pp, FixedRng(rr))
+        oo, orem, ost = O.measure_with_postprocess(psi, n, locs, code, reset_val, rr)
+        assert res.outcome == oo
+        assert maxdiff(r.state_vec(), ost) < 1e-14
+        if post == "remove":
+            assert maxdiff(res.removed.state_vec(), orem) < 1e-14
+            assert abs(res.removed.norm() - 1) < 1e-13
+
+
+# ----------------------------------------------------------- density matrix
+CHANNELS = [
+    lambda: NoiseChannel.BitFlip(0.13), lambda: NoiseChannel.PhaseFlip(0.21),
+    lambda: NoiseChannel.Depolarizing(1, 0.17), lambda: NoiseChannel.PauliChannel(0.1, 0.05, 0.2),
+    lambda: NoiseChannel.Reset(0.1, 0.2), lambda: NoiseChannel.AmplitudeDamping(0.3, 0.1),
+    lambda: NoiseChannel.PhaseDamping(0.25), lambda: NoiseChannel.PhaseAmplitudeDamping(0.2, 0.1, 0.3),
+    lambda: NoiseChannel.ThermalRelaxation(1.0, 1.5, 0.2, 0.05),
+]
+
+
+def random_noisy_circuit(rng, n, depth):
+    base = random_circuit(rng, n, depth, max_ctrl=min(2, n - 1) if n > 1 else 0)
+    els = []
+    for el in base.elements:
+        els.append(el)
+        if rng.random() < 0.5:
+            q = int(rng.integers(n))
+            if n >= 2 and rng.random() < 0.3:
+                a, b = [int(x) for x in rng.permutation(n)[:2]]
+                els.append(Y.channel([a, b], NoiseChannel.Depolarizing(2, 0.07)))
+            else:
+                els.append(Y.channel([q], CHANNELS[int(rng.integers(len(CHANNELS)))]()))
+    return Y.Circuit.qubits(n, els)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5])
+def test_density_matrix_bit_exact(n):
+    rng = np.random.default_rng(300 + n)
+    c = random_noisy_circuit(rng, n, 25)
+    psi = random_state(rng, n)
+    rho0 = O.dm_from_reg(psi, n)
+    ref = O.dm_apply_circuit(c, rho0)
+    d = Y.DensityMatrix.from_reg(Y.ArrayReg.from_vec(n, psi))
+    assert maxdiff(d.state_data(), rho0) == 0.0
+    d.apply(c)
+    out = d.state_data()
+    assert maxdiff(out, ref) == 0.0
+    t = d.trace()
+    assert abs(t - O.dm_trace(ref, n)) < 1e-13
+    assert abs(d.purity() - O.dm_purity(ref, n)) < 1e-12
+    for traced in ([0], [n - 1], list(range(0, n, 2))):
+        if len(set(traced)) >= n:
+            continue
+        assert maxdiff(d.partial_tr(traced).state_data(), O.dm_partial_tr(ref, n, traced)) == 0.0
+    op = random_polynomial(rng, n, 6)
+    assert abs(Y.expect_dm(d, op) - O.expect_dm(ref, n, op)) < 1e-12
+    assert maxdiff(Y.probs(d), O.dm_probs(ref, n)) == 0.0
+    assert maxdiff(Y.probs(d, [n - 1, 0] if n > 1 else [0]), O.dm_probs(ref, n, [n - 1, 0] if n > 1 else [0])) == 0.0
+
+
+def test_density_matrix_golden(golden):
+    from test_oracle_golden import dm_cases
+    for key, c, psi, n, exp in dm_cases(golden):
+        d = Y.DensityMatrix.from_reg(Y.ArrayReg.from_vec(n, psi))
+        d.apply(c)
+        assert maxdiff(d.matrix(), exp) < 1e-10, key
+
+
+def test_density_matrix_purity_large():
+    """Purity through the tiled transpose kernel (dim >= 64) against numpy."""
+    n = 8
+    rng = np.random.default_rng(8)
+    c = random_noisy_circuit(rng, n, 20)
+    d = Y.DensityMatrix.from_reg(Y.ArrayReg.from_vec(n, random_state(rng, n)))
+    d.apply(c)
+    m = d.matrix()
+    assert abs(d.purity() - np.real(np.trace(m @ m))) < 1e-12
+    assert abs(d.purity() - O.dm_purity(d.state_data(), n)) < 1e-12
+    mixed = Y.DensityMatrix.mixed([0.5, 0.5], [Y.ArrayReg.zero_state(1), Y.ArrayReg.product_state([1])])
+    assert abs(mixed.purity() - 0.5) < 1e-12

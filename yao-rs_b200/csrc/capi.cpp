@@ -1,0 +1,1229 @@
+// capi.cpp — the extern "C" entry points of include/yao_gpu.h.
+//
+// Host-side responsibilities: argument validation with yao-rs's error
+// semantics (a panic or Err there is a negative status and a message here),
+// the conversion of the circuit wire format into lowered gates, and the
+// sequencing of device launches.  All device work runs on the context's
+// stream; functions that return host values synchronise it.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <set>
+#include <sstream>
+
+#include "yao_internal.h"
+
+// The opaque handle types of the C ABI; every object is created as one of
+// these, so the casts between the handle and its base type are valid.
+struct yao_ctx : yao::Ctx {};
+struct yao_circuit : yao::Circuit {};
+struct yao_reg : yao::Reg {};
+struct yao_dm : yao::DM {};
+
+namespace yao {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_err;
+void set_error(const std::string& m) { g_err = m; }
+void clear_error() { g_err.clear(); }
+int fail(int st, const std::string& m) {
+    g_err = m;
+    return st;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+    std::string m = std::string("CUDA error: ") + cudaGetErrorString(e) + " (" + what + ")";
+    g_err = m;
+    return e == cudaErrorMemoryAllocation ? YAO_ERR_OUT_OF_MEMORY : YAO_ERR_CUDA;
+}
+
+// ----------------------------------------------------------------- context
+int Ctx::ensure_scratch(size_t bytes) {
+    if (bytes <= scratch_bytes) return 0;
+    size_t nb = std::max<size_t>(bytes, 1 << 20);
+    if (scratch) {
+        cudaStreamSynchronize(stream);
+        cudaFree(scratch);
+        scratch = nullptr;
+        scratch_bytes = 0;
+    }
+    if (cudaMalloc(&scratch, nb) != cudaSuccess) {
+        scratch = nullptr;
+        fail(YAO_ERR_OUT_OF_MEMORY, "cannot allocate reduction scratch");
+        return -1;
+    }
+    scratch_bytes = nb;
+    return 0;
+}
+
+int Ctx::ensure_host_pinned(size_t bytes) {
+    if (bytes <= host_pinned_bytes) return 0;
+    size_t nb = std::max<size_t>(bytes, 4096);
+    if (host_pinned) cudaFreeHost(host_pinned);
+    if (cudaMallocHost(&host_pinned, nb) != cudaSuccess) {
+        host_pinned = nullptr;
+        host_pinned_bytes = 0;
+        fail(YAO_ERR_OUT_OF_MEMORY, "cannot allocate pinned host memory");
+        return -1;
+    }
+    host_pinned_bytes = nb;
+    return 0;
+}
+
+cudaEvent_t Ctx::take_event() {
+    if (!event_pool.empty()) {
+        cudaEvent_t e = event_pool.back();
+        event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void Ctx::prof_begin(const char* name, double bytes) {
+    ProfRec r;
+    r.name = name;
+    r.bytes = bytes;
+    r.a = take_event();
+    r.b = take_event();
+    cudaEventRecord(r.a, stream);
+    recs.push_back(r);
+}
+
+void Ctx::prof_end() {
+    if (!recs.empty()) cudaEventRecord(recs.back().b, stream);
+}
+
+static int use_device(const Ctx* c) {
+    YAO_CUDA(cudaSetDevice(c->device));
+    return YAO_OK;
+}
+
+// ---------------------------------------------------------- wire format
+
+static int read_element(const yao_element& e, Element& out) {
+    out.kind = e.kind;
+    if (e.kind == YAO_ELEM_GATE) {
+        GateElem& g = out.g;
+        g.type = e.type;
+        if (e.type < YAO_GATE_X || e.type > YAO_GATE_CUSTOM) return fail(YAO_ERR_INVALID_ARGUMENT, "unknown gate type");
+        g.targets.assign(e.targets, e.targets + e.ntargets);
+        g.ctrls.assign(e.ctrl_locs, e.ctrl_locs + e.nctrl);
+        if (e.ctrl_configs)
+            g.cfgs.assign(e.ctrl_configs, e.ctrl_configs + e.nconfigs);
+        else
+            g.cfgs.assign(e.nctrl, 1);
+        for (int i = 0; i < 4; i++) g.params[i] = e.params[i];
+        if (e.type == YAO_GATE_CUSTOM) {
+            if (!e.matrix || e.matrix_dim == 0) return fail(YAO_ERR_INVALID_ARGUMENT, "Custom gate needs a matrix");
+            g.custom_dim = e.matrix_dim;
+            const Cx* m = (const Cx*)e.matrix;
+            g.custom.assign(m, m + (size_t)e.matrix_dim * e.matrix_dim);
+            g.custom_diag = e.is_diagonal != 0;
+        }
+    } else if (e.kind == YAO_ELEM_CHANNEL) {
+        ChannelElem& c = out.ch;
+        c.type = e.type;
+        if (e.type < YAO_NOISE_BIT_FLIP || e.type > YAO_NOISE_CUSTOM)
+            return fail(YAO_ERR_INVALID_ARGUMENT, "unknown noise channel type");
+        c.locs.assign(e.targets, e.targets + e.ntargets);
+        for (int i = 0; i < 4; i++) c.params[i] = e.params[i];
+        c.depol_n = e.depol_n;
+        if (e.type == YAO_NOISE_COHERENT || e.type == YAO_NOISE_CUSTOM) {
+            if (!e.matrix || e.matrix_dim == 0) return fail(YAO_ERR_INVALID_ARGUMENT, "channel needs matrices");
+            c.dim = e.matrix_dim;
+            c.nkraus = e.type == YAO_NOISE_CUSTOM ? e.nkraus : 1;
+            const Cx* m = (const Cx*)e.matrix;
+            c.mats.assign(m, m + (size_t)c.dim * c.dim * c.nkraus);
+        }
+    } else if (e.kind == YAO_ELEM_ANNOTATION) {
+        if (e.ntargets < 1 || !e.targets) return fail(YAO_ERR_INVALID_ARGUMENT, "annotation needs a location");
+        out.annot_loc = e.targets[0];
+    } else {
+        return fail(YAO_ERR_INVALID_ARGUMENT, "unknown element kind");
+    }
+    return YAO_OK;
+}
+
+static int ilog2_exact(uint32_t d) {
+    int n = 0;
+    uint32_t p = 1;
+    while (p < d) p *= 2, n++;
+    return p == d ? n : -1;
+}
+
+static uint32_t channel_num_qubits(const ChannelElem& c) {
+    if (c.type == YAO_NOISE_DEPOLARIZING) return (uint32_t)c.depol_n;
+    if (c.type == YAO_NOISE_CUSTOM || c.type == YAO_NOISE_COHERENT) {
+        int n = ilog2_exact(c.dim);
+        return n < 0 ? 0xffffffffu : (uint32_t)n;
+    }
+    return 1;
+}
+
+static std::string locs_str(const std::vector<uint32_t>& v) {
+    std::ostringstream o;
+    o << "[";
+    for (size_t i = 0; i < v.size(); i++) o << (i ? ", " : "") << v[i];
+    o << "]";
+    return o.str();
+}
+
+// Circuit::new validation (src/circuit.rs:150-272), same rule order.
+static int validate(const std::vector<uint32_t>& dims, const std::vector<Element>& elems, int32_t* ce) {
+    const uint32_t ns = (uint32_t)dims.size();
+    auto err = [&](int kind, const std::string& m) {
+        if (ce) *ce = kind;
+        return fail(YAO_ERR_CIRCUIT, m);
+    };
+    for (const Element& el : elems) {
+        if (el.kind == YAO_ELEM_GATE) {
+            const GateElem& g = el.g;
+            if (g.cfgs.size() != g.ctrls.size())
+                return err(YAO_CE_CONTROL_CONFIG_LENGTH_MISMATCH, "control_configs length does not match control_locs length");
+            for (uint32_t l : g.targets)
+                if (l >= ns)
+                    return err(YAO_CE_LOC_OUT_OF_RANGE, "location " + std::to_string(l) + " is out of range (num_sites = " + std::to_string(ns) + ")");
+            for (uint32_t l : g.ctrls)
+                if (l >= ns)
+                    return err(YAO_CE_LOC_OUT_OF_RANGE, "location " + std::to_string(l) + " is out of range (num_sites = " + std::to_string(ns) + ")");
+            std::vector<uint32_t> ov;
+            for (uint32_t t : g.targets)
+                if (std::find(g.ctrls.begin(), g.ctrls.end(), t) != g.ctrls.end() &&
+                    std::find(ov.begin(), ov.end(), t) == ov.end())
+                    ov.push_back(t);
+            if (!ov.empty())
+                return err(YAO_CE_OVERLAPPING_LOCS, "target_locs and control_locs overlap at locations: " + locs_str(ov));
+            for (uint32_t l : g.ctrls)
+                if (dims[l] != 2)
+                    return err(YAO_CE_CONTROL_SITE_NOT_QUBIT, "control site at location " + std::to_string(l) + " has dimension " + std::to_string(dims[l]) + " (must be 2)");
+            if (g.type != YAO_GATE_CUSTOM)
+                for (uint32_t l : g.targets)
+                    if (dims[l] != 2)
+                        return err(YAO_CE_NAMED_GATE_TARGET_NOT_QUBIT, "named gate target site at location " + std::to_string(l) + " has dimension " + std::to_string(dims[l]) + " (must be 2)");
+            uint64_t prod = 1;
+            for (uint32_t l : g.targets) prod *= dims[l];
+            uint32_t msize = g.type == YAO_GATE_CUSTOM ? g.custom_dim : (g.type == YAO_GATE_SWAP || g.type == YAO_GATE_ISWAP || g.type == YAO_GATE_FSIM ? 4 : 2);
+            if (msize != prod)
+                return err(YAO_CE_MATRIX_SIZE_MISMATCH, "gate matrix size " + std::to_string(msize) + " does not match product of target site dimensions " + std::to_string(prod));
+        } else if (el.kind == YAO_ELEM_CHANNEL) {
+            const ChannelElem& c = el.ch;
+            for (uint32_t l : c.locs)
+                if (l >= ns)
+                    return err(YAO_CE_LOC_OUT_OF_RANGE, "location " + std::to_string(l) + " is out of range (num_sites = " + std::to_string(ns) + ")");
+            uint32_t nq = channel_num_qubits(c);
+            if (nq == 0xffffffffu) return fail(YAO_ERR_INVALID_ARGUMENT, "channel dimension is not a power of 2");
+            if (c.locs.size() != nq)
+                return err(YAO_CE_MATRIX_SIZE_MISMATCH, "gate matrix size " + std::to_string(c.locs.size()) + " does not match product of target site dimensions " + std::to_string(nq));
+            for (uint32_t l : c.locs)
+                if (dims[l] != 2)
+                    return err(YAO_CE_NAMED_GATE_TARGET_NOT_QUBIT, "named gate target site at location " + std::to_string(l) + " has dimension " + std::to_string(dims[l]) + " (must be 2)");
+            std::vector<uint32_t> seen, ov;
+            for (uint32_t l : c.locs) {
+                if (std::find(seen.begin(), seen.end(), l) != seen.end()) {
+                    if (std::find(ov.begin(), ov.end(), l) == ov.end()) ov.push_back(l);
+                } else {
+                    seen.push_back(l);
+                }
+            }
+            if (!ov.empty())
+                return err(YAO_CE_OVERLAPPING_LOCS, "target_locs and control_locs overlap at locations: " + locs_str(ov));
+        } else {
+            if (el.annot_loc >= ns)
+                return err(YAO_CE_LOC_OUT_OF_RANGE, "location " + std::to_string(el.annot_loc) + " is out of range (num_sites = " + std::to_string(ns) + ")");
+        }
+    }
+    return YAO_OK;
+}
+
+// The lowered gate list of a circuit (pure-state path, apply.rs:123-147).
+static const std::vector<LGate>& lowered(Circuit* c) {
+    std::lock_guard<std::mutex> lk(c->mu);
+    auto it = c->lowered.find(c->nbits);
+    if (it != c->lowered.end()) return it->second;
+    std::vector<LGate> prog;
+    for (const Element& el : c->elems)
+        if (el.kind == YAO_ELEM_GATE) lower_gate(el.g, c->nbits, 0, false, prog);
+    return c->lowered.emplace(c->nbits, std::move(prog)).first->second;
+}
+
+static int check_apply(const Circuit* c, const Reg* r) {
+    if (!c->qubit_only) return fail(YAO_ERR_QUBIT_ONLY, "ArrayReg only supports qubit-only circuits");
+    if (c->nbits != r->nbits) return fail(YAO_ERR_NBITS_MISMATCH, "Register and circuit qubit count mismatch");
+    return YAO_OK;
+}
+
+static int alloc_reg(Ctx* ctx, uint32_t nbits, int32_t prec, Reg** out) {
+    if (nbits > (uint32_t)kMaxQubits) return fail(YAO_ERR_INVALID_ARGUMENT, "too many qubits");
+    if (prec != YAO_C128 && prec != YAO_C64) return fail(YAO_ERR_INVALID_ARGUMENT, "unknown precision");
+    int s = use_device(ctx);
+    if (s) return s;
+    std::unique_ptr<yao_reg> r(new yao_reg());
+    r->ctx = ctx;
+    r->nbits = nbits;
+    r->precision = prec;
+    cudaError_t e = cudaMalloc(&r->d, r->bytes());
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(YAO_ERR_OUT_OF_MEMORY, "cannot allocate a " + std::to_string(nbits) + "-qubit register (" +
+                                               std::to_string(r->bytes()) + " bytes)");
+    }
+    *out = r.release();
+    return YAO_OK;
+}
+
+static int alloc_dm(Ctx* ctx, uint32_t nbits, DM** out) {
+    if (2 * nbits > (uint32_t)kMaxQubits) return fail(YAO_ERR_INVALID_ARGUMENT, "too many qubits");
+    int s = use_device(ctx);
+    if (s) return s;
+    std::unique_ptr<yao_dm> d(new yao_dm());
+    d->ctx = ctx;
+    d->nbits = nbits;
+    if (cudaMalloc(&d->d, d->bytes()) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(YAO_ERR_OUT_OF_MEMORY, "cannot allocate the density matrix");
+    }
+    *out = d.release();
+    return YAO_OK;
+}
+
+static int check_measure_locs(uint32_t nbits, const uint32_t* locs, uint32_t n) {
+    std::set<uint32_t> seen;
+    for (uint32_t i = 0; i < n; i++) {
+        if (locs[i] >= nbits)
+            return fail(YAO_ERR_MEASURE_LOCS, "measurement location " + std::to_string(locs[i]) +
+                                                  " is out of range for " + std::to_string(nbits) + " qubits");
+        if (!seen.insert(locs[i]).second)
+            return fail(YAO_ERR_MEASURE_LOCS, "duplicate measurement location " + std::to_string(locs[i]));
+    }
+    return YAO_OK;
+}
+
+static Cx cxmul(Cx a, Cx b) { return Cx{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+
+}  // namespace yao
+
+using namespace yao;
+
+#define CHECK_NULL(p)                                                                \
+    do {                                                                             \
+        if (!(p)) return fail(YAO_ERR_INVALID_ARGUMENT, "null argument: " #p);        \
+    } while (0)
+
+extern "C" {
+
+const char* yao_last_error(void) { return g_err.c_str(); }
+int yao_abi_version(void) { return YAO_GPU_ABI_VERSION; }
+
+// ------------------------------------------------------------------ context
+int yao_ctx_create(int device, yao_ctx** out) {
+    CHECK_NULL(out);
+    clear_error();
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(YAO_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= n) return fail(YAO_ERR_INVALID_ARGUMENT, "device index out of range");
+    YAO_CUDA(cudaSetDevice(device));
+    std::unique_ptr<yao_ctx> c(new yao_ctx());
+    c->device = device;
+    YAO_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    int sms = 0;
+    YAO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    c->num_sms = sms;
+    *out = c.release();
+    return YAO_OK;
+}
+
+int yao_ctx_destroy(yao_ctx* c) {
+    if (!c) return YAO_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    if (c->scratch) cudaFree(c->scratch);
+    if (c->host_pinned) cudaFreeHost(c->host_pinned);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return YAO_OK;
+}
+
+int yao_ctx_synchronize(yao_ctx* c) {
+    CHECK_NULL(c);
+    YAO_CUDA(cudaStreamSynchronize(c->stream));
+    return YAO_OK;
+}
+
+int yao_ctx_launch_count(const yao_ctx* c, uint64_t* out) {
+    CHECK_NULL(c);
+    CHECK_NULL(out);
+    *out = c->launches;
+    return YAO_OK;
+}
+
+int yao_ctx_stream(const yao_ctx* c, void** out) {
+    CHECK_NULL(c);
+    CHECK_NULL(out);
+    *out = (void*)c->stream;
+    return YAO_OK;
+}
+
+int yao_ctx_profile(yao_ctx* c, int enable) {
+    CHECK_NULL(c);
+    YAO_CUDA(cudaStreamSynchronize(c->stream));
+    for (auto& r : c->recs) {
+        c->event_pool.push_back(r.a);
+        c->event_pool.push_back(r.b);
+    }
+    c->recs.clear();
+    c->prof = enable != 0;
+    return YAO_OK;
+}
+
+int yao_ctx_profile_report(yao_ctx* c, char* buf, size_t cap) {
+    CHECK_NULL(c);
+    CHECK_NULL(buf);
+    YAO_CUDA(cudaStreamSynchronize(c->stream));
+    struct Agg {
+        uint64_t n = 0;
+        double ms = 0, bytes = 0;
+    };
+    std::map<std::string, Agg> agg;
+    std::vector<std::string> order;
+    for (auto& r : c->recs) {
+        float ms = 0.f;
+        YAO_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+        if (!agg.count(r.name)) order.push_back(r.name);
+        Agg& a = agg[r.name];
+        a.n++;
+        a.ms += ms;
+        a.bytes += r.bytes;
+    }
+    std::ostringstream o;
+    o.precision(17);
+    o << "[";
+    for (size_t i = 0; i < order.size(); i++) {
+        const Agg& a = agg[order[i]];
+        o << (i ? "," : "") << "{\"kernel\":\"" << order[i] << "\",\"launches\":" << a.n << ",\"ms\":" << a.ms
+          << ",\"bytes\":" << a.bytes << "}";
+    }
+    o << "]";
+    std::string s = o.str();
+    if (s.size() + 1 > cap) return fail(YAO_ERR_INVALID_ARGUMENT, "report buffer too small");
+    memcpy(buf, s.c_str(), s.size() + 1);
+    return YAO_OK;
+}
+
+// ------------------------------------------------------------------ circuit
+int yao_circuit_create(const uint32_t* dims, uint32_t nsites, const yao_element* elems, size_t nelems,
+                       yao_circuit** out, int32_t* ce_kind) {
+    CHECK_NULL(out);
+    clear_error();
+    if (ce_kind) *ce_kind = YAO_CE_NONE;
+    if (nsites && !dims) return fail(YAO_ERR_INVALID_ARGUMENT, "null dims");
+    if (nelems && !elems) return fail(YAO_ERR_INVALID_ARGUMENT, "null elements");
+    std::unique_ptr<yao_circuit> c(new yao_circuit());
+    c->dims.assign(dims, dims + nsites);
+    c->nbits = nsites;
+    c->qubit_only = std::all_of(c->dims.begin(), c->dims.end(), [](uint32_t d) { return d == 2; });
+    c->elems.resize(nelems);
+    for (size_t i = 0; i < nelems; i++) {
+        int s = read_element(elems[i], c->elems[i]);
+        if (s) return s;
+    }
+    int s = validate(c->dims, c->elems, ce_kind);
+    if (s) return s;
+    *out = c.release();
+    return YAO_OK;
+}
+
+void yao_circuit_free(yao_circuit* c) { delete c; }
+
+int yao_circuit_num_params(const yao_circuit* c, size_t* out) {
+    CHECK_NULL(c);
+    CHECK_NULL(out);
+    size_t n = 0;
+    for (const Element& el : c->elems)
+        if (el.kind == YAO_ELEM_GATE) n += (size_t)gate_num_params(el.g.type);
+    *out = n;
+    return YAO_OK;
+}
+
+int yao_circuit_parameters(const yao_circuit* c, double* out, size_t n) {
+    CHECK_NULL(c);
+    size_t np;
+    yao_circuit_num_params(c, &np);
+    if (n != np) return fail(YAO_ERR_INVALID_ARGUMENT, "parameter buffer length does not match num_params");
+    size_t k = 0;
+    for (const Element& el : c->elems)
+        if (el.kind == YAO_ELEM_GATE)
+            for (int i = 0; i < gate_num_params(el.g.type); i++) out[k++] = el.g.params[i];
+    return YAO_OK;
+}
+
+// Circuit::dispatch (src/circuit.rs:332-352)
+int yao_circuit_dispatch(yao_circuit* c, const double* params, size_t n) {
+    CHECK_NULL(c);
+    size_t np;
+    yao_circuit_num_params(c, &np);
+    if (n != np)
+        return fail(YAO_ERR_INVALID_ARGUMENT, "dispatch length " + std::to_string(n) + " does not match num_params " +
+                                                  std::to_string(np));
+    size_t k = 0;
+    for (Element& el : c->elems)
+        if (el.kind == YAO_ELEM_GATE)
+            for (int i = 0; i < gate_num_params(el.g.type); i++) el.g.params[i] = params[k++];
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->lowered.clear();
+    c->version++;
+    return YAO_OK;
+}
+
+// Circuit::dagger (src/circuit.rs:360-378)
+int yao_circuit_dagger(const yao_circuit* c, yao_circuit** out) {
+    CHECK_NULL(c);
+    CHECK_NULL(out);
+    std::unique_ptr<yao_circuit> d(new yao_circuit());
+    d->dims = c->dims;
+    d->nbits = c->nbits;
+    d->qubit_only = c->qubit_only;
+    for (size_t i = c->elems.size(); i-- > 0;) {
+        Element e = c->elems[i];
+        if (e.kind == YAO_ELEM_GATE) e.g = gate_dagger(e.g);
+        d->elems.push_back(e);
+    }
+    int s = validate(d->dims, d->elems, nullptr);
+    if (s) return s;
+    *out = d.release();
+    return YAO_OK;
+}
+
+int yao_gate_matrix(int32_t gate, const double* params, double* out, uint32_t* dim) {
+    CHECK_NULL(out);
+    CHECK_NULL(dim);
+    double zero[4] = {0, 0, 0, 0};
+    std::vector<Cx> m;
+    if (named_gate_matrix(gate, params ? params : zero, m, *dim) != 0)
+        return fail(YAO_ERR_INVALID_ARGUMENT, "not a named gate");
+    memcpy(out, m.data(), sizeof(Cx) * m.size());
+    return YAO_OK;
+}
+
+int yao_noise_kraus(const yao_element* ch, double* out, uint32_t max_kraus, uint32_t* nkraus, uint32_t* dim) {
+    CHECK_NULL(ch);
+    CHECK_NULL(nkraus);
+    CHECK_NULL(dim);
+    Element el;
+    int s = read_element(*ch, el);
+    if (s) return s;
+    std::vector<Cx> k;
+    s = channel_kraus(el.ch, k, *nkraus, *dim);
+    if (s) return s;
+    if (*nkraus > max_kraus) return fail(YAO_ERR_INVALID_ARGUMENT, "output buffer too small");
+    if (out) memcpy(out, k.data(), sizeof(Cx) * k.size());
+    return YAO_OK;
+}
+
+// NoiseChannel::superop (src/noise.rs:359-379): S = sum_i kron(conj(K_i), K_i)
+int yao_noise_superop(const yao_element* ch, double* out, uint32_t* dim2) {
+    CHECK_NULL(ch);
+    CHECK_NULL(out);
+    CHECK_NULL(dim2);
+    Element el;
+    int s = read_element(*ch, el);
+    if (s) return s;
+    std::vector<Cx> k;
+    uint32_t nk, d;
+    s = channel_kraus(el.ch, k, nk, d);
+    if (s) return s;
+    uint32_t d2 = d * d;
+    Cx* S = (Cx*)out;
+    for (uint32_t i = 0; i < d2 * d2; i++) S[i] = Cx{0, 0};
+    for (uint32_t q = 0; q < nk; q++) {
+        const Cx* K = k.data() + (size_t)q * d * d;
+        for (uint32_t i = 0; i < d; i++)
+            for (uint32_t j = 0; j < d; j++)
+                for (uint32_t kr = 0; kr < d; kr++)
+                    for (uint32_t kc = 0; kc < d; kc++) {
+                        Cx kcj = Cx{K[i * d + j].re, -K[i * d + j].im};
+                        Cx p = cxmul(kcj, K[kr * d + kc]);
+                        Cx& t = S[(i * d + kr) * d2 + j * d + kc];
+                        t.re += p.re;
+                        t.im += p.im;
+                    }
+    }
+    *dim2 = d2;
+    return YAO_OK;
+}
+
+// ---------------------------------------------------------------- registers
+int yao_reg_zero_state(yao_ctx* ctx, uint32_t nbits, int32_t precision, yao_reg** out) {
+    CHECK_NULL(ctx);
+    CHECK_NULL(out);
+    Reg* r;
+    int s = alloc_reg(ctx, nbits, precision, &r);
+    if (s) return s;
+    s = launch_fill_zero_state(ctx, r, 0);
+    if (s) {
+        cudaFree(r->d);
+        delete r;
+        return s;
+    }
+    *out = static_cast<yao_reg*>(r);
+    return YAO_OK;
+}
+
+int yao_reg_product_state(yao_ctx* ctx, uint32_t nbits, uint64_t basis, yao_reg** out) {
+    CHECK_NULL(ctx);
+    CHECK_NULL(out);
+    if (nbits < 64 && basis >= ((uint64_t)1 << nbits)) return fail(YAO_ERR_INVALID_ARGUMENT, "basis index out of range");
+    Reg* r;
+    int s = alloc_reg(ctx, nbits, YAO_C128, &r);
+    if (s) return s;
+    s = launch_fill_zero_state(ctx, r, basis);
+    *out = static_cast<yao_reg*>(r);
+    return s;
+}
+
+int yao_reg_from_host(yao_ctx* ctx, uint32_t nbits, const double* amps, yao_reg** out) {
+    CHECK_NULL(ctx);
+    CHECK_NULL(amps);
+    CHECK_NULL(out);
+    Reg* r;
+    int s = alloc_reg(ctx, nbits, YAO_C128, &r);
+    if (s) return s;
+    cudaError_t e = cudaMemcpyAsync(r->d, amps, r->bytes(), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(r->d);
+        delete r;
+        return cuda_fail(e, "upload");
+    }
+    *out = static_cast<yao_reg*>(r);
+    return YAO_OK;
+}
+
+int yao_reg_uniform_state(yao_ctx* ctx, uint32_t nbits, yao_reg** out) {
+    CHECK_NULL(ctx);
+    CHECK_NULL(out);
+    Reg* r;
+    int s = alloc_reg(ctx, nbits, YAO_C128, &r);
+    if (s) return s;
+    s = launch_uniform_state(ctx, r);
+    *out = static_cast<yao_reg*>(r);
+    return s;
+}
+
+// ArrayReg::ghz_state (src/register.rs:56-63)
+int yao_reg_ghz_state(yao_ctx* ctx, uint32_t nbits, yao_reg** out) {
+    CHECK_NULL(ctx);
+    CHECK_NULL(out);
+    Reg* r;
+    int s = alloc_reg(ctx, nbits, YAO_C128, &r);
+    if (s) return s;
+    s = launch_fill_zero_state(ctx, r, 0);
+    if (!s) {
+        double amp[2] = {1.0 / std::sqrt(2.0), 0.0};
+        uint64_t last = ((uint64_t)1 << nbits) - 1;
+        YAO_CUDA(cudaMemcpyAsync(r->d, amp, 16, cudaMemcpyHostToDevice, ctx->stream));
+        YAO_CUDA(cudaMemcpyAsync((char*)r->d + 16 * last, amp, 16, cudaMemcpyHostToDevice, ctx->stream));
+        YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    *out = static_cast<yao_reg*>(r);
+    return s;
+}
+
+int yao_reg_deterministic_state(yao_ctx* ctx, uint32_t nbits, yao_reg** out) {
+    CHECK_NULL(ctx);
+    CHECK_NULL(out);
+    Reg* r;
+    int s = alloc_reg(ctx, nbits, YAO_C128, &r);
+    if (s) return s;
+    s = launch_deterministic_state(ctx, r);
+    *out = static_cast<yao_reg*>(r);
+    return s;
+}
+
+void yao_reg_free(yao_reg* r) {
+    if (!r) return;
+    cudaSetDevice(r->ctx->device);
+    cudaStreamSynchronize(r->ctx->stream);
+    cudaFree(r->d);
+    delete r;
+}
+
+int yao_reg_clone(const yao_reg* r, yao_reg** out) {
+    CHECK_NULL(r);
+    CHECK_NULL(out);
+    Reg* c;
+    int s = alloc_reg(r->ctx, r->nbits, r->precision, &c);
+    if (s) return s;
+    YAO_CUDA(cudaMemcpyAsync(c->d, r->d, r->bytes(), cudaMemcpyDeviceToDevice, r->ctx->stream));
+    *out = static_cast<yao_reg*>(c);
+    return YAO_OK;
+}
+
+int yao_reg_convert(const yao_reg* r, int32_t precision, yao_reg** out) {
+    CHECK_NULL(r);
+    CHECK_NULL(out);
+    Reg* c;
+    int s = alloc_reg(r->ctx, r->nbits, precision, &c);
+    if (s) return s;
+    s = launch_convert(r->ctx, r, c);
+    *out = static_cast<yao_reg*>(c);
+    return s;
+}
+
+int yao_reg_nbits(const yao_reg* r, uint32_t* out) {
+    CHECK_NULL(r);
+    CHECK_NULL(out);
+    *out = r->nbits;
+    return YAO_OK;
+}
+
+int yao_reg_precision(const yao_reg* r, int32_t* out) {
+    CHECK_NULL(r);
+    CHECK_NULL(out);
+    *out = r->precision;
+    return YAO_OK;
+}
+
+int yao_reg_to_host(const yao_reg* r, void* amps) {
+    CHECK_NULL(r);
+    CHECK_NULL(amps);
+    YAO_CUDA(cudaSetDevice(r->ctx->device));
+    YAO_CUDA(cudaMemcpyAsync(amps, r->d, r->bytes(), cudaMemcpyDeviceToHost, r->ctx->stream));
+    YAO_CUDA(cudaStreamSynchronize(r->ctx->stream));
+    return YAO_OK;
+}
+
+int yao_reg_upload(yao_reg* r, const void* amps) {
+    CHECK_NULL(r);
+    CHECK_NULL(amps);
+    YAO_CUDA(cudaSetDevice(r->ctx->device));
+    YAO_CUDA(cudaMemcpyAsync(r->d, amps, r->bytes(), cudaMemcpyHostToDevice, r->ctx->stream));
+    YAO_CUDA(cudaStreamSynchronize(r->ctx->stream));
+    return YAO_OK;
+}
+
+int yao_reg_device_ptr(const yao_reg* r, void** out) {
+    CHECK_NULL(r);
+    CHECK_NULL(out);
+    *out = r->d;
+    return YAO_OK;
+}
+
+int yao_reg_norm(const yao_reg* r, double* out) {
+    CHECK_NULL(r);
+    CHECK_NULL(out);
+    YAO_CUDA(cudaSetDevice(r->ctx->device));
+    double ns;
+    int s = reduce_norm_sqr(r->ctx, r, &ns);
+    if (s) return s;
+    *out = std::sqrt(ns);
+    return YAO_OK;
+}
+
+int yao_reg_normalize(yao_reg* r) {
+    double nrm;
+    int s = yao_reg_norm(r, &nrm);
+    if (s) return s;
+    if (nrm > 0.0) return launch_scale(r->ctx, r, nrm);
+    return YAO_OK;
+}
+
+int yao_reg_fidelity(const yao_reg* a, const yao_reg* b, double* out) {
+    CHECK_NULL(a);
+    CHECK_NULL(b);
+    CHECK_NULL(out);
+    if (a->nbits != b->nbits) return fail(YAO_ERR_NBITS_MISMATCH, "fidelity of registers with different qubit counts");
+    if (a->ctx != b->ctx) return fail(YAO_ERR_INVALID_ARGUMENT, "registers of different contexts");
+    YAO_CUDA(cudaSetDevice(a->ctx->device));
+    Cx inner;
+    int s = reduce_inner(a->ctx, a, b, &inner);
+    if (s) return s;
+    *out = inner.re * inner.re + inner.im * inner.im;
+    return YAO_OK;
+}
+
+int yao_reg_max_abs_diff(const yao_reg* a, const yao_reg* b, double* out) {
+    CHECK_NULL(a);
+    CHECK_NULL(b);
+    CHECK_NULL(out);
+    if (a->nbits != b->nbits) return fail(YAO_ERR_NBITS_MISMATCH, "registers with different qubit counts");
+    YAO_CUDA(cudaSetDevice(a->ctx->device));
+    return reduce_max_abs_diff(a->ctx, a, b, out);
+}
+
+// --------------------------------------------------------------------- apply
+int yao_apply_inplace_mode(const yao_circuit* cc, yao_reg* r, int32_t mode, int32_t k) {
+    CHECK_NULL(cc);
+    CHECK_NULL(r);
+    clear_error();
+    yao_circuit* c = const_cast<yao_circuit*>(cc);
+    int s = check_apply(c, r);
+    if (s) return s;
+    if (mode < YAO_MODE_PLAIN || mode > YAO_MODE_FUSED) return fail(YAO_ERR_INVALID_ARGUMENT, "unknown apply mode");
+    YAO_CUDA(cudaSetDevice(r->ctx->device));
+    const std::vector<LGate>& prog = lowered(c);
+    s = launch_program(r->ctx, r, prog, mode, k);
+    if (s) return s;
+    YAO_CUDA(cudaGetLastError());
+    return YAO_OK;
+}
+
+int yao_apply_inplace(const yao_circuit* c, yao_reg* r) { return yao_apply_inplace_mode(c, r, YAO_MODE_PLAIN, 0); }
+
+int yao_apply(const yao_circuit* c, const yao_reg* r, yao_reg** out) {
+    CHECK_NULL(c);
+    CHECK_NULL(r);
+    CHECK_NULL(out);
+    int s = check_apply(c, r);
+    if (s) return s;
+    yao_reg* n;
+    s = yao_reg_clone(r, &n);
+    if (s) return s;
+    s = yao_apply_inplace(c, n);
+    if (s) {
+        yao_reg_free(n);
+        return s;
+    }
+    *out = n;
+    return YAO_OK;
+}
+
+// ------------------------------------------------------------ density matrix
+int yao_dm_from_reg(const yao_reg* r, yao_dm** out) {
+    CHECK_NULL(r);
+    CHECK_NULL(out);
+    if (r->precision != YAO_C128) return fail(YAO_ERR_UNSUPPORTED, "density matrices are complex128");
+    DM* d;
+    int s = alloc_dm(r->ctx, r->nbits, &d);
+    if (s) return s;
+    s = launch_dm_from_reg(r->ctx, r, d);
+    *out = static_cast<yao_dm*>(d);
+    return s;
+}
+
+int yao_dm_zero_state(yao_ctx* ctx, uint32_t nbits, yao_dm** out) {
+    CHECK_NULL(ctx);
+    CHECK_NULL(out);
+    yao_reg* r;
+    int s = yao_reg_zero_state(ctx, nbits, YAO_C128, &r);
+    if (s) return s;
+    s = yao_dm_from_reg(r, out);
+    yao_reg_free(r);
+    return s;
+}
+
+int yao_dm_from_host(yao_ctx* ctx, uint32_t nbits, const double* rho, yao_dm** out) {
+    CHECK_NULL(ctx);
+    CHECK_NULL(rho);
+    CHECK_NULL(out);
+    DM* d;
+    int s = alloc_dm(ctx, nbits, &d);
+    if (s) return s;
+    YAO_CUDA(cudaMemcpyAsync(d->d, rho, d->bytes(), cudaMemcpyHostToDevice, ctx->stream));
+    YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+    *out = static_cast<yao_dm*>(d);
+    return YAO_OK;
+}
+
+int yao_dm_mixed(yao_ctx* ctx, const double* weights, const yao_reg* const* regs, size_t n, yao_dm** out) {
+    CHECK_NULL(ctx);
+    CHECK_NULL(out);
+    if (n == 0 || !weights || !regs) return fail(YAO_ERR_INVALID_ARGUMENT, "mixed needs at least one register");
+    uint32_t nb = regs[0]->nbits;
+    for (size_t i = 0; i < n; i++)
+        if (regs[i]->nbits != nb || regs[i]->precision != YAO_C128)
+            return fail(YAO_ERR_INVALID_ARGUMENT, "registers differ in size or precision");
+    DM* d;
+    int s = alloc_dm(ctx, nb, &d);
+    if (s) return s;
+    YAO_CUDA(cudaMemsetAsync(d->d, 0, d->bytes(), ctx->stream));
+    for (size_t i = 0; i < n && !s; i++) s = launch_dm_mixed_accum(ctx, regs[i], weights[i], d);
+    *out = static_cast<yao_dm*>(d);
+    return s;
+}
+
+void yao_dm_free(yao_dm* d) {
+    if (!d) return;
+    cudaSetDevice(d->ctx->device);
+    cudaStreamSynchronize(d->ctx->stream);
+    cudaFree(d->d);
+    delete d;
+}
+
+int yao_dm_clone(const yao_dm* d, yao_dm** out) {
+    CHECK_NULL(d);
+    CHECK_NULL(out);
+    DM* c;
+    int s = alloc_dm(d->ctx, d->nbits, &c);
+    if (s) return s;
+    YAO_CUDA(cudaMemcpyAsync(c->d, d->d, d->bytes(), cudaMemcpyDeviceToDevice, d->ctx->stream));
+    *out = static_cast<yao_dm*>(c);
+    return YAO_OK;
+}
+
+int yao_dm_nbits(const yao_dm* d, uint32_t* out) {
+    CHECK_NULL(d);
+    CHECK_NULL(out);
+    *out = d->nbits;
+    return YAO_OK;
+}
+
+int yao_dm_to_host(const yao_dm* d, double* rho) {
+    CHECK_NULL(d);
+    CHECK_NULL(rho);
+    YAO_CUDA(cudaSetDevice(d->ctx->device));
+    YAO_CUDA(cudaMemcpyAsync(rho, d->d, d->bytes(), cudaMemcpyDeviceToHost, d->ctx->stream));
+    YAO_CUDA(cudaStreamSynchronize(d->ctx->stream));
+    return YAO_OK;
+}
+
+int yao_dm_apply(yao_dm* d, const yao_circuit* cc) {
+    CHECK_NULL(d);
+    CHECK_NULL(cc);
+    clear_error();
+    const Circuit* c = cc;
+    if (!c->qubit_only) return fail(YAO_ERR_QUBIT_ONLY, "DensityMatrix only supports qubit-only circuits");
+    if (c->nbits != d->nbits) return fail(YAO_ERR_NBITS_MISMATCH, "Register and circuit qubit count mismatch");
+    YAO_CUDA(cudaSetDevice(d->ctx->device));
+    const uint32_t n = d->nbits, nb = 2 * n;
+    for (const Element& el : c->elems) {
+        if (el.kind == YAO_ELEM_GATE) {
+            std::vector<LGate> rows, cols;
+            lower_gate(el.g, nb, 0, false, rows);
+            lower_gate(el.g, nb, n, true, cols);
+            for (size_t i = 0; i < rows.size(); i++) {
+                int s = launch_dm_gate(d->ctx, d, rows[i], cols[i]);
+                if (s) return s;
+            }
+        } else if (el.kind == YAO_ELEM_CHANNEL) {
+            std::vector<Cx> kraus;
+            uint32_t nk, dim;
+            int s = channel_kraus(el.ch, kraus, nk, dim);
+            if (s) return s;
+            std::vector<LGate> rows, cols;
+            for (uint32_t q = 0; q < nk; q++) {
+                std::vector<Cx> K(kraus.begin() + (size_t)q * dim * dim, kraus.begin() + (size_t)(q + 1) * dim * dim);
+                bool diag = matrix_is_diagonal(K.data(), dim);
+                std::vector<Cx> Kc(K);
+                for (auto& v : Kc) v.im = -v.im;
+                rows.push_back(lower_matrix(K, dim, diag, el.ch.locs, {}, {}, nb, 0));
+                cols.push_back(lower_matrix(Kc, dim, diag, el.ch.locs, {}, {}, nb, n));
+            }
+            s = launch_dm_channel(d->ctx, d, rows, cols, {}, {});
+            if (s) return s;
+        }
+    }
+    YAO_CUDA(cudaGetLastError());
+    return YAO_OK;
+}
+
+int yao_dm_trace(const yao_dm* d, double out[2]) {
+    CHECK_NULL(d);
+    CHECK_NULL(out);
+    YAO_CUDA(cudaSetDevice(d->ctx->device));
+    Cx t;
+    int s = reduce_dm_trace(d->ctx, d, &t);
+    out[0] = t.re;
+    out[1] = t.im;
+    return s;
+}
+
+int yao_dm_purity(const yao_dm* d, double* out) {
+    CHECK_NULL(d);
+    CHECK_NULL(out);
+    YAO_CUDA(cudaSetDevice(d->ctx->device));
+    return reduce_dm_purity(d->ctx, d, out);
+}
+
+int yao_dm_partial_tr(const yao_dm* d, const uint32_t* traced, uint32_t n, yao_dm** out) {
+    CHECK_NULL(d);
+    CHECK_NULL(out);
+    if (n && !traced) return fail(YAO_ERR_INVALID_ARGUMENT, "null traced locs");
+    std::set<uint32_t> tr;
+    for (uint32_t i = 0; i < n; i++) {
+        if (traced[i] >= d->nbits) return fail(YAO_ERR_INVALID_ARGUMENT, "traced location out of range");
+        tr.insert(traced[i]);
+    }
+    DM* o;
+    int s = alloc_dm(d->ctx, d->nbits - (uint32_t)tr.size(), &o);
+    if (s) return s;
+    s = launch_dm_partial_tr(d->ctx, d, traced, n, o);
+    *out = static_cast<yao_dm*>(o);
+    return s;
+}
+
+// --------------------------------------------------------------- observables
+int yao_expect_arrayreg(const yao_reg* r, const yao_term* terms, size_t nterms, double out[2]) {
+    CHECK_NULL(r);
+    CHECK_NULL(out);
+    clear_error();
+    std::vector<MonoTerm> mt;
+    int s = build_mono_terms(terms, nterms, r->nbits, true, mt);
+    if (s) return s;
+    YAO_CUDA(cudaSetDevice(r->ctx->device));
+    std::vector<Cx> vals;
+    s = expect_terms(r->ctx, r, mt, vals);
+    if (s) return s;
+    Cx acc{0, 0};
+    for (size_t t = 0; t < mt.size(); t++) {
+        Cx p = cxmul(mt[t].coeff, vals[t]);
+        acc.re += p.re;
+        acc.im += p.im;
+    }
+    out[0] = acc.re;
+    out[1] = acc.im;
+    return YAO_OK;
+}
+
+int yao_expect_dm(const yao_dm* d, const yao_term* terms, size_t nterms, double out[2]) {
+    CHECK_NULL(d);
+    CHECK_NULL(out);
+    clear_error();
+    std::vector<MonoTerm> mt;
+    int s = build_mono_terms(terms, nterms, d->nbits, false, mt);
+    if (s) return s;
+    YAO_CUDA(cudaSetDevice(d->ctx->device));
+    std::vector<Cx> vals;
+    s = reduce_dm_expect(d->ctx, d, mt, vals);
+    if (s) return s;
+    Cx acc{0, 0};
+    for (size_t t = 0; t < mt.size(); t++) {
+        Cx p = cxmul(mt[t].coeff, vals[t]);
+        acc.re += p.re;
+        acc.im += p.im;
+    }
+    out[0] = acc.re;
+    out[1] = acc.im;
+    return YAO_OK;
+}
+
+// expect_grad (src/ad.rs:75-156)
+int yao_expect_grad(const yao_term* terms, size_t nterms, const yao_circuit* cc, const yao_reg* psi0,
+                    double* value, double* grad, size_t ngrad) {
+    CHECK_NULL(cc);
+    CHECK_NULL(psi0);
+    CHECK_NULL(value);
+    clear_error();
+    yao_circuit* c = const_cast<yao_circuit*>(cc);
+    for (const Element& el : c->elems)
+        if (el.kind == YAO_ELEM_CHANNEL)
+            return fail(YAO_ERR_CHANNEL_IN_AD,
+                        "expect_grad: circuit contains a noise channel; AD is unsupported for channels");
+    int s = check_apply(c, psi0);
+    if (s) return s;
+    if (psi0->precision != YAO_C128) return fail(YAO_ERR_UNSUPPORTED, "expect_grad runs on complex128 registers");
+    size_t np;
+    yao_circuit_num_params(c, &np);
+    if (ngrad != np) return fail(YAO_ERR_INVALID_ARGUMENT, "gradient buffer length does not match num_params");
+    if (np && !grad) return fail(YAO_ERR_INVALID_ARGUMENT, "null gradient buffer");
+    std::vector<MonoTerm> mt;
+    s = build_mono_terms(terms, nterms, psi0->nbits, true, mt);
+    if (s) return s;
+    Ctx* ctx = psi0->ctx;
+    YAO_CUDA(cudaSetDevice(ctx->device));
+    yao_reg* psi = nullptr;
+    yao_reg* lam = nullptr;
+    s = yao_reg_clone(psi0, &psi);
+    if (s) return s;
+    struct Guard {
+        yao_reg** a;
+        yao_reg** b;
+        ~Guard() {
+            yao_reg_free(*a);
+            yao_reg_free(*b);
+        }
+    } guard{&psi, &lam};
+    s = launch_program(ctx, psi, lowered(c), YAO_MODE_PLAIN, 0);
+    if (s) return s;
+    std::vector<Cx> vals;
+    s = expect_terms(ctx, psi, mt, vals);
+    if (s) return s;
+    Cx acc{0, 0};
+    for (size_t t = 0; t < mt.size(); t++) {
+        Cx p = cxmul(mt[t].coeff, vals[t]);
+        acc.re += p.re;
+        acc.im += p.im;
+    }
+    *value = acc.re;
+    if (np == 0) return YAO_OK;
+    Reg* l;
+    s = alloc_reg(ctx, psi0->nbits, YAO_C128, &l);
+    if (s) return s;
+    lam = static_cast<yao_reg*>(l);
+    s = build_lambda(ctx, psi, mt, lam);
+    if (s) return s;
+    size_t slot = np;
+    for (size_t ei = c->elems.size(); ei-- > 0;) {
+        const Element& el = c->elems[ei];
+        if (el.kind != YAO_ELEM_GATE) continue;
+        const GateElem& g = el.g;
+        std::vector<LGate> dag;
+        lower_gate(gate_dagger(g), psi0->nbits, 0, false, dag);
+        int npar = gate_num_params(g.type);
+        if (npar > 0) {
+            LGate gens[2];
+            gens[0].k = 0;
+            gens[1].k = 0;
+            for (int i = 0; i < npar; i++) {
+                std::vector<Cx> gm;
+                uint32_t gd;
+                gate_generator(g, i, gm, gd);
+                gens[i] = lower_matrix(gm, gd, false, g.targets, g.ctrls, g.cfgs, psi0->nbits, 0);
+            }
+            Cx dots[2];
+            s = adjoint_step(ctx, psi, lam, gens, dag, dots);
+            if (s) return s;
+            for (int i = 0; i < npar; i++) grad[slot - npar + i] = 2.0 * dots[i].re;
+            slot -= npar;
+        } else {
+            for (const LGate& dg : dag) {
+                s = launch_gate(ctx, psi->d, YAO_C128, psi0->nbits, dg);
+                if (s) return s;
+                s = launch_gate(ctx, lam->d, YAO_C128, psi0->nbits, dg);
+                if (s) return s;
+            }
+        }
+    }
+    YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+    return YAO_OK;
+}
+
+// --------------------------------------------------------------- measurement
+int yao_probs(const yao_reg* r, const uint32_t* locs, int32_t nlocs, double* out) {
+    CHECK_NULL(r);
+    CHECK_NULL(out);
+    clear_error();
+    Ctx* ctx = r->ctx;
+    YAO_CUDA(cudaSetDevice(ctx->device));
+    if (nlocs < 0) {
+        uint64_t n = (uint64_t)1 << r->nbits;
+        if (ctx->ensure_scratch(sizeof(double) * n)) return YAO_ERR_OUT_OF_MEMORY;
+        int s = launch_probs_full(ctx, r, (double*)ctx->scratch);
+        if (s) return s;
+        YAO_CUDA(cudaMemcpyAsync(out, ctx->scratch, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+        return YAO_OK;
+    }
+    int s = check_measure_locs(r->nbits, locs, (uint32_t)nlocs);
+    if (s) return s;
+    std::vector<uint32_t> bits(nlocs);
+    for (int32_t i = 0; i < nlocs; i++) bits[i] = r->nbits - 1 - locs[i];
+    return reduce_marginal(ctx, r, bits.data(), (uint32_t)nlocs, out);
+}
+
+int yao_dm_probs(const yao_dm* d, const uint32_t* locs, int32_t nlocs, double* out) {
+    CHECK_NULL(d);
+    CHECK_NULL(out);
+    clear_error();
+    YAO_CUDA(cudaSetDevice(d->ctx->device));
+    std::vector<uint32_t> bits;
+    if (nlocs >= 0) {
+        int s = check_measure_locs(d->nbits, locs, (uint32_t)nlocs);
+        if (s) return s;
+        for (int32_t i = 0; i < nlocs; i++) bits.push_back(d->nbits - 1 - locs[i]);
+    }
+    return reduce_dm_marginal(d->ctx, d, bits.data(), nlocs, out);
+}
+
+// measure_with_postprocess (src/measure.rs:243-274)
+int yao_measure_with_postprocess(yao_reg* r, const uint32_t* locs, uint32_t nlocs, int32_t post, uint64_t reset_val,
+                                 double rand01, uint8_t* outcome, yao_reg** removed) {
+    CHECK_NULL(r);
+    clear_error();
+    int s = check_measure_locs(r->nbits, locs, nlocs);
+    if (s) return s;
+    if (nlocs && (!locs || !outcome)) return fail(YAO_ERR_INVALID_ARGUMENT, "null locs or outcome");
+    if (post == YAO_POST_REMOVE_MEASURED && !removed) return fail(YAO_ERR_INVALID_ARGUMENT, "null removed");
+    Ctx* ctx = r->ctx;
+    YAO_CUDA(cudaSetDevice(ctx->device));
+    uint64_t np = (uint64_t)1 << nlocs;
+    std::vector<double> probs(np);
+    std::vector<uint32_t> bits(nlocs);
+    for (uint32_t i = 0; i < nlocs; i++) bits[i] = r->nbits - 1 - locs[i];
+    s = reduce_marginal(ctx, r, bits.data(), nlocs, probs.data());
+    if (s) return s;
+    // sample_from_probs (:140-150): sequential cumsum, first r < cumsum
+    uint64_t idx = np - 1;
+    double cumsum = 0.0;
+    for (uint64_t i = 0; i < np; i++) {
+        cumsum += probs[i];
+        if (rand01 < cumsum) {
+            idx = i;
+            break;
+        }
+    }
+    // decode_outcome_bits (:152-156): MSB first
+    uint64_t mask = 0, value = 0;
+    for (uint32_t i = 0; i < nlocs; i++) {
+        outcome[i] = (uint8_t)((idx >> (nlocs - 1 - i)) & 1);
+        mask |= (uint64_t)1 << bits[i];
+        if (outcome[i]) value |= (uint64_t)1 << bits[i];
+    }
+    if (post == YAO_POST_NONE) return YAO_OK;
+    if (post == YAO_POST_RESET_TO && reset_val >= np)
+        return fail(YAO_ERR_INVALID_ARGUMENT, "reset value " + std::to_string(reset_val) + " does not fit in " +
+                                                  std::to_string(nlocs) + " measured qubits");
+    if (post != YAO_POST_RESET_TO && post != YAO_POST_REMOVE_MEASURED)
+        return fail(YAO_ERR_INVALID_ARGUMENT, "unknown post-processing");
+    // collapse_qubits_to (:158-185)
+    double norm_sq;
+    s = launch_collapse(ctx, r, mask, value, &norm_sq);
+    if (s) return s;
+    double nrm = std::sqrt(norm_sq);
+    if (nrm > 1e-15) {
+        s = launch_scale(ctx, r, nrm);
+        if (s) return s;
+    }
+    if (post == YAO_POST_RESET_TO) {
+        // reset_qubits_to (:187-215)
+        uint64_t swap = 0;
+        for (uint32_t i = 0; i < nlocs; i++) {
+            uint8_t to = (uint8_t)((reset_val >> (nlocs - 1 - i)) & 1);
+            if (to != outcome[i]) swap |= (uint64_t)1 << bits[i];
+        }
+        if (swap) s = launch_reset_move(ctx, r, mask, value, swap);
+        if (!s) YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+        return s;
+    }
+    // remove_measured_qubits (:217-240)
+    std::vector<uint32_t> kept;
+    for (uint32_t loc = 0; loc < r->nbits; loc++)
+        if (std::find(locs, locs + nlocs, loc) == locs + nlocs) kept.push_back(r->nbits - 1 - loc);
+    Reg* nr;
+    s = alloc_reg(ctx, (uint32_t)kept.size(), r->precision, &nr);
+    if (s) return s;
+    s = launch_remove_gather_fixed(ctx, r, nr, kept.data(), (uint32_t)kept.size(), value);
+    if (!s) {
+        double ns2;
+        s = reduce_norm_sqr(ctx, nr, &ns2);
+        if (!s && std::sqrt(ns2) > 0.0) s = launch_scale(ctx, nr, std::sqrt(ns2));
+    }
+    if (s) {
+        yao_reg_free(static_cast<yao_reg*>(nr));
+        return s;
+    }
+    YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+    *removed = static_cast<yao_reg*>(nr);
+    return YAO_OK;
+}
+
+// ------------------------------------------------------------------ batched
+int yao_batch_apply(const yao_circuit* const* circuits, yao_reg* const* regs, size_t n, int32_t mode, int32_t k) {
+    if (n && (!circuits || !regs)) return fail(YAO_ERR_INVALID_ARGUMENT, "null batch arrays");
+    for (size_t i = 0; i < n; i++) {
+        int s = check_apply(circuits[i], regs[i]);
+        if (s) return s;
+    }
+    for (size_t i = 0; i < n; i++) {
+        int s = yao_apply_inplace_mode(circuits[i], regs[i], mode, k);
+        if (s) return s;
+    }
+    return YAO_OK;
+}
+
+}  // extern "C"

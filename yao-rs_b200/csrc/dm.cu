@@ -1,0 +1,583 @@
+// dm.cu — density-matrix kernels.
+//
+// rho is stored row-major (rho[row * dim + col], yao-rs
+// src/density_matrix.rs:7-12) and treated as a 2n-qubit vector whose high n
+// bits are the row index.  yao-rs applies a gate as two full passes (U on
+// the row bits, then conj(U) on the column bits, :161-178) and a channel as
+// about eight passes per Kraus operator (:181-224).  Here:
+//
+//  - a gate is ONE pass: each group of 4^k entries (k row targets x k column
+//    targets) is loaded once, U is applied along the row bits and then
+//    conj(U) along the column bits, with the PLAIN arithmetic.  Every entry
+//    sees the same operation sequence as in the two-pass CPU code, so the
+//    result is bit-identical.
+//  - a channel is ONE pass: for each group, branch = original, K_i on the
+//    rows, conj(K_i) on the columns, acc += branch, for every Kraus operator
+//    in order: the CPU path's accumulation, per entry, in one HBM round trip.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "device_common.cuh"
+
+namespace yao {
+
+#define GRID_STRIDE(i, n) \
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (uint64_t)gridDim.x * blockDim.x)
+
+constexpr int kDT = 256;
+
+// ------------------------------------------------------------- from_reg
+
+// rho[r, c] = psi[r] * conj(psi[c]) (src/density_matrix.rs:23-35)
+__global__ void k_dm_from_reg(const double2* __restrict__ psi, double2* __restrict__ rho, uint32_t n) {
+    const uint64_t dim = 1ull << n;
+    GRID_STRIDE(i, dim * dim) {
+        uint64_t r = i >> n, c = i & (dim - 1);
+        double2 a = psi[r], b = psi[c];
+        rho[i] = cmul_x(a, make_double2(b.x, -b.y));
+    }
+}
+
+int launch_dm_from_reg(Ctx* ctx, const Reg* r, DM* d) {
+    uint64_t tot = (uint64_t)1 << (2 * r->nbits);
+    k_dm_from_reg<<<grid_for(tot, 256, ctx->num_sms), 256, 0, ctx->stream>>>((const double2*)r->d, (double2*)d->d,
+                                                                             r->nbits);
+    ctx->launches++;
+    YAO_CUDA(cudaGetLastError());
+    return YAO_OK;
+}
+
+// rho[r, c] += (w * psi[r]) * conj(psi[c]) (DensityMatrix::mixed, :37-57)
+__global__ void k_dm_mixed(const double2* __restrict__ psi, double2* __restrict__ rho, uint32_t n, double w) {
+    const uint64_t dim = 1ull << n;
+    GRID_STRIDE(i, dim * dim) {
+        uint64_t r = i >> n, c = i & (dim - 1);
+        double2 a = cmul_x(make_double2(w, 0.0), psi[r]);
+        double2 b = psi[c];
+        rho[i] = cadd_x(rho[i], cmul_x(a, make_double2(b.x, -b.y)));
+    }
+}
+
+int launch_dm_mixed_accum(Ctx* ctx, const Reg* r, double w, DM* d) {
+    uint64_t tot = (uint64_t)1 << (2 * r->nbits);
+    k_dm_mixed<<<grid_for(tot, 256, ctx->num_sms), 256, 0, ctx->stream>>>((const double2*)r->d, (double2*)d->d,
+                                                                          r->nbits, w);
+    ctx->launches++;
+    YAO_CUDA(cudaGetLastError());
+    return YAO_OK;
+}
+
+// ------------------------------------------------------------- gate pass
+
+struct DMGate {
+    int32_t cls, k, nlocked, pad;
+    int8_t locked[32];
+    uint64_t roff[4], coff[4];
+    uint64_t rcmask, rcval, ccmask, ccval;
+    uint32_t ractive, cactive;
+    double2 mr[16], mc[16];
+};
+
+// apply a k<=2 gate (class CLS) along one axis of a 2^k x 2^k block v[a][b]
+template <int CLS, int K>
+__device__ __forceinline__ void axis_apply(double2 (&v)[1 << K][1 << K], const double2* m, uint32_t active, bool rows) {
+    constexpr int NL = 1 << K;
+#pragma unroll
+    for (int o = 0; o < NL; o++) {
+        double2 x[NL];
+#pragma unroll
+        for (int i = 0; i < NL; i++) x[i] = rows ? v[i][o] : v[o][i];
+        double2 y[NL];
+#pragma unroll
+        for (int i = 0; i < NL; i++) y[i] = x[i];
+        if (CLS == GC_X) {
+            y[0] = x[1];
+            y[1] = x[0];
+        } else if (CLS == GC_SWAP) {
+            y[1] = x[2];
+            y[2] = x[1];
+        } else if (CLS == GC_DIAG) {
+#pragma unroll
+            for (int i = 0; i < NL; i++)
+                if ((active >> i) & 1) y[i] = cmulassign_x(x[i], m[i]);
+        } else if (K == 1) {
+            y[0] = cadd_x(cmul_x(m[0], x[0]), cmul_x(m[1], x[1]));
+            y[1] = cadd_x(cmul_x(m[2], x[0]), cmul_x(m[3], x[1]));
+        } else {
+#pragma unroll
+            for (int i = 0; i < NL; i++) {
+                double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int j = 0; j < NL; j++) acc = cadd_x(acc, cmul_x(m[i * NL + j], x[j]));
+                y[i] = acc;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NL; i++) {
+            if (rows)
+                v[i][o] = y[i];
+            else
+                v[o][i] = y[i];
+        }
+    }
+}
+
+template <int CLS, int K>
+__global__ void __launch_bounds__(kDT) k_dm_gate(double2* __restrict__ rho, uint64_t ngroups, const DMGate op) {
+    constexpr int NL = 1 << K;
+    GRID_STRIDE(g, ngroups) {
+        uint64_t base = insert_zeros(g, op.locked, op.nlocked);
+        bool rok = (base & op.rcmask) == op.rcval, cok = (base & op.ccmask) == op.ccval;
+        if (!rok && !cok) continue;
+        double2 v[NL][NL];
+#pragma unroll
+        for (int a = 0; a < NL; a++)
+#pragma unroll
+            for (int b = 0; b < NL; b++) v[a][b] = rho[base + op.roff[a] + op.coff[b]];
+        if (rok) axis_apply<CLS, K>(v, op.mr, op.ractive, true);
+        if (cok) axis_apply<CLS, K>(v, op.mc, op.cactive, false);
+#pragma unroll
+        for (int a = 0; a < NL; a++)
+#pragma unroll
+            for (int b = 0; b < NL; b++) rho[base + op.roff[a] + op.coff[b]] = v[a][b];
+    }
+}
+
+static uint32_t active_mask(const LGate& g) {
+    uint32_t a = 0;
+    if (g.cls != GC_DIAG) return 0;
+    for (size_t i = 0; i < g.m.size(); i++)
+        if (!(g.m[i].re == 1.0 && g.m[i].im == 0.0)) a |= 1u << i;
+    return a;
+}
+
+static void offsets(const LGate& g, uint64_t* off) {
+    for (int l = 0; l < (1 << g.k); l++) {
+        uint64_t o = 0;
+        for (int i = 0; i < g.k; i++) o |= (uint64_t)((l >> i) & 1) << g.tb[i];
+        off[l] = o;
+    }
+}
+
+int launch_dm_gate(Ctx* ctx, DM* d, const LGate& row, const LGate& col) {
+    uint32_t nb = 2 * d->nbits;
+    if (row.k > 2 || row.cls != col.cls) {
+        int s = launch_gate(ctx, d->d, YAO_C128, nb, row);
+        if (s) return s;
+        return launch_gate(ctx, d->d, YAO_C128, nb, col);
+    }
+    DMGate op;
+    memset(&op, 0, sizeof(op));
+    op.cls = row.cls;
+    op.k = row.k;
+    std::vector<int> pos;
+    for (int i = 0; i < row.k; i++) pos.push_back(row.tb[i]);
+    for (int i = 0; i < col.k; i++) pos.push_back(col.tb[i]);
+    std::sort(pos.begin(), pos.end());
+    op.nlocked = (int)pos.size();
+    for (size_t i = 0; i < pos.size(); i++) op.locked[i] = (int8_t)pos[i];
+    offsets(row, op.roff);
+    offsets(col, op.coff);
+    op.rcmask = row.cmask();
+    op.rcval = row.cval();
+    op.ccmask = col.cmask();
+    op.ccval = col.cval();
+    op.ractive = active_mask(row);
+    op.cactive = active_mask(col);
+    for (size_t i = 0; i < row.m.size() && i < 16; i++) op.mr[i] = make_double2(row.m[i].re, row.m[i].im);
+    for (size_t i = 0; i < col.m.size() && i < 16; i++) op.mc[i] = make_double2(col.m[i].re, col.m[i].im);
+    if (op.cls == GC_DIAG && op.ractive == 0 && op.cactive == 0) return YAO_OK;
+    uint64_t ngroups = (uint64_t)1 << (nb - op.nlocked);
+    unsigned grid = grid_for(ngroups, kDT, ctx->num_sms);
+    cudaStream_t s = ctx->stream;
+    ProfScope prof(ctx, "dm_gate", (double)ngroups * (double)(1 << (2 * op.k)) * 32.0);
+    switch (op.cls * 4 + op.k) {
+    case GC_X * 4 + 1: k_dm_gate<GC_X, 1><<<grid, kDT, 0, s>>>((double2*)d->d, ngroups, op); break;
+    case GC_SWAP * 4 + 2: k_dm_gate<GC_SWAP, 2><<<grid, kDT, 0, s>>>((double2*)d->d, ngroups, op); break;
+    case GC_DIAG * 4 + 1: k_dm_gate<GC_DIAG, 1><<<grid, kDT, 0, s>>>((double2*)d->d, ngroups, op); break;
+    case GC_DIAG * 4 + 2: k_dm_gate<GC_DIAG, 2><<<grid, kDT, 0, s>>>((double2*)d->d, ngroups, op); break;
+    case GC_DENSE * 4 + 1: k_dm_gate<GC_DENSE, 1><<<grid, kDT, 0, s>>>((double2*)d->d, ngroups, op); break;
+    case GC_DENSE * 4 + 2: k_dm_gate<GC_DENSE, 2><<<grid, kDT, 0, s>>>((double2*)d->d, ngroups, op); break;
+    default: return fail(YAO_ERR_INVALID_ARGUMENT, "unsupported density-matrix gate class");
+    }
+    ctx->launches++;
+    YAO_CUDA(cudaGetLastError());
+    return YAO_OK;
+}
+
+// ---------------------------------------------------------- channel pass
+
+constexpr int kMaxKraus = 16;
+constexpr int kDCT = 128;  // channel kernel block size
+struct DMChan {
+    int32_t k, nk, nlocked, pad;
+    int8_t locked[32];
+    uint64_t roff[4], coff[4];
+    int32_t cls[kMaxKraus];       // GC_DIAG or GC_DENSE per Kraus operator
+    uint32_t active[kMaxKraus];
+};
+
+// The untouched original group is kept in shared memory (one column per
+// thread), the branch and the accumulator in registers.
+template <int K>
+__global__ void __launch_bounds__(kDCT) k_dm_channel(double2* __restrict__ rho, uint64_t ngroups, const DMChan op,
+                                                    const double2* __restrict__ kr, const double2* __restrict__ kc) {
+    constexpr int NL = 1 << K, MS = NL * NL;
+    __shared__ double2 smr[kMaxKraus * MS], smc[kMaxKraus * MS];
+    __shared__ double2 sorig[MS * kDCT];
+    for (int i = threadIdx.x; i < op.nk * MS; i += blockDim.x) {
+        smr[i] = kr[i];
+        smc[i] = kc[i];
+    }
+    __syncthreads();
+    double2* orig = sorig + threadIdx.x;  // orig[(a*NL+b) * kDCT]
+    GRID_STRIDE(g, ngroups) {
+        uint64_t base = insert_zeros(g, op.locked, op.nlocked);
+        double2 acc[NL][NL], br[NL][NL];
+#pragma unroll
+        for (int a = 0; a < NL; a++)
+#pragma unroll
+            for (int b = 0; b < NL; b++) {
+                orig[(a * NL + b) * kDCT] = rho[base + op.roff[a] + op.coff[b]];
+                acc[a][b] = make_double2(0.0, 0.0);
+            }
+        for (int q = 0; q < op.nk; q++) {
+#pragma unroll
+            for (int a = 0; a < NL; a++)
+#pragma unroll
+                for (int b = 0; b < NL; b++) br[a][b] = orig[(a * NL + b) * kDCT];
+            if (op.cls[q] == GC_DIAG) {
+                axis_apply<GC_DIAG, K>(br, smr + q * MS, op.active[q], true);
+                axis_apply<GC_DIAG, K>(br, smc + q * MS, op.active[q], false);
+            } else {
+                axis_apply<GC_DENSE, K>(br, smr + q * MS, 0, true);
+                axis_apply<GC_DENSE, K>(br, smc + q * MS, 0, false);
+            }
+#pragma unroll
+            for (int a = 0; a < NL; a++)
+#pragma unroll
+                for (int b = 0; b < NL; b++) acc[a][b] = cadd_x(acc[a][b], br[a][b]);
+        }
+#pragma unroll
+        for (int a = 0; a < NL; a++)
+#pragma unroll
+            for (int b = 0; b < NL; b++) rho[base + op.roff[a] + op.coff[b]] = acc[a][b];
+    }
+}
+
+int launch_dm_channel(Ctx* ctx, DM* d, const std::vector<LGate>& rows, const std::vector<LGate>& cols,
+                      const std::vector<uint32_t>& row_bits, const std::vector<uint32_t>& col_bits) {
+    const int k = rows.empty() ? 0 : rows[0].k;
+    const int nk = (int)rows.size();
+    if (k < 1 || k > 2 || nk > kMaxKraus) return fail(YAO_ERR_UNSUPPORTED, "channel pass supports 1- and 2-qubit channels with <= 16 Kraus operators");
+    DMChan op;
+    memset(&op, 0, sizeof(op));
+    op.k = k;
+    op.nk = nk;
+    std::vector<int> pos;
+    for (int i = 0; i < k; i++) pos.push_back(rows[0].tb[i]);
+    for (int i = 0; i < k; i++) pos.push_back(cols[0].tb[i]);
+    std::sort(pos.begin(), pos.end());
+    op.nlocked = (int)pos.size();
+    for (size_t i = 0; i < pos.size(); i++) op.locked[i] = (int8_t)pos[i];
+    offsets(rows[0], op.roff);
+    offsets(cols[0], op.coff);
+    const int NL = 1 << k, MS = NL * NL;
+    std::vector<double2> hr((size_t)nk * MS), hc((size_t)nk * MS);
+    for (int q = 0; q < nk; q++) {
+        // the 2q lowering sorts each Kraus operator's bits identically
+        op.cls[q] = rows[q].cls;
+        op.active[q] = active_mask(rows[q]) | active_mask(cols[q]);
+        for (size_t i = 0; i < rows[q].m.size(); i++) hr[(size_t)q * MS + i] = make_double2(rows[q].m[i].re, rows[q].m[i].im);
+        for (size_t i = 0; i < cols[q].m.size(); i++) hc[(size_t)q * MS + i] = make_double2(cols[q].m[i].re, cols[q].m[i].im);
+        if (rows[q].cls == GC_DIAG) op.active[q] = (1u << NL) - 1;  // multiply every entry, as the CPU path does
+    }
+    void* buf = nullptr;
+    size_t bytes = sizeof(double2) * (size_t)nk * MS;
+    YAO_CUDA(cudaMallocAsync(&buf, 2 * bytes, ctx->stream));
+    YAO_CUDA(cudaMemcpyAsync(buf, hr.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
+    YAO_CUDA(cudaMemcpyAsync((char*)buf + bytes, hc.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
+    uint64_t ngroups = (uint64_t)1 << (2 * d->nbits - op.nlocked);
+    unsigned grid = grid_for(ngroups, kDT, ctx->num_sms);
+    ProfScope prof(ctx, "dm_channel", (double)ngroups * (double)(1 << (2 * k)) * 32.0);
+    if (k == 1)
+        k_dm_channel<1><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op, (const double2*)buf,
+                                                        (const double2*)((char*)buf + bytes));
+    else
+        k_dm_channel<2><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op, (const double2*)buf,
+                                                        (const double2*)((char*)buf + bytes));
+    ctx->launches++;
+    YAO_CUDA(cudaGetLastError());
+    YAO_CUDA(cudaFreeAsync(buf, ctx->stream));
+    (void)row_bits;
+    (void)col_bits;
+    return YAO_OK;
+}
+
+// ------------------------------------------------------------ reductions
+
+static int dm_finish(Ctx* ctx, double* part, int nb, int nv, double* host_out);
+
+__global__ void k_dm_final(const double* __restrict__ partial, int nblocks, int nv, double* __restrict__ out) {
+    __shared__ double sm[kDT / 32];
+    for (int v = 0; v < nv; v++) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partial[(size_t)b * nv + v];
+        s = warp_sum(s);
+        if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sm[w];
+            out[v] = t;
+        }
+        __syncthreads();
+    }
+}
+
+static int dm_finish(Ctx* ctx, double* part, int nb, int nv, double* host_out) {
+    double* dout = part + (size_t)nb * nv;
+    k_dm_final<<<1, kDT, 0, ctx->stream>>>(part, nb, nv, dout);
+    ctx->launches++;
+    YAO_CUDA(cudaGetLastError());
+    if (ctx->ensure_host_pinned(sizeof(double) * nv)) return YAO_ERR_OUT_OF_MEMORY;
+    YAO_CUDA(cudaMemcpyAsync(ctx->host_pinned, dout, sizeof(double) * nv, cudaMemcpyDeviceToHost, ctx->stream));
+    YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+    memcpy(host_out, ctx->host_pinned, sizeof(double) * nv);
+    return YAO_OK;
+}
+
+static int dm_scratch(Ctx* ctx, int nb, int nv, double** part) {
+    if (ctx->ensure_scratch(sizeof(double) * ((size_t)nb * nv + nv))) return YAO_ERR_OUT_OF_MEMORY;
+    *part = (double*)ctx->scratch;
+    return YAO_OK;
+}
+
+// trace (src/density_matrix.rs:63-67)
+__global__ void __launch_bounds__(kDT) k_dm_trace(const double2* __restrict__ rho, uint64_t dim, double* partial) {
+    __shared__ double sm[2 * kDT / 32];
+    double acc[2] = {0.0, 0.0};
+    GRID_STRIDE(i, dim) {
+        double2 v = rho[i * dim + i];
+        acc[0] += v.x;
+        acc[1] += v.y;
+    }
+    block_sum_write(acc, 2, sm, partial + 2 * blockIdx.x);
+}
+
+int reduce_dm_trace(Ctx* ctx, const DM* d, Cx* out) {
+    uint64_t dim = (uint64_t)1 << d->nbits;
+    int nb = (int)grid_for(dim, kDT, ctx->num_sms, 2);
+    double* part;
+    if (dm_scratch(ctx, nb, 2, &part)) return YAO_ERR_OUT_OF_MEMORY;
+    k_dm_trace<<<nb, kDT, 0, ctx->stream>>>((const double2*)d->d, dim, part);
+    ctx->launches++;
+    YAO_CUDA(cudaGetLastError());
+    double r[2];
+    int s = dm_finish(ctx, part, nb, 2, r);
+    *out = Cx{r[0], r[1]};
+    return s;
+}
+
+// purity = Re sum_{r,i} rho[r,i] rho[i,r] (src/density_matrix.rs:69-78).
+// A block takes a 32x32 tile pair (R, C), R <= C, reading rho[R, C] and
+// rho[C, R] with coalesced rows; an off-diagonal pair counts twice.
+__global__ void __launch_bounds__(kDT) k_dm_purity(const double2* __restrict__ rho, uint64_t dim, uint64_t nt,
+                                                  uint64_t npairs, double* partial) {
+    __shared__ double2 A[32][33], B[32][33];
+    __shared__ double sm[kDT / 32];
+    double acc = 0.0;
+    for (uint64_t p = blockIdx.x; p < npairs; p += gridDim.x) {
+        // p -> (R, C) with R <= C, row-major over the upper triangle
+        uint64_t R = (uint64_t)((2.0 * nt + 1.0 - sqrt((2.0 * nt + 1.0) * (2.0 * nt + 1.0) - 8.0 * (double)p)) / 2.0);
+        while (R > 0 && R * nt - R * (R - 1) / 2 > p) R--;
+        while ((R + 1) * nt - (R + 1) * R / 2 <= p) R++;
+        uint64_t C = R + (p - (R * nt - R * (R - 1) / 2));
+        const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+        for (int r = ty; r < 32; r += kDT / 32) {
+            A[r][tx] = rho[(R * 32 + r) * dim + C * 32 + tx];
+            B[r][tx] = rho[(C * 32 + r) * dim + R * 32 + tx];
+        }
+        __syncthreads();
+        double w = (R == C) ? 1.0 : 2.0;
+        for (int r = ty; r < 32; r += kDT / 32) {
+            double2 a = A[r][tx], b = B[tx][r];
+            acc += w * (a.x * b.x - a.y * b.y);
+        }
+        __syncthreads();
+    }
+    block_sum_write(&acc, 1, sm, partial + blockIdx.x);
+}
+
+__global__ void __launch_bounds__(kDT) k_dm_purity_small(const double2* __restrict__ rho, uint64_t dim,
+                                                        double* partial) {
+    __shared__ double sm[kDT / 32];
+    double acc = 0.0;
+    GRID_STRIDE(i, dim * dim) {
+        uint64_t r = i / dim, c = i % dim;
+        double2 a = rho[r * dim + c], b = rho[c * dim + r];
+        acc += a.x * b.x - a.y * b.y;
+    }
+    block_sum_write(&acc, 1, sm, partial + blockIdx.x);
+}
+
+int reduce_dm_purity(Ctx* ctx, const DM* d, double* out) {
+    uint64_t dim = (uint64_t)1 << d->nbits;
+    int nb;
+    double* part;
+    if (dim < 64) {
+        nb = 1;
+        if (dm_scratch(ctx, nb, 1, &part)) return YAO_ERR_OUT_OF_MEMORY;
+        k_dm_purity_small<<<1, kDT, 0, ctx->stream>>>((const double2*)d->d, dim, part);
+    } else {
+        uint64_t nt = dim / 32, npairs = nt * (nt + 1) / 2;
+        nb = (int)std::min<uint64_t>(npairs, (uint64_t)ctx->num_sms * 8);
+        if (dm_scratch(ctx, nb, 1, &part)) return YAO_ERR_OUT_OF_MEMORY;
+        k_dm_purity<<<nb, kDT, 0, ctx->stream>>>((const double2*)d->d, dim, nt, npairs, part);
+    }
+    ctx->launches++;
+    YAO_CUDA(cudaGetLastError());
+    return dm_finish(ctx, part, nb, 1, out);
+}
+
+// Tr(O rho) for monomial terms (src/expect.rs:44-72): for each row r the
+// only non-zero entry of O is at column c = r ^ xmask with value phase(r),
+// and yao-rs reads rho[c * dim + r].
+struct DMTerm {
+    uint64_t xmask, d1, d2, need1, need0;
+    int32_t base, zero;
+};
+
+__global__ void __launch_bounds__(kDT) k_dm_expect(const double2* __restrict__ rho, uint64_t dim, const DMTerm t,
+                                                  double* partial) {
+    __shared__ double sm[2 * kDT / 32];
+    double acc[2] = {0.0, 0.0};
+    if (!t.zero) {
+        GRID_STRIDE(r, dim) {
+            if ((r & t.need1) != t.need1 || (r & t.need0) != 0) continue;
+            int q = (t.base + __popcll(r & t.d1) + 2 * __popcll(r & t.d2)) & 3;
+            uint64_t c = r ^ t.xmask;
+            double2 v = rho[c * dim + r];
+            double2 u;
+            switch (q) {
+            case 0: u = v; break;
+            case 1: u = make_double2(-v.y, v.x); break;
+            case 2: u = make_double2(-v.x, -v.y); break;
+            default: u = make_double2(v.y, -v.x); break;
+            }
+            acc[0] += u.x;
+            acc[1] += u.y;
+        }
+    }
+    block_sum_write(acc, 2, sm, partial + 2 * blockIdx.x);
+}
+
+int reduce_dm_expect(Ctx* ctx, const DM* d, const std::vector<MonoTerm>& terms, std::vector<Cx>& values) {
+    uint64_t dim = (uint64_t)1 << d->nbits;
+    values.assign(terms.size(), Cx{0, 0});
+    for (size_t i = 0; i < terms.size(); i++) {
+        DMTerm t;
+        t.xmask = terms[i].xmask;
+        t.d1 = terms[i].d1mask;
+        t.d2 = terms[i].d2mask;
+        t.need1 = terms[i].need1;
+        t.need0 = terms[i].need0;
+        t.base = terms[i].base;
+        t.zero = terms[i].zero;
+        int nb = (int)grid_for(dim, kDT, ctx->num_sms, 2);
+        double* part;
+        if (dm_scratch(ctx, nb, 2, &part)) return YAO_ERR_OUT_OF_MEMORY;
+        k_dm_expect<<<nb, kDT, 0, ctx->stream>>>((const double2*)d->d, dim, t, part);
+        ctx->launches++;
+        YAO_CUDA(cudaGetLastError());
+        double r[2];
+        int s = dm_finish(ctx, part, nb, 2, r);
+        if (s) return s;
+        values[i] = Cx{r[0], r[1]};
+    }
+    return YAO_OK;
+}
+
+// probabilities of a density matrix: diagonal, re.max(0) (src/measure.rs:50-57, 106-122)
+__global__ void k_dm_diag_probs(const double2* __restrict__ rho, uint64_t dim, double* out) {
+    GRID_STRIDE(i, dim) out[i] = fmax(rho[i * dim + i].x, 0.0);
+}
+
+int reduce_dm_marginal(Ctx* ctx, const DM* d, const uint32_t* bits, int32_t nl, double* host_out) {
+    uint64_t dim = (uint64_t)1 << d->nbits;
+    if (ctx->ensure_scratch(sizeof(double) * dim)) return YAO_ERR_OUT_OF_MEMORY;
+    double* dp = (double*)ctx->scratch;
+    k_dm_diag_probs<<<grid_for(dim, 256, ctx->num_sms), 256, 0, ctx->stream>>>((const double2*)d->d, dim, dp);
+    ctx->launches++;
+    YAO_CUDA(cudaGetLastError());
+    std::vector<double> diag(dim);
+    YAO_CUDA(cudaMemcpyAsync(diag.data(), dp, sizeof(double) * dim, cudaMemcpyDeviceToHost, ctx->stream));
+    YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (nl < 0) {
+        memcpy(host_out, diag.data(), sizeof(double) * dim);
+        return YAO_OK;
+    }
+    // the diagonal has only 2^n entries: bin it on the host in basis order,
+    // exactly as the CPU loop does
+    uint64_t nout = (uint64_t)1 << nl;
+    for (uint64_t o = 0; o < nout; o++) host_out[o] = 0.0;
+    for (uint64_t b = 0; b < dim; b++) {
+        uint64_t idx = 0;
+        for (int32_t i = 0; i < nl; i++) idx |= ((b >> bits[i]) & 1) << (nl - 1 - i);
+        host_out[idx] += diag[b];
+    }
+    return YAO_OK;
+}
+
+// partial_tr (src/density_matrix.rs:80-112; loc = bit position, LSB first).
+// One thread per reduced entry sums its 2^nt contributions in increasing
+// (row, col) order, which is the CPU loop's order: bit-identical.
+struct PTSpec {
+    int32_t nk, nt;
+    int8_t kept[64];
+    int8_t traced[64];
+};
+
+__global__ void k_dm_partial_tr(const double2* __restrict__ rho, double2* __restrict__ out, uint32_t n,
+                                const PTSpec sp) {
+    const uint64_t dr = 1ull << sp.nk, dim = 1ull << n, ntr = 1ull << sp.nt;
+    GRID_STRIDE(o, dr * dr) {
+        uint64_t rr = o / dr, rc = o % dr;
+        uint64_t row0 = 0, col0 = 0;
+        for (int k = 0; k < sp.nk; k++) {
+            row0 |= ((rr >> k) & 1) << sp.kept[k];
+            col0 |= ((rc >> k) & 1) << sp.kept[k];
+        }
+        double2 acc = make_double2(0.0, 0.0);
+        for (uint64_t t = 0; t < ntr; t++) {
+            uint64_t tb = 0;
+            for (int j = 0; j < sp.nt; j++) tb |= ((t >> j) & 1) << sp.traced[j];
+            acc = cadd_x(acc, rho[(row0 | tb) * dim + (col0 | tb)]);
+        }
+        out[o] = acc;
+    }
+}
+
+int launch_dm_partial_tr(Ctx* ctx, const DM* d, const uint32_t* traced, uint32_t nt, DM* out) {
+    PTSpec sp;
+    memset(&sp, 0, sizeof(sp));
+    std::vector<int> tr(traced, traced + nt);
+    std::sort(tr.begin(), tr.end());
+    tr.erase(std::unique(tr.begin(), tr.end()), tr.end());
+    sp.nt = (int)tr.size();
+    for (int j = 0; j < sp.nt; j++) sp.traced[j] = (int8_t)tr[j];
+    int nk = 0;
+    for (uint32_t loc = 0; loc < d->nbits; loc++)
+        if (!std::binary_search(tr.begin(), tr.end(), (int)loc)) sp.kept[nk++] = (int8_t)loc;
+    sp.nk = nk;
+    uint64_t tot = (uint64_t)1 << (2 * nk);
+    k_dm_partial_tr<<<grid_for(tot, 256, ctx->num_sms), 256, 0, ctx->stream>>>((const double2*)d->d, (double2*)out->d,
+                                                                               d->nbits, sp);
+    ctx->launches++;
+    YAO_CUDA(cudaGetLastError());
+    return YAO_OK;
+}
+
+}  // namespace yao

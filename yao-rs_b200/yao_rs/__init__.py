@@ -1,0 +1,27 @@
+"""yao_rs — Python mirror of the yao-rs crate API (src/lib.rs:25-48) over the
+B200 library libyao_gpu.so.
+
+Circuits, gates, noise channels and operators are host values; registers
+and density matrices live in GPU memory.  Every compute call goes through
+the C ABI of include/yao_gpu.h; there is no CPU fallback.
+"""
+from . import _abi
+from ._abi import (C64, C128, MODE_FUSED, MODE_PLAIN, MODE_TILED, CircuitError, YaoError, context,
+                   launch_count)
+from .circuit import (Circuit, PositionedAnnotation, PositionedChannel, PositionedGate, channel, control,
+                      elements_array, label, put)
+from .gate import Gate
+from .noise import NoiseChannel
+from .operator import Op, OperatorPolynomial, OperatorString, op_matrix
+from .ops import (MeasureResult, PostProcess, apply, apply_inplace, batch_apply, expect_arrayreg, expect_dm,
+                  expect_grad, measure_with_postprocess, probs)
+from .register import ArrayReg, DensityMatrix, Register, density_matrix_from_reg
+
+__all__ = [
+    "ArrayReg", "C64", "C128", "Circuit", "CircuitError", "DensityMatrix", "Gate", "MODE_FUSED", "MODE_PLAIN",
+    "MODE_TILED", "MeasureResult", "NoiseChannel", "Op", "OperatorPolynomial", "OperatorString",
+    "PositionedAnnotation", "PositionedChannel", "PositionedGate", "PostProcess", "Register", "YaoError",
+    "apply", "apply_inplace", "batch_apply", "channel", "context", "control", "density_matrix_from_reg",
+    "elements_array", "expect_arrayreg", "expect_dm", "expect_grad", "label", "launch_count",
+    "measure_with_postprocess", "op_matrix", "probs", "put",
+]
