@@ -248,10 +248,18 @@ static const std::vector<LGate>& lowered(Circuit* c) {
     return c->lowered.emplace(c->nbits, std::move(prog)).first->second;
 }
 
+// The kernels take at most kMaxTargets targets per gate (a 64 x 64 matrix).
+static int check_widths(const Circuit* c) {
+    for (const Element& el : c->elems)
+        if (el.kind == YAO_ELEM_GATE && el.g.targets.size() > (size_t)kMaxTargets)
+            return fail(YAO_ERR_UNSUPPORTED, "gates on more than 6 target qubits are not supported");
+    return YAO_OK;
+}
+
 static int check_apply(const Circuit* c, const Reg* r) {
     if (!c->qubit_only) return fail(YAO_ERR_QUBIT_ONLY, "ArrayReg only supports qubit-only circuits");
     if (c->nbits != r->nbits) return fail(YAO_ERR_NBITS_MISMATCH, "Register and circuit qubit count mismatch");
-    return YAO_OK;
+    return check_widths(c);
 }
 
 static int alloc_reg(Ctx* ctx, uint32_t nbits, int32_t prec, Reg** out) {
@@ -889,6 +897,8 @@ int yao_dm_apply(yao_dm* d, const yao_circuit* cc) {
     const Circuit* c = cc;
     if (!c->qubit_only) return fail(YAO_ERR_QUBIT_ONLY, "DensityMatrix only supports qubit-only circuits");
     if (c->nbits != d->nbits) return fail(YAO_ERR_NBITS_MISMATCH, "Register and circuit qubit count mismatch");
+    int sw = check_widths(c);
+    if (sw) return sw;
     YAO_CUDA(cudaSetDevice(d->ctx->device));
     const uint32_t n = d->nbits, nb = 2 * n;
     for (const Element& el : c->elems) {

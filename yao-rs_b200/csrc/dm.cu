@@ -391,9 +391,12 @@ __global__ void __launch_bounds__(kDT) k_dm_purity(const double2* __restrict__ r
     double acc = 0.0;
     for (uint64_t p = blockIdx.x; p < npairs; p += gridDim.x) {
         // p -> (R, C) with R <= C, row-major over the upper triangle
-        uint64_t R = (uint64_t)((2.0 * nt + 1.0 - sqrt((2.0 * nt + 1.0) * (2.0 * nt + 1.0) - 8.0 * (double)p)) / 2.0);
+        double est = (2.0 * nt + 1.0 - sqrt((2.0 * nt + 1.0) * (2.0 * nt + 1.0) - 8.0 * (double)p)) / 2.0;
+        uint64_t R = est <= 0.0 ? 0 : (uint64_t)est;
+        if (R > nt - 1) R = nt - 1;
+        // row R starts at pair R*nt - R(R-1)/2; fix a rounding error of the estimate
         while (R > 0 && R * nt - R * (R - 1) / 2 > p) R--;
-        while ((R + 1) * nt - (R + 1) * R / 2 <= p) R++;
+        while (R + 1 < nt && (R + 1) * nt - (R + 1) * R / 2 <= p) R++;
         uint64_t C = R + (p - (R * nt - R * (R - 1) / 2));
         const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
         for (int r = ty; r < 32; r += kDT / 32) {

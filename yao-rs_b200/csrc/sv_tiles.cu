@@ -405,6 +405,8 @@ static void host_apply(const LGate& g, const std::vector<int>& local_of_bit, std
 struct Block {
     std::vector<int> bits;  // ascending global bit positions
     std::vector<Cx> m;      // 2^|bits| x 2^|bits|
+    bool passthrough = false;  // a gate on more than kMaxTargets qubits, kept as is
+    LGate gate;
 };
 
 static void block_extend(Block& b, const std::vector<int>& add) {
@@ -459,7 +461,16 @@ static void fuse_blocks(const std::vector<LGate>& prog, uint32_t nbits, int k, s
         for (int c = 0; c < g.nc; c++) S.push_back(g.cb[c]);
         int B = -1;
         for (int b : S) B = std::max(B, last[b]);
-        if (B >= 0) {
+        if ((int)S.size() > kMaxTargets) {
+            // too wide to fuse (its block matrix would exceed 2^6 x 2^6)
+            Block pb;
+            pb.passthrough = true;
+            pb.gate = g;
+            blocks.push_back(pb);
+            for (int b : S) last[b] = (int)blocks.size() - 1;
+            continue;
+        }
+        if (B >= 0 && !blocks[B].passthrough) {
             std::set<int> u(blocks[B].bits.begin(), blocks[B].bits.end());
             for (int b : S) u.insert(b);
             if ((int)u.size() <= std::max<int>(k, (int)blocks[B].bits.size())) {
@@ -480,6 +491,10 @@ static void fuse_blocks(const std::vector<LGate>& prog, uint32_t nbits, int k, s
         for (int b : S) last[b] = (int)blocks.size() - 1;
     }
     for (const Block& b : blocks) {
+        if (b.passthrough) {
+            out.push_back(b.gate);
+            continue;
+        }
         LGate g;
         g.k = (int)b.bits.size();
         for (int i = 0; i < g.k; i++) g.tb[i] = b.bits[i];
