@@ -240,7 +240,11 @@ def main():
     ap.add_argument("--qubits", type=int, default=NQ)
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--profile-case", default=None, choices=["plain", "tiled", "fused64", "fused32", "vqe", "dm"],
+                    help="run one small case of a kernel family (for ncu captures) and exit")
     args = ap.parse_args()
+    if args.profile_case:
+        return profile_case(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -366,6 +370,43 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def profile_case(args):
+    """One layer of the layered circuit at --qubits (default 30; use 27 for a
+    2 GiB state, still larger than L2) in one execution form, or one VQE
+    gradient (n=20), or one noisy density-matrix layer (n=12); for ncu."""
+    import yao_rs as Y
+    from yao_rs import _abi as A
+
+    n = args.qubits
+    if args.profile_case == "vqe":
+        nv = 20
+        rng = np.random.default_rng(1)
+        c = vqe_circuit(Y, nv, 2, rng.uniform(-3, 3, size=4 * nv))
+        Y.expect_grad(tfim(Y, nv), c, Y.ArrayReg.zero_state(nv))
+    elif args.profile_case == "dm":
+        nd = 12
+        els = []
+        for q in range(nd):
+            els.append(Y.put([q], Y.Gate.Ry(0.3 + q)))
+            els.append(Y.channel([q], Y.NoiseChannel.Depolarizing(1, 1e-3)))
+        for q in range(0, nd - 1, 2):
+            els.append(Y.control([q], [q + 1], Y.Gate.Z))
+            els.append(Y.channel([q, q + 1], Y.NoiseChannel.Depolarizing(2, 1e-3)))
+        for q in range(nd):
+            els.append(Y.channel([q], Y.NoiseChannel.AmplitudeDamping(1e-3, 0.0)))
+        d = Y.DensityMatrix.zero_state(nd)
+        d.apply(Y.Circuit.qubits(nd, els))
+        d.purity()
+    else:
+        mode, prec, k = {"plain": (Y.MODE_PLAIN, Y.C128, 0), "tiled": (Y.MODE_TILED, Y.C128, 0),
+                         "fused64": (Y.MODE_FUSED, Y.C128, 5), "fused32": (Y.MODE_FUSED, Y.C64, 5)}[args.profile_case]
+        c = Y.Circuit.qubits(n, layer_elements(Y, n, 0))
+        r = Y.ArrayReg.zero_state(n, prec)
+        Y.apply_inplace(c, r, mode, k)
+    A.synchronize()
+    print(f"profile case {args.profile_case} done: {Y.launch_count()} launches")
 
 
 def run_extras(Y, A, torch, stream, circuits, n, dev):

@@ -328,42 +328,62 @@ int build_mono_terms(const yao_term* terms, size_t nterms, uint32_t nbits, bool 
                          [](const std::pair<uint32_t, int32_t>& a, const std::pair<uint32_t, int32_t>& b) {
                              return a.first < b.first;
                          });
-        // per-site 2x2 product in application order (later op on the left);
-        // each entry kept as (nonzero, quarter turns)
+        // Per-site 2x2 matrix, each entry kept as (non-zero?, quarter turns).
+        // Pure states (expect.rs:26-36) apply the ops of one site in order, a
+        // matrix product with the later op on the left; expect_opstring_dm
+        // (expect.rs:55-59) multiplies the ops' entries at the same
+        // (row bit, column bit), an elementwise product.
         MonoTerm mt;
         mt.coeff = Cx{tm.coeff_re, tm.coeff_im};
         size_t i = 0;
         while (i < ops.size()) {
             uint32_t site = ops[i].first;
-            // row r -> (column, zero?, quarter turns)
-            int col[2] = {0, 1}, nz[2] = {1, 1}, q[2] = {0, 0};
+            int nzm[2][2], qm[2][2];
+            bool first = true;
             for (; i < ops.size() && ops[i].first == site; i++) {
                 int op = ops[i].second;
-                // op matrix as row -> (col, nonzero, quarter)
-                int oc[2], onz[2], oq[2];
+                if (op == YAO_OP_I) continue;  // dropped by OperatorString::new
+                int onz[2][2] = {{0, 0}, {0, 0}}, oq[2][2] = {{0, 0}, {0, 0}};
                 switch (op) {
-                case YAO_OP_I: oc[0] = 0; oc[1] = 1; onz[0] = onz[1] = 1; oq[0] = oq[1] = 0; break;
-                case YAO_OP_X: oc[0] = 1; oc[1] = 0; onz[0] = onz[1] = 1; oq[0] = oq[1] = 0; break;
-                case YAO_OP_Y: oc[0] = 1; oc[1] = 0; onz[0] = onz[1] = 1; oq[0] = 3; oq[1] = 1; break;
-                case YAO_OP_Z: oc[0] = 0; oc[1] = 1; onz[0] = onz[1] = 1; oq[0] = 0; oq[1] = 2; break;
-                case YAO_OP_P0: oc[0] = 0; oc[1] = 1; onz[0] = 1; onz[1] = 0; oq[0] = oq[1] = 0; break;
-                case YAO_OP_P1: oc[0] = 0; oc[1] = 1; onz[0] = 0; onz[1] = 1; oq[0] = oq[1] = 0; break;
-                case YAO_OP_PU: oc[0] = 1; oc[1] = 0; onz[0] = 1; onz[1] = 0; oq[0] = oq[1] = 0; break;
-                default: oc[0] = 1; oc[1] = 0; onz[0] = 0; onz[1] = 1; oq[0] = oq[1] = 0; break;  // Pd
+                case YAO_OP_X: onz[0][1] = onz[1][0] = 1; break;
+                case YAO_OP_Y: onz[0][1] = onz[1][0] = 1; oq[0][1] = 3; oq[1][0] = 1; break;
+                case YAO_OP_Z: onz[0][0] = onz[1][1] = 1; oq[1][1] = 2; break;
+                case YAO_OP_P0: onz[0][0] = 1; break;
+                case YAO_OP_P1: onz[1][1] = 1; break;
+                case YAO_OP_PU: onz[0][1] = 1; break;
+                default: onz[1][0] = 1; break;  // Pd
                 }
-                // new = op * old: row r of new picks op's (r -> c1), then old's row c1
-                int ncol[2], nnz[2], nq[2];
-                for (int r = 0; r < 2; r++) {
-                    int c1 = oc[r];
-                    ncol[r] = col[c1];
-                    nnz[r] = onz[r] && nz[c1];
-                    nq[r] = (oq[r] + q[c1]) & 3;
+                if (first) {
+                    memcpy(nzm, onz, sizeof nzm);
+                    memcpy(qm, oq, sizeof qm);
+                    first = false;
+                } else if (msb_first) {
+                    // new = op * old; op has at most one non-zero per row
+                    int nn[2][2], nq[2][2];
+                    for (int r = 0; r < 2; r++)
+                        for (int c = 0; c < 2; c++) {
+                            int k = onz[r][0] ? 0 : 1;
+                            nn[r][c] = onz[r][k] && nzm[k][c];
+                            nq[r][c] = (oq[r][k] + qm[k][c]) & 3;
+                        }
+                    memcpy(nzm, nn, sizeof nzm);
+                    memcpy(qm, nq, sizeof qm);
+                } else {
+                    for (int r = 0; r < 2; r++)
+                        for (int c = 0; c < 2; c++) {
+                            nzm[r][c] = nzm[r][c] && onz[r][c];
+                            qm[r][c] = (qm[r][c] + oq[r][c]) & 3;
+                        }
                 }
-                for (int r = 0; r < 2; r++) {
-                    col[r] = ncol[r];
-                    nz[r] = nnz[r];
-                    q[r] = nq[r];
-                }
+            }
+            if (first) continue;  // only identities on this site
+            // row form: row r -> (column, non-zero?, quarter turns)
+            int col[2], nz[2], q[2];
+            for (int r = 0; r < 2; r++) {
+                int c = nzm[r][0] ? 0 : 1;
+                col[r] = c;
+                nz[r] = nzm[r][c];
+                q[r] = qm[r][c];
             }
             uint32_t bit = msb_first ? (nbits - 1 - site) : site;
             uint64_t bm = (uint64_t)1 << bit;
@@ -685,11 +705,13 @@ int adjoint_step(Ctx* ctx, Reg* psi, Reg* lambda, const LGate* gen, const std::v
 
 // ------------------------------------------------------- probabilities
 
+// |amp|^2 = re*re + im*im (norm_sqr), without FMA contraction: bit-identical
+// to the CPU path (src/measure.rs:40-42).
 template <typename V>
 __global__ void k_probs_full(const V* __restrict__ st, double* __restrict__ out, uint64_t n) {
     GRID_STRIDE(i, n) {
         double2 v = to_d2(st[i]);
-        out[i] = v.x * v.x + v.y * v.y;
+        out[i] = __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y));
     }
 }
 
