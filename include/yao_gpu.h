@@ -244,6 +244,18 @@ int yao_dm_partial_tr(const yao_dm* d, const uint32_t* traced_locs, uint32_t n, 
  * expect_dm keeps yao-rs's site convention of that function: site s is bit s
  * of the row/column index (least significant first). */
 int yao_expect_arrayreg(const yao_reg* r, const yao_term* terms, size_t nterms, double out[2]);
+/* The same value as yao_expect_arrayreg, computed without allocating any
+ * memory.  No yao-rs counterpart: it exists for callers that cannot allocate
+ * at call time -- an application whose memory pool already holds nearly all
+ * of the GPU's memory for its state vectors (a cudaMalloc would fail or make
+ * the pool give memory back), or one that must not stall the GPU (cudaFree
+ * synchronises the device).  The reduction scratch is a 131,200-byte
+ * file-scope device array that every GPU loading the library keeps until
+ * exit; its address is looked up on the first call on each device (make
+ * that first call before any stream capture).  Limits: at most 64 terms of
+ * at most 64 ops each, else YAO_ERR_INVALID_ARGUMENT.  All calls share the
+ * array: calls that overlap on the GPU race and must be serialised. */
+int yao_expect_arrayreg_noalloc(const yao_reg* r, const yao_term* terms, size_t nterms, double out[2]);
 int yao_expect_dm(const yao_dm* d, const yao_term* terms, size_t nterms, double out[2]);
 /* expect_grad (src/ad.rs:75-156): value = Re <psi|H|psi>, grad in
  * Circuit::parameters() order; ngrad must equal num_params. */

@@ -990,6 +990,13 @@ int yao_expect_arrayreg(const yao_reg* r, const yao_term* terms, size_t nterms, 
     return YAO_OK;
 }
 
+int yao_expect_arrayreg_noalloc(const yao_reg* r, const yao_term* terms, size_t nterms, double out[2]) {
+    CHECK_NULL(r);
+    CHECK_NULL(out);
+    YAO_CUDA(cudaSetDevice(r->ctx->device));
+    return expect_noalloc(r->ctx, r, terms, nterms, out);
+}
+
 int yao_expect_dm(const yao_dm* d, const yao_term* terms, size_t nterms, double out[2]) {
     CHECK_NULL(d);
     CHECK_NULL(out);

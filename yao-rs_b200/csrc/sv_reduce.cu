@@ -887,4 +887,177 @@ int launch_remove_gather_fixed(Ctx* ctx, const Reg* src, Reg* dst, const uint32_
     return YAO_OK;
 }
 
+// ============================================ expectation without allocation
+//
+// yao_expect_arrayreg_noalloc computes the same value as yao_expect_arrayreg
+// but allocates nothing: no cudaMalloc / cudaMallocHost / cudaFree and no
+// heap memory on the normal path.  Its reduction partials live in the
+// file-scope device array below (every GPU that loads the library holds it
+// until the process exits), the operator terms are converted into fixed-size
+// arrays on the stack, and the result is copied straight into the caller's
+// host memory.
+//
+// Limits: at most kNoAllocMaxTerms terms and kNoAllocMaxOps ops per term;
+// larger inputs are rejected with YAO_ERR_INVALID_ARGUMENT.  The register
+// size is not limited: a reduction uses at most kNoAllocBlocks blocks.
+//
+// All calls share the array.  Every call writes each partial it reads
+// before reading it, so nothing has to start at zero; but two calls that
+// overlap on the GPU (different streams or threads at the same time) race
+// on the array and must be serialised by the caller.
+
+constexpr int kNoAllocBlocks = 1024;
+constexpr int kNoAllocValues = 2 * kMaxGroupTerms;
+constexpr size_t kNoAllocDoubles = (size_t)kNoAllocBlocks * kNoAllocValues + kNoAllocValues;  // 131,200 bytes
+constexpr int kNoAllocMaxTerms = 64;
+constexpr int kNoAllocMaxOps = 64;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+// Device address of g_noalloc_scratch, looked up once per device with that
+// device current (host code cannot use the symbol itself as a pointer).
+static double* g_noalloc_ptr[kNoAllocMaxDevices];
+static cudaError_t g_noalloc_err[kNoAllocMaxDevices];
+static std::once_flag g_noalloc_once[kNoAllocMaxDevices];
+
+static int noalloc_scratch(int device, double** out) {
+    if (device < 0 || device >= kNoAllocMaxDevices) return fail(YAO_ERR_INVALID_ARGUMENT, "device index too large");
+    std::call_once(g_noalloc_once[device], [device]() {
+        cudaError_t e = cudaSetDevice(device);
+        if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&g_noalloc_ptr[device], g_noalloc_scratch);
+        g_noalloc_err[device] = e;
+    });
+    if (g_noalloc_err[device] != cudaSuccess) return cuda_fail(g_noalloc_err[device], "cudaGetSymbolAddress");
+    *out = g_noalloc_ptr[device];
+    return YAO_OK;
+}
+
+// One term to a Pauli monomial (the same rules as build_mono_terms, pure-state
+// site order), using only the caller's fixed arrays.
+static int noalloc_term(const yao_term& tm, uint32_t nbits, MonoTerm& mt) {
+    if (tm.nops > (uint32_t)kNoAllocMaxOps)
+        return fail(YAO_ERR_INVALID_ARGUMENT, "noalloc expectation: more than 64 ops in one term");
+    uint32_t sites[kNoAllocMaxOps];
+    int32_t ops[kNoAllocMaxOps];
+    uint32_t n = 0;
+    for (uint32_t i = 0; i < tm.nops; i++) {
+        if (tm.ops[i] < YAO_OP_I || tm.ops[i] > YAO_OP_PD) return fail(YAO_ERR_INVALID_ARGUMENT, "unknown Op");
+        if (tm.sites[i] >= nbits) return fail(YAO_ERR_INVALID_ARGUMENT, "operator site out of range");
+        if (tm.ops[i] == YAO_OP_I) continue;  // dropped by OperatorString::new
+        // stable insertion by site (OperatorString::new sorts by site)
+        uint32_t j = n++;
+        while (j > 0 && sites[j - 1] > tm.sites[i]) {
+            sites[j] = sites[j - 1];
+            ops[j] = ops[j - 1];
+            j--;
+        }
+        sites[j] = tm.sites[i];
+        ops[j] = tm.ops[i];
+    }
+    mt = MonoTerm();
+    mt.coeff = Cx{tm.coeff_re, tm.coeff_im};
+    uint32_t i = 0;
+    while (i < n) {
+        uint32_t site = sites[i];
+        int nzm[2][2] = {{1, 0}, {0, 1}}, qm[2][2] = {{0, 0}, {0, 0}};
+        for (; i < n && sites[i] == site; i++) {
+            int onz[2][2] = {{0, 0}, {0, 0}}, oq[2][2] = {{0, 0}, {0, 0}};
+            switch (ops[i]) {
+            case YAO_OP_X: onz[0][1] = onz[1][0] = 1; break;
+            case YAO_OP_Y: onz[0][1] = onz[1][0] = 1; oq[0][1] = 3; oq[1][0] = 1; break;
+            case YAO_OP_Z: onz[0][0] = onz[1][1] = 1; oq[1][1] = 2; break;
+            case YAO_OP_P0: onz[0][0] = 1; break;
+            case YAO_OP_P1: onz[1][1] = 1; break;
+            case YAO_OP_PU: onz[0][1] = 1; break;
+            default: onz[1][0] = 1; break;
+            }
+            int nn[2][2], nq[2][2];  // op * accumulated
+            for (int r = 0; r < 2; r++)
+                for (int c = 0; c < 2; c++) {
+                    int k = onz[r][0] ? 0 : 1;
+                    nn[r][c] = onz[r][k] && nzm[k][c];
+                    nq[r][c] = (oq[r][k] + qm[k][c]) & 3;
+                }
+            memcpy(nzm, nn, sizeof nzm);
+            memcpy(qm, nq, sizeof qm);
+        }
+        int col[2], nz[2], q[2];
+        for (int r = 0; r < 2; r++) {
+            int c = nzm[r][0] ? 0 : 1;
+            col[r] = c;
+            nz[r] = nzm[r][c];
+            q[r] = qm[r][c];
+        }
+        uint64_t bm = (uint64_t)1 << (nbits - 1 - site);
+        if (nz[0] ? (col[0] == 1) : (nz[1] && col[1] == 0)) mt.xmask |= bm;
+        if (!nz[0] && !nz[1]) mt.zero = 1;
+        if (!nz[0]) mt.need1 |= bm;
+        if (!nz[1]) mt.need0 |= bm;
+        mt.base = (mt.base + q[0]) & 3;
+        int diff = (q[1] - q[0]) & 3;
+        if (diff & 1) mt.d1mask |= bm;
+        if (diff & 2) mt.d2mask |= bm;
+    }
+    return YAO_OK;
+}
+
+int expect_noalloc(Ctx* ctx, const Reg* r, const yao_term* terms, size_t nterms, double* out) {
+    if (nterms > (size_t)kNoAllocMaxTerms)
+        return fail(YAO_ERR_INVALID_ARGUMENT, "noalloc expectation: more than 64 terms");
+    if (nterms && !terms) return fail(YAO_ERR_INVALID_ARGUMENT, "null terms");
+    double* scratch;
+    int s = noalloc_scratch(ctx->device, &scratch);
+    if (s) return s;
+    MonoTerm mt[kNoAllocMaxTerms];
+    for (size_t t = 0; t < nterms; t++) {
+        s = noalloc_term(terms[t], r->nbits, mt[t]);
+        if (s) return s;
+    }
+    Cx values[kNoAllocMaxTerms];
+    bool done[kNoAllocMaxTerms] = {false};
+    const uint64_t n = (uint64_t)1 << r->nbits;
+    for (size_t t0 = 0; t0 < nterms; t0++) {
+        if (done[t0]) continue;
+        MonoGroup grp;
+        memset(&grp, 0, sizeof(grp));
+        grp.xmask = mt[t0].xmask;
+        grp.hbit = grp.xmask ? 63 - __builtin_clzll(grp.xmask) : 0;
+        size_t idx[kMaxGroupTerms];
+        int cnt = 0;
+        for (size_t t = t0; t < nterms && cnt < kMaxGroupTerms; t++)
+            if (!done[t] && mt[t].xmask == grp.xmask) {
+                grp.t[cnt] = to_dev(mt[t]);
+                idx[cnt++] = t;
+                done[t] = true;
+            }
+        grp.nt = cnt;
+        const int nv = 2 * cnt;
+        const uint64_t nwork = grp.xmask ? n / 2 : n;
+        const int nb = std::min(reduce_blocks(ctx, nwork), kNoAllocBlocks);
+        if (r->precision == YAO_C128)
+            k_expect_group<double2><<<nb, kRT, 0, ctx->stream>>>((const double2*)r->d, nwork, grp, scratch);
+        else
+            k_expect_group<float2><<<nb, kRT, 0, ctx->stream>>>((const float2*)r->d, nwork, grp, scratch);
+        double* dres = scratch + (size_t)nb * nv;
+        k_final_sum<<<1, kRT, 0, ctx->stream>>>(scratch, nb, nv, dres);
+        ctx->launches += 2;
+        YAO_CUDA(cudaGetLastError());
+        double res[kNoAllocValues];
+        YAO_CUDA(cudaMemcpyAsync(res, dres, sizeof(double) * nv, cudaMemcpyDeviceToHost, ctx->stream));
+        YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (int q = 0; q < cnt; q++) values[idx[q]] = Cx{res[2 * q], res[2 * q + 1]};
+    }
+    // sum_t coeff_t * value_t in term order (src/expect.rs:7-11)
+    double re = 0.0, im = 0.0;
+    for (size_t t = 0; t < nterms; t++) {
+        Cx c = mt[t].coeff, v = values[t];
+        re += c.re * v.re - c.im * v.im;
+        im += c.re * v.im + c.im * v.re;
+    }
+    out[0] = re;
+    out[1] = im;
+    return YAO_OK;
+}
+
 }  // namespace yao

@@ -203,6 +203,8 @@ struct MonoTerm {
 int build_mono_terms(const yao_term* terms, size_t nterms, uint32_t nbits, bool msb_first,
                      std::vector<MonoTerm>& out);
 int expect_terms(Ctx* ctx, const Reg* r, const std::vector<MonoTerm>& terms, std::vector<Cx>& values);
+// The allocation-free expectation value (static device scratch), sv_reduce.cu.
+int expect_noalloc(Ctx* ctx, const Reg* r, const yao_term* terms, size_t nterms, double* out);
 int build_lambda(Ctx* ctx, const Reg* psi, const std::vector<MonoTerm>& terms, Reg* lambda);
 int adjoint_step(Ctx* ctx, Reg* psi, Reg* lambda, const LGate* gen, const std::vector<LGate>& dag,
                  Cx* dot_out);

@@ -138,6 +138,7 @@ SIGNATURES = {
     "yao_dm_purity": (C.c_int, [vp, dptr]),
     "yao_dm_partial_tr": (C.c_int, [vp, u32p, u32, pp]),
     "yao_expect_arrayreg": (C.c_int, [vp, C.POINTER(yao_term), sz, dptr]),
+    "yao_expect_arrayreg_noalloc": (C.c_int, [vp, C.POINTER(yao_term), sz, dptr]),
     "yao_expect_dm": (C.c_int, [vp, C.POINTER(yao_term), sz, dptr]),
     "yao_expect_grad": (C.c_int, [C.POINTER(yao_term), sz, vp, vp, dptr, dptr, sz]),
     "yao_probs": (C.c_int, [vp, u32p, i32, dptr]),
