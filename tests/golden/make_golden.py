@@ -67,6 +67,20 @@ def make_pysim(ref: Path, count: int = 40, seed: int = 20261203):
     (HERE / "pysim.json").write_text(json.dumps({"seed": seed, "cases": cases}, separators=(",", ":")))
 
 
+def copy_cli_examples(ref: Path):
+    """The documentation examples of yao-cli: circuit JSON files and the
+    `yao probs` / `yao expect` outputs yao-rs generated for them."""
+    base = ref / "docs" / "src" / "examples" / "generated"
+    cases = []
+    for res in sorted((base / "results").glob("*.json")):
+        stem = res.name.rsplit("-", 1)[0]
+        circ = base / "circuits" / f"{stem}.json"
+        if not circ.exists():
+            continue
+        cases.append({"name": stem, "circuit": json.loads(circ.read_text()), "result": json.loads(res.read_text())})
+    (HERE / "cli_examples.json").write_text(json.dumps({"cases": cases}, separators=(",", ":")))
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -74,4 +88,5 @@ if __name__ == "__main__":
     ref = Path(a.ref)
     copy_reference_data(ref)
     make_pysim(ref)
+    copy_cli_examples(ref)
     print("wrote", sorted(p.name for p in HERE.glob("*.json")))
