@@ -172,6 +172,20 @@ def cpu_baseline_sample(n, budget_s, layer=0):
     return b_total / t_total / 1e9, gates, t_total
 
 
+def max_over_ranks(torch, ms, world, device):
+    """The slowest rank's time (every rank calls this; one MAX all-reduce)."""
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gbps(bytes_per_rank, world, ms):
+    """Whole-job GB/s: every rank moved bytes_per_rank in at most ms."""
+    return world * bytes_per_rank / (ms / 1e3) / 1e9
+
+
 def host_ram_gb():
     try:
         for line in open("/proc/meminfo"):
@@ -240,7 +254,8 @@ def main():
     ap.add_argument("--qubits", type=int, default=NQ)
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
-    ap.add_argument("--profile-case", default=None, choices=["plain", "tiled", "fused64", "fused32", "vqe", "dm"],
+    ap.add_argument("--profile-case", default=None, choices=["plain", "tiled", "fused64", "fused32", "vqe", "dm", "batch",
+                                                             "vqe_batch"],
                     help="run one small case of a kernel family (for ncu captures) and exit")
     args = ap.parse_args()
     if args.profile_case:
@@ -297,23 +312,27 @@ def main():
     prof = A.profile_report(dev)
     A.profile(False, dev)
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev}")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms = max_over_ranks(torch, e0.elapsed_time(e1), world, f"cuda:{dev}")
     nbytes = sum(layer_bytes(n, i % LAYERS) for i in range(args.steps))
-    value = world * nbytes / (ms / 1e3) / 1e9
+    value = job_gbps(nbytes, world, ms)
     prof_bytes = sum(p["bytes"] for p in prof)
 
     # roofline of the dominant kernel (largest share of device time)
     peak, peak_kind = measured_peaks()
     top = max(prof, key=lambda p: p["ms"])
     achieved = top["bytes"] / (top["ms"] / 1e3) / 1e9
+    # DRAM traffic per launch of the dense 1-qubit kernel: ncu capture of
+    # `bench.py --profile-case plain --qubits 27` (dram__bytes_read.sum +
+    # dram__bytes_write.sum = 2.1475 + 2.0905 GB for 2^27 amplitudes), scaled
+    # by the amplitudes one launch processes here.
+    traffic = None
+    if top["kernel"] == "gate_dense1":
+        traffic = (2.1475e9 + 2.0905e9) * (1 << n) / (1 << 27)
     roofline = {"bound": "hbm", "kernel": top["kernel"], "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
                 "bytes_per_launch": top["bytes"] / top["launches"], "launches": top["launches"],
-                "avg_launch_ms": top["ms"] / top["launches"], "traffic": None,
+                "avg_launch_ms": top["ms"] / top["launches"], "traffic": traffic,
+                "traffic_source": "ncu capture at n=27 scaled by 2^(n-27)" if traffic else None,
                 "share": top["ms"] / sum(p["ms"] for p in prof)}
     kernels = [{"kernel": p["kernel"], "launches": p["launches"], "ms": round(p["ms"], 3),
                 "GBps": round(p["bytes"] / (p["ms"] / 1e3) / 1e9, 1)} for p in prof]
@@ -331,13 +350,9 @@ def main():
     A.check(A.lib().yao_reg_to_host(reg.handle, A.C.c_void_p(hp)))
     f1.record(stream)
     f1.synchronize()
-    e2e_ms = f0.elapsed_time(f1)
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{dev}")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(torch, f0.elapsed_time(f1), world, f"cuda:{dev}")
     state_bytes = 16 * (1 << n)
-    e2e = {"value": world * nbytes / (e2e_ms / 1e3) / 1e9, "unit": "GB/s",
+    e2e = {"value": job_gbps(nbytes, world, e2e_ms), "unit": "GB/s",
            "h2d_bytes_per_step": state_bytes / args.steps, "d2h_bytes_per_step": state_bytes / args.steps,
            "note": "one upload of the input state and one download of the final state per K steps"}
     del host
@@ -385,6 +400,15 @@ def profile_case(args):
         rng = np.random.default_rng(1)
         c = vqe_circuit(Y, nv, 2, rng.uniform(-3, 3, size=4 * nv))
         Y.expect_grad(tfim(Y, nv), c, Y.ArrayReg.zero_state(nv))
+    elif args.profile_case == "batch":
+        draws, cs = uneven_batch(Y, count=256)
+        regs = [Y.ArrayReg.zero_state(nq, Y.C64) for nq, _ in draws]
+        Y.batch_apply(cs, regs, Y.MODE_FUSED, 4)
+    elif args.profile_case == "vqe_batch":
+        rng = np.random.default_rng(16)
+        sets = rng.uniform(-math.pi, math.pi, size=(512, 2 * 16 * 2))
+        c = vqe_circuit(Y, 16, 2, sets[0])
+        Y.expect_grad_batch(tfim(Y, 16), c, sets, Y.ArrayReg.zero_state(16))
     elif args.profile_case == "dm":
         nd = 12
         els = []
@@ -423,20 +447,22 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
         b.synchronize()
         return a.elapsed_time(b) / 1e3
 
+    # the 40 layers as one Circuit: tiles and fused blocks span layers
+    whole = Y.Circuit.qubits(n, [el for l in range(LAYERS) for el in layer_elements(Y, n, l)])
     ref = Y.ArrayReg.zero_state(n, device=dev)
     # warm the tiled path (plan + first launches) on a throwaway pass
     Y.apply_inplace(circuits[0], ref, Y.MODE_TILED)
     del ref
     ref = Y.ArrayReg.zero_state(n, device=dev)
-    t_tiled = timed(lambda: [Y.apply_inplace(c, ref, Y.MODE_TILED) for c in circuits])
+    t_tiled = timed(lambda: Y.apply_inplace(whole, ref, Y.MODE_TILED))
     out["s_per_circuit_tiled"] = t_tiled
     forms = {}
-    for name, prec, k in (("fused_f64_k5", Y.C128, 5), ("fused_c64_k5", Y.C64, 5)):
+    for name, prec, k in (("fused_f64_k5", Y.C128, 5), ("fused_c64_k5", Y.C64, 5), ("fused_c64_k4", Y.C64, 4)):
         r = Y.ArrayReg.zero_state(n, prec, device=dev)
         Y.apply_inplace(circuits[0], r, Y.MODE_FUSED, k)
         del r
         r = Y.ArrayReg.zero_state(n, prec, device=dev)
-        t = timed(lambda: [Y.apply_inplace(c, r, Y.MODE_FUSED, k) for c in circuits])
+        t = timed(lambda: Y.apply_inplace(whole, r, Y.MODE_FUSED, k))
         f = ref.fidelity(r)
         forms[name] = {"s_per_circuit": t, "one_minus_fidelity": max(0.0, 1.0 - f),
                        "max_abs_err": ref.max_abs_diff(r)}
@@ -456,9 +482,191 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
     for _ in range(reps):
         val, g = Y.expect_grad(op, vc, z)
     dt = (time.perf_counter() - t0) / reps
+    # central finite differences (eps = 1e-5) on a few parameters
+    eps, fd_err = 1e-5, 0.0
+    for i in (0, len(params) // 2, len(params) - 1):
+        pp, pm = list(params), list(params)
+        pp[i] += eps
+        pm[i] -= eps
+        fp = Y.expect_arrayreg(Y.apply(vqe_circuit(Y, nv, lv, pp), z), op).real
+        fm = Y.expect_arrayreg(Y.apply(vqe_circuit(Y, nv, lv, pm), z), op).real
+        fd = (fp - fm) / (2 * eps)
+        fd_err = max(fd_err, abs(fd - g[i]) / max(1e-12, abs(g[i])))
     out["vqe"] = {"qubits": nv, "params": len(g), "gates": len(vc.elements), "grads_per_s": 1.0 / dt,
-                  "s_per_grad": dt, "energy": val}
+                  "s_per_grad": dt, "energy": val, "fd_max_rel_err": fd_err}
+    del z
+    out["qft20"] = qft_extra(Y, A, torch, stream, dev, timed)
+    out["noisy_dm14"] = dm_extra(Y, A, torch, stream, dev, timed)
+    out["batched_circuits"] = batch_extra(Y, A, torch, stream, dev, timed)
+    out["batched_vqe"] = vqe_batch_extra(Y, A, torch, stream, dev, timed)
     return out
+
+
+def uneven_batch(Y, count=2048, seed=4096):
+    """`count` circuits, n ~ U{10..20}, depth ~ U{10..50} layers of the
+    layered-circuit layer type (circuit (n, d) is the first d layers of the
+    n-qubit layered circuit, so equal draws share one Circuit)."""
+    rng = np.random.default_rng(seed)
+    draws = [(int(rng.integers(10, 21)), int(rng.integers(10, 51))) for _ in range(count)]
+    layers, built = {}, {}
+    for n, d in sorted(set(draws)):
+        els = []
+        for l in range(d):
+            if (n, l) not in layers:
+                layers[(n, l)] = layer_elements(Y, n, l)
+            els += layers[(n, l)]
+        built[(n, d)] = Y.Circuit.qubits(n, els)
+    return draws, [built[x] for x in draws]
+
+
+def batch_extra(Y, A, torch, stream, dev, timed):
+    """2048 uneven circuits from |0...0>: the PLAIN per-circuit loop (FP64,
+    the reference result) against one persistent launch per form: TILED
+    complex128 (bit-exact), FUSED complex128 and FUSED complex64 with split
+    coefficients (1 - F and max |error| against the PLAIN states)."""
+    t0 = time.perf_counter()
+    draws, circuits = uneven_batch(Y)
+    build_s = time.perf_counter() - t0
+    gates = sum(len(c.elements) for c in circuits)
+    amps = sum(1 << n for n, _ in draws)
+    res = {"circuits": len(circuits), "gates": gates, "amplitudes": amps, "host_build_s": build_s}
+    ref = [Y.ArrayReg.zero_state(n, device=dev) for n, _ in draws]
+    res["s_plain"] = timed(lambda: Y.batch_apply(circuits, ref, Y.MODE_PLAIN))
+    forms = {}
+    for name, mode, prec, k in (("tiled_c128", Y.MODE_TILED, Y.C128, 0), ("fused_c128_k4", Y.MODE_FUSED, Y.C128, 4),
+                                ("fused_c64_k4", Y.MODE_FUSED, Y.C64, 4)):
+        regs = [Y.ArrayReg.zero_state(n, prec, device=dev) for n, _ in draws]
+        t0 = time.perf_counter()
+        t = timed(lambda: Y.batch_apply(circuits, regs, mode, k))
+        wall = time.perf_counter() - t0
+        worst_f = max(max(0.0, 1.0 - a.fidelity(b)) for a, b in zip(ref, regs))
+        worst_e = max(a.max_abs_diff(b) for a, b in zip(ref, regs))
+        forms[name] = {"s": t, "wall_s": wall, "speedup_vs_plain": res["s_plain"] / t,
+                       "max_one_minus_fidelity": worst_f, "max_abs_err": worst_e}
+        del regs
+    res["forms"] = forms
+    del ref
+    return res
+
+
+def vqe_batch_extra(Y, A, torch, stream, dev, timed):
+    """4096 parameter sets of the 8-layer Ry.Rz + CNOT-ring ansatz at n=16
+    with the TFIM energy and adjoint gradient in one batched sweep, against
+    expect_grad called set by set (rate from the first 32 sets, which are
+    also compared)."""
+    n, layers, nsets = 16, 8, 4096
+    rng = np.random.default_rng(16)
+    sets = rng.uniform(-math.pi, math.pi, size=(nsets, 2 * n * layers))
+    c = vqe_circuit(Y, n, layers, sets[0])
+    op = tfim(Y, n)
+    z = Y.ArrayReg.zero_state(n, device=dev)
+    Y.expect_grad_batch(op, c, sets[:8], z)
+    t0 = time.perf_counter()
+    vals, grads = Y.expect_grad_batch(op, c, sets, z)
+    tb = time.perf_counter() - t0
+    ns, err_v, err_g = 32, 0.0, 0.0
+    t0 = time.perf_counter()
+    for s in range(ns):
+        c.dispatch(list(sets[s]))
+        v, g = Y.expect_grad(op, c, z)
+        err_v = max(err_v, abs(v - vals[s]))
+        err_g = max(err_g, float(np.max(np.abs(np.array(g) - grads[s]))))
+    ts = (time.perf_counter() - t0) / ns
+    return {"qubits": n, "params": int(sets.shape[1]), "sets": nsets, "batched_grads_per_s": nsets / tb,
+            "batched_s": tb, "single_grads_per_s": 1.0 / ts, "speedup": ts * nsets / tb,
+            "max_energy_diff": err_v, "max_grad_diff": err_g}
+
+
+def qft_circuit(Y, n):
+    els = []
+    for i in range(n):
+        els.append(Y.put([i], Y.Gate.H))
+        for j in range(1, n - i):
+            els.append(Y.control([i + j], [i], Y.Gate.Phase(2.0 * math.pi / float(1 << (j + 1)))))
+    for i in range(n // 2):
+        els.append(Y.put([i, n - 1 - i], Y.Gate.SWAP))
+    return Y.Circuit.qubits(n, els)
+
+
+def qft_extra(Y, A, torch, stream, dev, timed):
+    """QFT on 20 qubits (220 gates) on a seeded Gaussian state: s/circuit of
+    the PLAIN and TILED forms, and the oracle's CPU time for the same run."""
+    n = 20
+    rng = np.random.default_rng(20)
+    psi = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    psi /= np.linalg.norm(psi)
+    c = qft_circuit(Y, n)
+    res = {"qubits": n, "gates": len(c.elements)}
+    for name, mode in (("plain", Y.MODE_PLAIN), ("tiled", Y.MODE_TILED)):
+        r = Y.ArrayReg.from_vec(n, psi, device=dev)
+        Y.apply_inplace(c, r, mode)
+        reps = 5
+        r.set_state(psi)
+        t = timed(lambda: [Y.apply_inplace(c, r, mode) for _ in range(reps)])
+        res[f"s_per_circuit_{name}"] = t / reps
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    t0 = time.perf_counter()
+    ref = O.apply_circuit(c, psi)
+    res["cpu_s_per_circuit"] = time.perf_counter() - t0
+    r = Y.ArrayReg.from_vec(n, psi, device=dev)
+    Y.apply_inplace(c, r, Y.MODE_TILED)
+    res["max_abs_diff_vs_oracle"] = float(np.max(np.abs(r.state_vec() - ref)))
+    return res
+
+
+def noisy_dm_circuit(Y, n, layers, seed=14):
+    """Per layer: Ry, Rz on every qubit (U[0, 2 pi)), each followed by
+    Depolarizing(1, 1e-3); CZ brickwork (2i, 2i+1) / (2i+1, 2i+2), each CZ
+    followed by Depolarizing(2, 1e-3); AmplitudeDamping(1e-3) on every qubit."""
+    rng = np.random.default_rng(seed)
+    els = []
+    for layer in range(layers):
+        for q in range(n):
+            for G in (Y.Gate.Ry, Y.Gate.Rz):
+                els.append(Y.put([q], G(float(rng.uniform(0, 2 * math.pi)))))
+                els.append(Y.channel([q], Y.NoiseChannel.Depolarizing(1, 1e-3)))
+        for a in range(0 if layer % 2 == 0 else 1, n - 1, 2):
+            els.append(Y.control([a], [a + 1], Y.Gate.Z))
+            els.append(Y.channel([a, a + 1], Y.NoiseChannel.Depolarizing(2, 1e-3)))
+        for q in range(n):
+            els.append(Y.channel([q], Y.NoiseChannel.AmplitudeDamping(1e-3, 0.0)))
+    return Y.Circuit.qubits(n, els)
+
+
+def dm_extra(Y, A, torch, stream, dev, timed):
+    """Noisy density matrix, n = 14 (4^14 complex128 = 4.3 GB), 20 layers:
+    s/circuit, <Z_i> for every qubit and the purity; the oracle's CPU time
+    for the same circuit at n = 8 (full run) stands beside it."""
+    n, layers = 14, 20
+    c = noisy_dm_circuit(Y, n, layers)
+    d = Y.DensityMatrix.zero_state(n, device=dev)
+    d.apply(noisy_dm_circuit(Y, n, 1, seed=99))  # warm-up
+    del d
+    d = Y.DensityMatrix.zero_state(n, device=dev)
+    A.profile(True, dev)
+    t = timed(lambda: d.apply(c))
+    prof = A.profile_report(dev)
+    A.profile(False, dev)
+    zs = [Y.expect_dm(d, Y.OperatorPolynomial.single(i, Y.Op.Z, 1.0)).real for i in range(n)]
+    res = {"qubits": n, "layers": layers, "elements": len(c.elements), "s_per_circuit": t,
+           "purity": d.purity(), "trace_re": d.trace().real, "z": zs,
+           "kernels": [{"kernel": p["kernel"], "launches": p["launches"], "ms": round(p["ms"], 2),
+                        "GBps": round(p["bytes"] / (p["ms"] / 1e3) / 1e9, 1)} for p in prof]}
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    ns = 8
+    cs = noisy_dm_circuit(Y, ns, layers)
+    rho0 = np.zeros(1 << (2 * ns), complex)
+    rho0[0] = 1
+    t0 = time.perf_counter()
+    ref = O.dm_apply_circuit(cs, rho0)
+    res["cpu_s_per_circuit_n8"] = time.perf_counter() - t0
+    g = Y.DensityMatrix.zero_state(ns, device=dev)
+    g.apply(cs)
+    res["n8_max_abs_diff_vs_oracle"] = float(np.max(np.abs(g.state_data() - ref)))
+    del d
+    return res
 
 
 if __name__ == "__main__":

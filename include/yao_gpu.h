@@ -283,6 +283,13 @@ int yao_measure_with_postprocess(yao_reg* r, const uint32_t* locs, uint32_t nloc
  * (src/apply.rs:123). */
 int yao_batch_apply(const yao_circuit* const* circuits, yao_reg* const* regs, size_t n,
                     int32_t mode, int32_t k);
+/* expect_grad (src/ad.rs:75-156) for nsets parameter vectors of one circuit:
+ * params is nsets x num_params (row-major, Circuit::parameters() order),
+ * values receives nsets energies, grads nsets x num_params.  The circuit's
+ * own parameters are not used or changed.  All sets start from psi0. */
+int yao_expect_grad_batch(const yao_term* terms, size_t nterms, const yao_circuit* c,
+                          const double* params, size_t nsets, const yao_reg* psi0,
+                          double* values, double* grads);
 
 #ifdef __cplusplus
 }

@@ -148,6 +148,35 @@ def test_fused_fp64_and_c64(n):
     assert 1 - abs(np.vdot(ref, out)) ** 2 < 1e-6
 
 
+def test_batched_launch():
+    """Uneven circuits (3..14 qubits, 1..6 layers) in one persistent launch:
+    TILED is bit-exact against the oracle, FUSED (c128 and c64) within its
+    bars; registers of other circuits are not touched."""
+    rng = np.random.default_rng(404)
+    circuits, states = [], []
+    for i in range(24):
+        n = int(rng.integers(3, 15))
+        c = random_circuit(rng, n, int(rng.integers(5, 80)), max_ctrl=2) if i % 3 == 0 else \
+            layered_circuit(n, int(rng.integers(1, 7)), seed=int(rng.integers(1 << 30)))
+        circuits.append(c)
+        states.append(random_state(rng, n))
+    refs = [O.apply_circuit(c, s) for c, s in zip(circuits, states)]
+    regs = [Y.ArrayReg.from_vec(c.nbits, s) for c, s in zip(circuits, states)]
+    Y.batch_apply(circuits, regs, Y.MODE_TILED)
+    for r, ref in zip(regs, refs):
+        assert maxdiff(r.state_vec(), ref) == 0.0
+    for k in (2, 5):
+        regs = [Y.ArrayReg.from_vec(c.nbits, s) for c, s in zip(circuits, states)]
+        Y.batch_apply(circuits, regs, Y.MODE_FUSED, k)
+        for r, ref in zip(regs, refs):
+            assert maxdiff(r.state_vec(), ref) < 1e-10
+    regs = [Y.ArrayReg.from_vec(c.nbits, s).to_precision(Y.C64) for c, s in zip(circuits, states)]
+    Y.batch_apply(circuits, regs, Y.MODE_FUSED, 2)
+    for r, ref in zip(regs, refs):
+        out = r.state_vec().astype(np.complex128)
+        assert 1 - abs(np.vdot(ref, out)) ** 2 < 1e-6
+
+
 def test_layered_circuit_exact_and_roundtrip():
     """The layered workload (Rx, Ry, Rz per qubit + CNOT brickwork) at n=16
     against the oracle, and apply -> dagger round trip at n=24."""
@@ -278,6 +307,67 @@ def test_expect_grad_matches_oracle_and_fd():
         fm = Y.expect_arrayreg(Y.apply(c, r0), op).real
         assert abs((fp - fm) / (2 * h) - g[i]) < 1e-6
     c.dispatch(p0)
+
+
+def test_expect_grad_batch_matches_single_sets():
+    """Many parameter sets of one circuit in one sweep: every set's energy
+    and gradient equal expect_grad on that set (and the oracle)."""
+    rng = np.random.default_rng(31)
+    n = 6
+    els = []
+    for _ in range(2):
+        for q in range(n):
+            els.append(Y.put([q], Gate.Ry(0.1)))
+            els.append(Y.put([q], Gate.Rz(0.2)))
+            els.append(Y.put([q], Gate.Rx(0.0)))
+        els.append(Y.control([0], [3], Gate.Ry(0.3)))
+        els.append(Y.PositionedGate(Gate.Phase(0.4), [2], [4, 5], [True, False]))
+        els.append(Y.put([4, 1], Gate.FSim(0.5, 0.6)))
+        els.append(Y.put([2], Gate.SqrtW))
+        els.append(Y.control([1], [2], Gate.X))
+        els.append(Y.put([0, 5], Gate.ISWAP))
+        els.append(Y.put([3, 1], Gate.SWAP))
+    c = Y.Circuit.qubits(n, els)
+    op = tfim(n, 0.8) + Y.OperatorPolynomial.single(2, Y.Op.Y, 0.3) + \
+        Y.OperatorPolynomial([0.25 - 0.1j], [Y.OperatorString([(0, Y.Op.X), (3, Y.Op.Y)])])
+    psi0 = random_state(rng, n)
+    r0 = Y.ArrayReg.from_vec(n, psi0)
+    p_own = c.parameters()
+    sets = rng.uniform(-math.pi, math.pi, size=(5, c.num_params()))
+    vals, grads = Y.expect_grad_batch(op, c, sets, r0)
+    assert c.parameters() == p_own
+    assert grads.shape == (5, c.num_params())
+    for s in range(5):
+        c.dispatch(list(sets[s]))
+        v, g = Y.expect_grad(op, c, r0)
+        assert abs(vals[s] - v) < 1e-12
+        assert np.max(np.abs(grads[s] - np.array(g))) < 1e-11
+        if s < 2:
+            vo, go = O.expect_grad(op, c, psi0)
+            assert abs(vals[s] - vo) < 1e-12
+            assert np.max(np.abs(grads[s] - np.array(go))) < 1e-11
+    c.dispatch(p_own)
+    # the register is untouched and an empty batch is a no-op
+    assert maxdiff(r0.state_vec(), psi0) == 0.0
+    v0, g0 = Y.expect_grad_batch(op, c, np.zeros((0, c.num_params())), r0)
+    assert v0.shape == (0,) and g0.shape == (0, c.num_params())
+
+
+def test_expect_grad_batch_vqe_many_sets():
+    """64 sets of the VQE ansatz at n=10 against per-set oracle runs."""
+    n, layers, nsets = 10, 2, 64
+    rng = np.random.default_rng(5)
+    sets = rng.uniform(-math.pi, math.pi, size=(nsets, 2 * n * layers))
+    c = vqe_ansatz(n, layers, sets[0])
+    op = tfim(n)
+    vals, grads = Y.expect_grad_batch(op, c, sets, Y.ArrayReg.zero_state(n))
+    z = np.zeros(1 << n, complex)
+    z[0] = 1
+    for s in (0, 17, 63):
+        c.dispatch(list(sets[s]))
+        vo, go = O.expect_grad(op, c, z)
+        assert abs(vals[s] - vo) < 1e-12
+        assert np.max(np.abs(grads[s] - go)) < 1e-11
 
 
 def test_expect_grad_rejects_channels():

@@ -1110,6 +1110,31 @@ int yao_expect_grad(const yao_term* terms, size_t nterms, const yao_circuit* cc,
     return YAO_OK;
 }
 
+int yao_expect_grad_batch(const yao_term* terms, size_t nterms, const yao_circuit* cc, const double* params,
+                          size_t nsets, const yao_reg* psi0, double* values, double* grads) {
+    CHECK_NULL(cc);
+    CHECK_NULL(psi0);
+    CHECK_NULL(values);
+    clear_error();
+    const Circuit* c = cc;
+    for (const Element& el : c->elems)
+        if (el.kind == YAO_ELEM_CHANNEL)
+            return fail(YAO_ERR_CHANNEL_IN_AD,
+                        "expect_grad: circuit contains a noise channel; AD is unsupported for channels");
+    int s = check_apply(c, psi0);
+    if (s) return s;
+    if (psi0->precision != YAO_C128) return fail(YAO_ERR_UNSUPPORTED, "expect_grad runs on complex128 registers");
+    size_t np;
+    yao_circuit_num_params(cc, &np);
+    if (nsets == 0) return YAO_OK;
+    if (np && (!params || !grads)) return fail(YAO_ERR_INVALID_ARGUMENT, "null params or grads");
+    std::vector<MonoTerm> mt;
+    s = build_mono_terms(terms, nterms, psi0->nbits, true, mt);
+    if (s) return s;
+    YAO_CUDA(cudaSetDevice(psi0->ctx->device));
+    return expect_grad_batch(psi0->ctx, mt, c, params, nsets, psi0, values, grads);
+}
+
 // --------------------------------------------------------------- measurement
 int yao_probs(const yao_reg* r, const uint32_t* locs, int32_t nlocs, double* out) {
     CHECK_NULL(r);
@@ -1232,15 +1257,32 @@ int yao_measure_with_postprocess(yao_reg* r, const uint32_t* locs, uint32_t nloc
 // ------------------------------------------------------------------ batched
 int yao_batch_apply(const yao_circuit* const* circuits, yao_reg* const* regs, size_t n, int32_t mode, int32_t k) {
     if (n && (!circuits || !regs)) return fail(YAO_ERR_INVALID_ARGUMENT, "null batch arrays");
+    if (mode < YAO_MODE_PLAIN || mode > YAO_MODE_FUSED) return fail(YAO_ERR_INVALID_ARGUMENT, "unknown apply mode");
     for (size_t i = 0; i < n; i++) {
         int s = check_apply(circuits[i], regs[i]);
         if (s) return s;
+        if (regs[i]->ctx != regs[0]->ctx || regs[i]->precision != regs[0]->precision)
+            return fail(YAO_ERR_INVALID_ARGUMENT, "batched registers must share one context and precision");
     }
+    if (n == 0) return YAO_OK;
+    bool small = false;
+    for (size_t i = 0; i < n; i++) small |= regs[i]->nbits < 3;
+    if (mode == YAO_MODE_PLAIN || small) {
+        // one kernel per gate, circuit after circuit
+        for (size_t i = 0; i < n; i++) {
+            int s = yao_apply_inplace_mode(circuits[i], regs[i], mode, k);
+            if (s) return s;
+        }
+        return YAO_OK;
+    }
+    std::vector<const std::vector<LGate>*> progs(n);
+    std::vector<Reg*> rs(n);
     for (size_t i = 0; i < n; i++) {
-        int s = yao_apply_inplace_mode(circuits[i], regs[i], mode, k);
-        if (s) return s;
+        progs[i] = &lowered(const_cast<yao_circuit*>(circuits[i]));
+        rs[i] = regs[i];
     }
-    return YAO_OK;
+    YAO_CUDA(cudaSetDevice(regs[0]->ctx->device));
+    return launch_batch(regs[0]->ctx, progs, rs, mode, k);
 }
 
 }  // extern "C"

@@ -229,8 +229,11 @@ static int launch_gate_n(Ctx* ctx, V* st, uint32_t nbits, const LGate& g, uint64
     return YAO_OK;
 }
 
+// nsets > 1: the gate acts on nsets registers of nbits qubits stored back to
+// back; the register index sits above every locked bit, so the groups of all
+// registers are enumerated as one range.
 template <typename V>
-static int launch_gate_t(Ctx* ctx, V* st, uint32_t nbits, const LGate& g) {
+static int launch_gate_t(Ctx* ctx, V* st, uint32_t nbits, const LGate& g, uint64_t nsets = 1) {
     DOpT<V> op;
     memset(&op, 0, sizeof(op));
     op.cls = g.cls;
@@ -238,7 +241,7 @@ static int launch_gate_t(Ctx* ctx, V* st, uint32_t nbits, const LGate& g) {
     make_locked(g, op.locked, op.nlocked);
     if (op.nlocked > (int)nbits) return fail(YAO_ERR_INVALID_ARGUMENT, "gate locks more bits than the register has");
     op.cval = g.cval();
-    uint64_t ngroups = (uint64_t)1 << (nbits - op.nlocked);
+    uint64_t ngroups = nsets << (nbits - op.nlocked);
     if (g.k >= 3 && (g.cls == GC_DIAG || g.cls == GC_DENSE))
         return launch_gate_n<V>(ctx, st, nbits, g, ngroups, op.locked, op.nlocked);
     int nl = 1 << g.k;
@@ -286,6 +289,10 @@ static int launch_gate_t(Ctx* ctx, V* st, uint32_t nbits, const LGate& g) {
 int launch_gate(Ctx* ctx, void* state, int32_t precision, uint32_t nbits, const LGate& g) {
     if (precision == YAO_C128) return launch_gate_t<double2>(ctx, (double2*)state, nbits, g);
     return launch_gate_t<float2>(ctx, (float2*)state, nbits, g);
+}
+
+int launch_gate_sets(Ctx* ctx, void* state, uint32_t nbits, const LGate& g, uint64_t nsets) {
+    return launch_gate_t<double2>(ctx, (double2*)state, nbits, g, nsets);
 }
 
 }  // namespace yao

@@ -556,7 +556,14 @@ __global__ void __launch_bounds__(256) k_lambda(const double2* __restrict__ psi,
 }
 
 int build_lambda(Ctx* ctx, const Reg* psi, const std::vector<MonoTerm>& terms, Reg* lambda) {
-    uint64_t n = (uint64_t)1 << psi->nbits;
+    return build_lambda_sets(ctx, psi->d, lambda->d, psi->nbits, 1, terms);
+}
+
+// nsets registers back to back: every mask lies below the register-index
+// bits, so one pass over all nsets * 2^nbits amplitudes builds every lambda.
+int build_lambda_sets(Ctx* ctx, const void* psi_d, void* lam_d, uint32_t nbits, uint64_t nsets,
+                      const std::vector<MonoTerm>& terms) {
+    uint64_t n = nsets << nbits;
     std::vector<MonoFull> h(terms.size());
     for (size_t t = 0; t < terms.size(); t++) {
         h[t].t = to_dev(terms[t]);
@@ -567,7 +574,7 @@ int build_lambda(Ctx* ctx, const Reg* psi, const std::vector<MonoTerm>& terms, R
     size_t bytes = std::max<size_t>(1, h.size()) * sizeof(MonoFull);
     YAO_CUDA(cudaMallocAsync(&d, bytes, ctx->stream));
     if (!h.empty()) YAO_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(MonoFull), cudaMemcpyHostToDevice, ctx->stream));
-    k_lambda<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>((const double2*)psi->d, (double2*)lambda->d, n,
+    k_lambda<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>((const double2*)psi_d, (double2*)lam_d, n,
                                                                        (const MonoFull*)d, (int)h.size());
     ctx->launches++;
     YAO_CUDA(cudaGetLastError());

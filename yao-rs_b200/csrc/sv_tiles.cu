@@ -31,9 +31,11 @@ struct TileHdr {
     int32_t tbits;
     int32_t m;
     int32_t nops;
-    int32_t pad;
+    int32_t nsegs;
     int8_t tb[16];
     uint64_t ntiles;
+    int32_t ncoef;
+    int32_t staged;  // op table, segments and coefficients are copied to shared memory
 };
 
 struct TOp {
@@ -46,7 +48,8 @@ struct TOp {
     uint64_t gcmask, gcval;  // out-of-tile controls (global bit positions)
     uint64_t active;         // DIAG: non-unit entries
     int32_t moff;            // first coefficient in the pass's coefficient array
-    int32_t pad;
+    int8_t rp[kMaxTargets];  // register segments: target positions among the segment's register bits
+    int8_t pad[2];
 };
 
 // Coefficient types: double2 for C128, float4 {hi.re, hi.im, lo.re, lo.im}
@@ -110,97 +113,194 @@ __device__ __forceinline__ bool coef_is_one<float2, float4>(float4 c) {
 }
 
 constexpr int kTileThreads = 512;
-constexpr int kMaxItems = 16;  // outputs per thread in a dense k >= 3 op (tile <= 8192)
+constexpr int kMaxItems = 16;  // outputs per thread in a wide op (2^RB <= 16)
+constexpr size_t kMaxStagedBytes = 48 * 1024;  // pass description staged in shared memory
 
-template <typename V, bool EXACT>
-__global__ void __launch_bounds__(kTileThreads) k_tile_pass(V* __restrict__ st, const TileHdr hdr,
-                                                            const TOp* __restrict__ ops,
-                                                            const typename CoefT<V>::C* __restrict__ coef) {
+// A pass is cut into segments.  In a register segment every thread owns
+// 2^RB amplitudes that differ only in the segment's register bits `rbs` (tile
+// positions, ascending); the segment's ops move amplitudes only along those
+// bits, so the thread applies all of them in registers and touches shared
+// memory once on entry and once on exit.  A wide segment is one dense op on
+// more than two targets, computed through shared memory.
+struct TSeg {
+    int32_t wide;
+    int32_t op_begin, op_end;
+    int8_t rbs[4];
+};
+
+// XOR swizzle of the shared-memory tile against bank conflicts when the
+// lanes of a warp step through higher tile bits.
+__device__ __forceinline__ uint32_t swz(uint32_t l, double2*) { return l ^ ((l >> 3) & 7); }
+__device__ __forceinline__ uint32_t swz(uint32_t l, float2*) { return l ^ ((l >> 4) & 15); }
+
+template <typename V>
+__device__ __forceinline__ uint64_t tile_global(uint64_t base, uint32_t l, const TileHdr& hdr) {
+    uint64_t gi = base | (l & ((1u << hdr.m) - 1));
+    for (int j = hdr.m; j < hdr.tbits; j++) gi |= (uint64_t)((l >> j) & 1) << hdr.tb[j];
+    return gi;
+}
+
+// 1-qubit op (X or dense) on register bit P
+template <typename V, bool EXACT, int RB, int P>
+__device__ __forceinline__ void reg1(V (&v)[1 << RB], const uint32_t lbase, const uint32_t (&roff)[1 << RB],
+                                     const TOp& op, const typename CoefT<V>::C* m) {
     typedef typename CoefT<V>::C C;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    V* s = (V*)smem_raw;
+    const bool isx = op.cls == GC_X;
+    C a, b, c, d;
+    if (!isx) {
+        a = m[0];
+        b = m[1];
+        c = m[2];
+        d = m[3];
+    }
+#pragma unroll
+    for (int j = 0; j < (1 << RB); j++) {
+        if (j & (1 << P)) continue;
+        const int j1 = j | (1 << P);
+        if (((lbase | roff[j]) & op.lcmask) != op.lcval) continue;
+        V w = v[j], x = v[j1];
+        if (isx) {
+            v[j] = x;
+            v[j1] = w;
+        } else {
+            v[j] = cfma_c<EXACT>(cmul_c<EXACT>(a, w), b, x);
+            v[j1] = cfma_c<EXACT>(cmul_c<EXACT>(c, w), d, x);
+        }
+    }
+}
+
+template <typename V, bool EXACT, int RB, int P>
+__device__ __forceinline__ void reg1_at(int p, V (&v)[1 << RB], const uint32_t lbase,
+                                        const uint32_t (&roff)[1 << RB], const TOp& op,
+                                        const typename CoefT<V>::C* m) {
+    if constexpr (P < RB) {
+        if (p == P)
+            reg1<V, EXACT, RB, P>(v, lbase, roff, op, m);
+        else
+            reg1_at<V, EXACT, RB, P + 1>(p, v, lbase, roff, op, m);
+    }
+}
+
+// 2-qubit op (SWAP or dense, bits sorted) on register bits P0 < P1
+template <typename V, bool EXACT, int RB, int P0, int P1>
+__device__ __forceinline__ void reg2(V (&v)[1 << RB], const uint32_t lbase, const uint32_t (&roff)[1 << RB],
+                                     const TOp& op, const typename CoefT<V>::C* m) {
+    typedef typename CoefT<V>::C C;
+#pragma unroll
+    for (int j = 0; j < (1 << RB); j++) {
+        if (j & ((1 << P0) | (1 << P1))) continue;
+        if (((lbase | roff[j]) & op.lcmask) != op.lcval) continue;
+        const int i1 = j | (1 << P0), i2 = j | (1 << P1), i3 = j | (1 << P0) | (1 << P1);
+        if (op.cls == GC_SWAP) {
+            V t = v[i1];
+            v[i1] = v[i2];
+            v[i2] = t;
+        } else {
+            V old[4] = {v[j], v[i1], v[i2], v[i3]};
+            V out[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                V acc = VecT<V>::zero();
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    C cc = m[r * 4 + q];
+                    acc = cfma_c<EXACT>(acc, cc, old[q]);
+                }
+                out[r] = acc;
+            }
+            v[j] = out[0];
+            v[i1] = out[1];
+            v[i2] = out[2];
+            v[i3] = out[3];
+        }
+    }
+}
+
+template <typename V, bool EXACT, int RB, int P0, int P1>
+__device__ __forceinline__ void reg2_at(int p0, int p1, V (&v)[1 << RB], const uint32_t lbase,
+                                        const uint32_t (&roff)[1 << RB], const TOp& op,
+                                        const typename CoefT<V>::C* m) {
+    if constexpr (P0 < RB - 1) {
+        if constexpr (P1 < RB) {
+            if (p0 == P0 && p1 == P1)
+                reg2<V, EXACT, RB, P0, P1>(v, lbase, roff, op, m);
+            else
+                reg2_at<V, EXACT, RB, P0, P1 + 1>(p0, p1, v, lbase, roff, op, m);
+        } else {
+            reg2_at<V, EXACT, RB, P0 + 1, P0 + 2>(p0, p1, v, lbase, roff, op, m);
+        }
+    }
+}
+
+__device__ __forceinline__ double2 ld_l2(const double2* p) { return __ldcg(p); }
+__device__ __forceinline__ float2 ld_l2(const float2* p) { return __ldcg(p); }
+
+// One tile of one pass: load, every segment, store.  COHERENT loads bypass
+// L1 (the tile may have been written by another SM during the same launch).
+template <typename V, bool EXACT, int RB, bool COHERENT>
+__device__ __forceinline__ void tile_body(V* __restrict__ st, const TileHdr& hdr, uint64_t t,
+                                          const TOp* __restrict__ ops, const TSeg* __restrict__ segs,
+                                          const typename CoefT<V>::C* __restrict__ coef, V* s) {
+    typedef typename CoefT<V>::C C;
+    constexpr int NA = 1 << RB;
+    V* tag = nullptr;  // selects the swizzle overload
     const uint32_t T = 1u << hdr.tbits;
-    const uint32_t lowmask = (1u << hdr.m) - 1;
     const int nt = blockDim.x;
-    for (uint64_t t = blockIdx.x; t < hdr.ntiles; t += gridDim.x) {
+    {
         const uint64_t base = insert_zeros(t, hdr.tb, hdr.tbits);
-        // ---- load
         for (uint32_t l = threadIdx.x; l < T; l += nt) {
-            uint64_t gi = base | (l & lowmask);
-            for (int j = hdr.m; j < hdr.tbits; j++) gi |= (uint64_t)((l >> j) & 1) << hdr.tb[j];
-            s[l] = st[gi];
+            const V* src = &st[tile_global<V>(base, l, hdr)];
+            s[swz(l, tag)] = COHERENT ? ld_l2(src) : *src;
         }
         __syncthreads();
-        // ---- ops
-        for (int oi = 0; oi < hdr.nops; oi++) {
-            const TOp& op = ops[oi];
-            if ((base & op.gcmask) != op.gcval) continue;  // uniform over the tile
-            const C* m = coef + op.moff;
-            if (op.cls == GC_X) {
-                const int tq = op.tl[0];
-                for (uint32_t p = threadIdx.x; p < T / 2; p += nt) {
-                    uint32_t i0 = ins0(p, tq);
-                    if ((i0 & op.lcmask) != op.lcval) continue;
-                    uint32_t i1 = i0 | (1u << tq);
-                    V a = s[i0];
-                    s[i0] = s[i1];
-                    s[i1] = a;
+        for (int si = 0; si < hdr.nsegs; si++) {
+            const TSeg sg = segs[si];
+            if (!sg.wide && threadIdx.x < (T >> RB)) {
+                uint32_t lbase = threadIdx.x;
+#pragma unroll
+                for (int i = 0; i < RB; i++) lbase = ins0(lbase, sg.rbs[i]);
+                uint32_t roff[NA];
+                V v[NA];
+#pragma unroll
+                for (int j = 0; j < NA; j++) {
+                    uint32_t o = 0;
+#pragma unroll
+                    for (int i = 0; i < RB; i++) o |= (uint32_t)((j >> i) & 1) << sg.rbs[i];
+                    roff[j] = o;
+                    v[j] = s[swz(lbase | o, tag)];
                 }
-            } else if (op.cls == GC_SWAP) {
-                const int t0 = op.tl[0], t1 = op.tl[1];
-                for (uint32_t q = threadIdx.x; q < T / 4; q += nt) {
-                    uint32_t b = ins0(ins0(q, min(t0, t1)), max(t0, t1));
-                    if ((b & op.lcmask) != op.lcval) continue;
-                    uint32_t i1 = b | (1u << t0), i2 = b | (1u << t1);
-                    V a = s[i1];
-                    s[i1] = s[i2];
-                    s[i2] = a;
-                }
-            } else if (op.cls == GC_DIAG) {
-                for (uint32_t l = threadIdx.x; l < T; l += nt) {
-                    if ((l & op.lcmask) != op.lcval) continue;
-                    uint32_t dl = 0;
-                    if (op.all_local) {
-                        for (int i = 0; i < op.k; i++) dl |= ((l >> op.tl[i]) & 1) << i;
+                for (int oi = sg.op_begin; oi < sg.op_end; oi++) {
+                    const TOp& op = ops[oi];
+                    if ((base & op.gcmask) != op.gcval) continue;  // uniform over the tile
+                    const C* m = coef + op.moff;
+                    if (op.cls == GC_DIAG) {
+#pragma unroll
+                        for (int j = 0; j < NA; j++) {
+                            const uint32_t l = lbase | roff[j];
+                            if ((l & op.lcmask) != op.lcval) continue;
+                            uint32_t dl = 0;
+                            if (op.all_local) {
+                                for (int i = 0; i < op.k; i++) dl |= ((l >> op.tl[i]) & 1) << i;
+                            } else {
+                                const uint64_t gi = tile_global<V>(base, l, hdr);
+                                for (int i = 0; i < op.k; i++) dl |= (uint32_t)((gi >> op.tg[i]) & 1) << i;
+                            }
+                            if ((op.active >> dl) & 1) v[j] = cmulassign_c<EXACT>(v[j], m[dl]);
+                        }
+                    } else if (op.k == 1) {
+                        reg1_at<V, EXACT, RB, 0>(op.rp[0], v, lbase, roff, op, m);
                     } else {
-                        uint64_t gi = base | (l & lowmask);
-                        for (int j = hdr.m; j < hdr.tbits; j++) gi |= (uint64_t)((l >> j) & 1) << hdr.tb[j];
-                        for (int i = 0; i < op.k; i++) dl |= (uint32_t)((gi >> op.tg[i]) & 1) << i;
-                    }
-                    if (!((op.active >> dl) & 1)) continue;
-                    s[l] = cmulassign_c<EXACT>(s[l], m[dl]);
-                }
-            } else if (op.k == 1) {
-                const int tq = op.tl[0];
-                const C a = m[0], b = m[1], c = m[2], d = m[3];
-                for (uint32_t p = threadIdx.x; p < T / 2; p += nt) {
-                    uint32_t i0 = ins0(p, tq);
-                    if ((i0 & op.lcmask) != op.lcval) continue;
-                    uint32_t i1 = i0 | (1u << tq);
-                    V w = s[i0], x = s[i1];
-                    s[i0] = cfma_c<EXACT>(cmul_c<EXACT>(a, w), b, x);
-                    s[i1] = cfma_c<EXACT>(cmul_c<EXACT>(c, w), d, x);
-                }
-            } else if (op.k == 2) {
-                const int t0 = op.tl[0], t1 = op.tl[1];  // t0 < t1 (sorted by the lowering)
-                for (uint32_t q = threadIdx.x; q < T / 4; q += nt) {
-                    uint32_t b = ins0(ins0(q, t0), t1);
-                    if ((b & op.lcmask) != op.lcval) continue;
-                    uint32_t idx[4] = {b, b | (1u << t0), b | (1u << t1), b | (1u << t0) | (1u << t1)};
-                    V old[4];
-#pragma unroll
-                    for (int j = 0; j < 4; j++) old[j] = s[idx[j]];
-#pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        V acc = VecT<V>::zero();
-#pragma unroll
-                        for (int j = 0; j < 4; j++) acc = cfma_c<EXACT>(acc, m[i * 4 + j], old[j]);
-                        s[idx[i]] = acc;
+                        reg2_at<V, EXACT, RB, 0, 1>(op.rp[0], op.rp[1], v, lbase, roff, op, m);
                     }
                 }
-            } else {
-                // dense k >= 3: item it = (group, row); outputs kept in registers
-                // until every thread has read its inputs.
+#pragma unroll
+                for (int j = 0; j < NA; j++) s[swz(lbase | roff[j], tag)] = v[j];
+            } else if (sg.wide) {
+                // one dense op on k >= 3 targets: item = (group, row); outputs
+                // stay in registers until every thread has read its inputs
+                const TOp& op = ops[sg.op_begin];
+                const bool on = (base & op.gcmask) == op.gcval;
+                const C* m = coef + op.moff;
                 const int k = op.k, nl = 1 << k;
                 int sorted[kMaxTargets];
                 for (int i = 0; i < k; i++) sorted[i] = op.tl[i];
@@ -213,11 +313,11 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_pass(V* __restrict__ st, 
                 V outv[kMaxItems];
                 uint32_t outi[kMaxItems];
                 int cnt = 0;
-                for (uint32_t it = threadIdx.x; it < T; it += nt) {
+                for (uint32_t it = threadIdx.x; on && it < T; it += nt) {
                     uint32_t g = it >> k, row = it & (nl - 1);
                     uint32_t b = g;
                     for (int i = 0; i < k; i++) b = ins0(b, sorted[i]);
-                    bool act = (b & op.lcmask) == op.lcval;
+                    const bool act = (b & op.lcmask) == op.lcval;
                     uint32_t ro = 0;
                     for (int i = 0; i < k; i++) ro |= ((row >> i) & 1) << op.tl[i];
                     V acc = VecT<V>::zero();
@@ -226,7 +326,7 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_pass(V* __restrict__ st, 
                         for (int c = 0; c < nl; c++) {
                             uint32_t co = 0;
                             for (int i = 0; i < k; i++) co |= ((c >> i) & 1) << op.tl[i];
-                            acc = cfma_c<EXACT>(acc, mr[c], s[b | co]);
+                            acc = cfma_c<EXACT>(acc, mr[c], s[swz(b | co, tag)]);
                         }
                     }
                     outv[cnt] = acc;
@@ -235,15 +335,144 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_pass(V* __restrict__ st, 
                 }
                 __syncthreads();
                 for (int i = 0; i < cnt; i++)
-                    if (outi[i] != 0xffffffffu) s[outi[i]] = outv[i];
+                    if (outi[i] != 0xffffffffu) s[swz(outi[i], tag)] = outv[i];
             }
             __syncthreads();
         }
-        // ---- store
-        for (uint32_t l = threadIdx.x; l < T; l += nt) {
-            uint64_t gi = base | (l & lowmask);
-            for (int j = hdr.m; j < hdr.tbits; j++) gi |= (uint64_t)((l >> j) & 1) << hdr.tb[j];
-            st[gi] = s[l];
+        for (uint32_t l = threadIdx.x; l < T; l += nt) st[tile_global<V>(base, l, hdr)] = s[swz(l, tag)];
+        if (COHERENT) __threadfence();  // the stores are visible device-wide before the tile is marked done
+        __syncthreads();
+    }
+}
+
+// Bytes of shared memory that hold a staged pass description.
+__host__ __device__ inline size_t staged_bytes(int nops, int nsegs, int ncoef, size_t coef_size) {
+    auto a16 = [](size_t x) { return (x + 15) / 16 * 16; };
+    return a16((size_t)nops * sizeof(TOp)) + a16((size_t)nsegs * sizeof(TSeg)) + a16((size_t)ncoef * coef_size);
+}
+
+// Copy a pass description (ops, segments, coefficients) after the tile in
+// shared memory when the host marked it `staged`; returns the pointers the
+// tile body reads.
+template <typename V>
+__device__ __forceinline__ void stage_pass(const TileHdr& hdr, unsigned char* smem, const TOp*& ops, const TSeg*& segs,
+                                           const typename CoefT<V>::C*& coef) {
+    typedef typename CoefT<V>::C C;
+    if (!hdr.staged) return;
+    auto a16 = [](size_t x) { return (x + 15) / 16 * 16; };
+    unsigned char* p = smem + ((size_t)1 << hdr.tbits) * sizeof(V);
+    TOp* so = (TOp*)p;
+    p += a16((size_t)hdr.nops * sizeof(TOp));
+    TSeg* ss = (TSeg*)p;
+    p += a16((size_t)hdr.nsegs * sizeof(TSeg));
+    C* sc = (C*)p;
+    {
+        const int* src = (const int*)ops;
+        int* dst = (int*)so;
+        for (int i = threadIdx.x; i < hdr.nops * (int)(sizeof(TOp) / 4); i += blockDim.x) dst[i] = src[i];
+        src = (const int*)segs;
+        dst = (int*)ss;
+        for (int i = threadIdx.x; i < hdr.nsegs * (int)(sizeof(TSeg) / 4); i += blockDim.x) dst[i] = src[i];
+    }
+    for (int i = threadIdx.x; i < hdr.ncoef; i += blockDim.x) sc[i] = coef[i];
+    __syncthreads();
+    ops = so;
+    segs = ss;
+    coef = sc;
+}
+
+template <typename V, bool EXACT, int RB>
+__global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
+    k_tile_pass(V* __restrict__ st, const TileHdr hdr, const TOp* __restrict__ gops, const TSeg* __restrict__ gsegs,
+                const typename CoefT<V>::C* __restrict__ gcoef) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const TOp* ops = gops;
+    const TSeg* segs = gsegs;
+    const typename CoefT<V>::C* coef = gcoef;
+    stage_pass<V>(hdr, smem_raw, ops, segs, coef);
+    for (uint64_t t = blockIdx.x; t < hdr.ntiles; t += gridDim.x)
+        tile_body<V, EXACT, RB, false>(st, hdr, t, ops, segs, coef, (V*)smem_raw);
+}
+
+// ------------------------------------------------------------- batches
+//
+// Many circuits (uneven sizes) in one persistent launch.  Every (circuit,
+// pass) is an entry; its tiles are jobs.  Entries are ordered level-major
+// (every circuit's pass 0, then every circuit's pass 1, ...), jobs are taken
+// from a global counter in that order, and a job first waits until all tiles
+// of its circuit's previous passes are done (`done[circuit]` counts finished
+// tiles).  A job only waits on jobs taken before it, by CTAs that are
+// running, so the waits end; each wait is still bounded in time, and a wait
+// that gives up sets `*err` and lets the job (and its circuit) fail.
+struct BatchEntry {
+    TileHdr hdr;
+    uint64_t state;      // device address of the circuit's state
+    uint64_t job_start;  // first job id of this entry
+    uint32_t circuit, pass;
+    int32_t ops_off, segs_off, coef_off, pad;
+};
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+constexpr uint64_t kBatchWaitNs = 2000000000ull;  // 2 s
+
+template <typename V, bool EXACT, int RB>
+__global__ void __launch_bounds__(kTileThreads, 1)
+    k_batch_tiles(const BatchEntry* __restrict__ entries, int nentries, uint64_t njobs,
+                  unsigned long long* __restrict__ next, unsigned int* __restrict__ done, int* __restrict__ err,
+                  const TOp* __restrict__ ops, const TSeg* __restrict__ segs,
+                  const typename CoefT<V>::C* __restrict__ coef) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ unsigned long long sj;
+    __shared__ int se, sskip;
+    for (;;) {
+        if (threadIdx.x == 0) sj = atomicAdd(next, 1ull);
+        __syncthreads();
+        const uint64_t j = sj;
+        if (j >= njobs) break;
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = nentries - 1;  // last entry with job_start <= j
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (entries[mid].job_start <= j)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            se = lo;
+            const BatchEntry& e = entries[lo];
+            const unsigned int need = (unsigned int)(e.pass * e.hdr.ntiles);
+            int skip = 0;
+            if (need > 0) {
+                const uint64_t t0 = global_ns();
+                while (*((volatile unsigned int*)&done[e.circuit]) < need) {
+                    if (global_ns() - t0 > kBatchWaitNs) {
+                        atomicExch(err, 1);
+                        skip = 1;
+                        break;
+                    }
+                    __nanosleep(256);
+                }
+                __threadfence();
+            }
+            sskip = skip;
+        }
+        __syncthreads();
+        const BatchEntry& e = entries[se];
+        if (!sskip) {
+            const TOp* o = ops + e.ops_off;
+            const TSeg* sgs = segs + e.segs_off;
+            const typename CoefT<V>::C* cf = coef + e.coef_off;
+            stage_pass<V>(e.hdr, smem_raw, o, sgs, cf);
+            tile_body<V, EXACT, RB, true>((V*)e.state, e.hdr, j - e.job_start, o, sgs, cf, (V*)smem_raw);
+        }
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(&done[e.circuit], 1u);
         }
         __syncthreads();
     }
@@ -256,8 +485,66 @@ struct PassPlan {
     LGate gate;
     TileHdr hdr;
     std::vector<TOp> ops;
+    std::vector<TSeg> segs;
     std::vector<Cx> coef;
+    int rb = 0;           // register bits per thread in register segments
 };
+
+// Largest number of register bits per thread (512 threads own a 2^12
+// complex128 or 2^13 complex64 tile).
+template <typename V>
+constexpr int max_reg_bits() {
+    return sizeof(V) == 16 ? 3 : 4;
+}
+
+// Cut a pass's ops into segments (see TSeg): consecutive ops whose moving
+// tile bits fit in rb register bits share a register segment; a dense op on
+// three or more targets is a wide segment of its own.
+static void plan_segments(PassPlan& pp, int rb) {
+    pp.rb = rb;
+    pp.segs.clear();
+    const int tbits = pp.hdr.tbits;
+    size_t i = 0;
+    while (i < pp.ops.size()) {
+        TOp& op0 = pp.ops[i];
+        TSeg sg;
+        memset(&sg, 0, sizeof(sg));
+        sg.op_begin = (int32_t)i;
+        if (op0.cls == GC_DENSE && op0.k >= 3) {
+            sg.wide = 1;
+            sg.op_end = (int32_t)i + 1;
+            pp.segs.push_back(sg);
+            i++;
+            continue;
+        }
+        std::set<int> bits;
+        size_t j = i;
+        for (; j < pp.ops.size(); j++) {
+            const TOp& op = pp.ops[j];
+            if (op.cls == GC_DENSE && op.k >= 3) break;
+            std::set<int> nb = bits;
+            if (op.cls != GC_DIAG)
+                for (int q = 0; q < op.k; q++) nb.insert(op.tl[q]);
+            if ((int)nb.size() > rb) break;
+            bits = nb;
+        }
+        // pad with the highest unused tile bits: lanes of a warp then step
+        // through the low bits, which are contiguous in shared memory
+        for (int b = tbits - 1; (int)bits.size() < rb && b >= 0; b--) bits.insert(b);
+        std::vector<int> rbs(bits.begin(), bits.end());
+        for (int q = 0; q < rb; q++) sg.rbs[q] = (int8_t)rbs[q];
+        for (size_t q = i; q < j; q++) {
+            TOp& op = pp.ops[q];
+            if (op.cls == GC_DIAG) continue;
+            for (int t = 0; t < op.k; t++)
+                op.rp[t] = (int8_t)(std::find(rbs.begin(), rbs.end(), (int)op.tl[t]) - rbs.begin());
+        }
+        sg.op_end = (int32_t)j;
+        pp.segs.push_back(sg);
+        i = j;
+    }
+    pp.hdr.nsegs = (int32_t)pp.segs.size();
+}
 
 // Bits a gate moves amplitudes along (DIAG moves none).
 static void moving_bits(const LGate& g, std::vector<int>& out) {
@@ -514,6 +801,36 @@ static void fuse_blocks(const std::vector<LGate>& prog, uint32_t nbits, int k, s
 
 // ------------------------------------------------------------ execution
 
+template <typename V, bool EXACT, int RB>
+static int launch_tile_rb(unsigned grid, unsigned threads, size_t smem, cudaStream_t s, V* st, const TileHdr& hdr,
+                          const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef) {
+    static bool attr = false;
+    if (!attr) {
+        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      160 * 1024));
+        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      cudaSharedmemCarveoutMaxShared));
+        attr = true;
+    }
+    k_tile_pass<V, EXACT, RB><<<grid, threads, smem, s>>>(st, hdr, ops, segs, coef);
+    return YAO_OK;
+}
+
+template <typename V, bool EXACT>
+static int launch_tile(int rb, unsigned grid, unsigned threads, size_t smem, cudaStream_t s, V* st,
+                       const TileHdr& hdr, const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef) {
+    switch (rb) {
+    case 1: return launch_tile_rb<V, EXACT, 1>(grid, threads, smem, s, st, hdr, ops, segs, coef);
+    case 2: return launch_tile_rb<V, EXACT, 2>(grid, threads, smem, s, st, hdr, ops, segs, coef);
+    case 3: return launch_tile_rb<V, EXACT, 3>(grid, threads, smem, s, st, hdr, ops, segs, coef);
+    case 4:
+        if constexpr (sizeof(V) == 8) return launch_tile_rb<V, EXACT, 4>(grid, threads, smem, s, st, hdr, ops, segs, coef);
+        break;
+    default: break;
+    }
+    return fail(YAO_ERR_INVALID_ARGUMENT, "unsupported register-bit count");
+}
+
 template <typename V, bool EXACT>
 static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
     typedef typename CoefT<V>::C C;
@@ -528,25 +845,31 @@ static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
             *p = make_float4(hr, hi, (float)(pp.coef[i].re - (double)hr), (float)(pp.coef[i].im - (double)hi));
         }
     }
-    size_t ob = pp.ops.size() * sizeof(TOp), cb = hc.size() * sizeof(C);
-    size_t cb_off = (ob + 255) / 256 * 256;
+    // one device buffer: ops | segments | coefficients (256-byte aligned parts)
+    size_t ob = pp.ops.size() * sizeof(TOp), sb = pp.segs.size() * sizeof(TSeg), cb = hc.size() * sizeof(C);
+    size_t sb_off = (ob + 255) / 256 * 256;
+    size_t cb_off = sb_off + (sb + 255) / 256 * 256;
     void* dbuf = nullptr;
     YAO_CUDA(cudaMallocAsync(&dbuf, cb_off + cb, ctx->stream));
     YAO_CUDA(cudaMemcpyAsync(dbuf, pp.ops.data(), ob, cudaMemcpyHostToDevice, ctx->stream));
+    YAO_CUDA(cudaMemcpyAsync((char*)dbuf + sb_off, pp.segs.data(), sb, cudaMemcpyHostToDevice, ctx->stream));
     YAO_CUDA(cudaMemcpyAsync((char*)dbuf + cb_off, hc.data(), cb, cudaMemcpyHostToDevice, ctx->stream));
-    size_t smem = ((size_t)1 << pp.hdr.tbits) * sizeof(V);
-    static bool attr_set[2][2] = {{false, false}, {false, false}};
-    bool& a = attr_set[sizeof(V) == 16][EXACT];
-    if (!a) {
-        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        a = true;
-    }
-    unsigned grid = (unsigned)std::min<uint64_t>(pp.hdr.ntiles, (uint64_t)ctx->num_sms * 4);
+    TileHdr hdr = pp.hdr;
+    hdr.ncoef = (int32_t)hc.size();
+    const size_t tile_bytes = ((size_t)1 << hdr.tbits) * sizeof(V);
+    const size_t stg = staged_bytes(hdr.nops, hdr.nsegs, hdr.ncoef, sizeof(C));
+    hdr.staged = stg <= kMaxStagedBytes ? 1 : 0;
+    const size_t smem = tile_bytes + (hdr.staged ? stg : 0);
+    const unsigned threads = (unsigned)(((uint32_t)1 << pp.hdr.tbits) >> pp.rb);
+    const unsigned grid = (unsigned)std::min<uint64_t>(pp.hdr.ntiles, (uint64_t)ctx->num_sms * 4);
+    const TOp* dops = (const TOp*)dbuf;
+    const TSeg* dsegs = (const TSeg*)((char*)dbuf + sb_off);
+    const C* dcoef = (const C*)((char*)dbuf + cb_off);
     {
         ProfScope prof(ctx, EXACT ? "tile_pass_exact" : "tile_pass_fused",
                        (double)pp.hdr.ntiles * (double)((uint64_t)1 << pp.hdr.tbits) * 2.0 * sizeof(V));
-        k_tile_pass<V, EXACT><<<grid, kTileThreads, smem, ctx->stream>>>(st, pp.hdr, (const TOp*)dbuf,
-                                                                          (const C*)((char*)dbuf + cb_off));
+        int s = launch_tile<V, EXACT>(pp.rb, grid, threads, smem, ctx->stream, st, hdr, dops, dsegs, dcoef);
+        if (s) return s;
     }
     ctx->launches++;
     YAO_CUDA(cudaGetLastError());
@@ -565,7 +888,13 @@ static int run_program_t(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32
         return YAO_OK;
     }
     // tile size: 2^12 complex128 (64 KiB) or 2^13 complex64 (64 KiB) per CTA
+    // tile: 2^tbits amplitudes per CTA (shared memory = 2^tbits * sizeof(V));
+    // YAO_TILE_BITS overrides the default for tuning runs
     int tbits = sizeof(V) == 16 ? 12 : 13;
+    if (const char* e = getenv("YAO_TILE_BITS")) {
+        int v = atoi(e);
+        if (v >= 6 && v <= (sizeof(V) == 16 ? 12 : 13)) tbits = v;
+    }
     std::vector<LGate> work;
     bool exact = (mode == YAO_MODE_TILED) && sizeof(V) == 16;
     if (mode == YAO_MODE_FUSED) {
@@ -576,6 +905,20 @@ static int run_program_t(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32
     }
     std::vector<PassPlan> passes;
     plan_passes(work, r->nbits, tbits, passes);
+    // register bits: 3 (8 amplitudes per thread) unless YAO_REG_BITS says
+    // otherwise, more only when the tile would need more than kTileThreads
+    // threads
+    int rb_pref = 3;
+    if (const char* e = getenv("YAO_REG_BITS")) {
+        int v = atoi(e);
+        if (v >= 1 && v <= 4) rb_pref = v;
+    }
+    for (PassPlan& pp : passes)
+        if (!pp.single) {
+            int tb = (int)pp.hdr.tbits;
+            int rb = std::max(tb - 9, std::min(rb_pref, tb));
+            plan_segments(pp, std::min(rb, max_reg_bits<V>()));
+        }
     for (const PassPlan& pp : passes) {
         int s;
         if (pp.single)
@@ -592,6 +935,153 @@ static int run_program_t(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32
 int launch_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k) {
     if (r->precision == YAO_C128) return run_program_t<double2>(ctx, r, prog, mode, k);
     return run_program_t<float2>(ctx, r, prog, mode, k);
+}
+
+// ------------------------------------------------------------ batch host
+
+template <typename V>
+static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs, const std::vector<Reg*>& regs,
+                   int32_t mode, int32_t k) {
+    typedef typename CoefT<V>::C C;
+    const int tbits_cap = 12, rb = 3;
+    const bool exact = mode == YAO_MODE_TILED && sizeof(V) == 16;
+    // plan every circuit
+    std::vector<std::vector<PassPlan>> plans(progs.size());
+    size_t maxpasses = 0;
+    for (size_t c = 0; c < progs.size(); c++) {
+        if (regs[c]->nbits < 3) return fail(YAO_ERR_UNSUPPORTED, "batched circuits need at least 3 qubits");
+        std::vector<LGate> work;
+        if (mode == YAO_MODE_FUSED)
+            fuse_blocks(*progs[c], regs[c]->nbits, k > 0 ? std::min(k, kMaxTargets) : 2, work);
+        else
+            work = *progs[c];
+        plan_passes(work, regs[c]->nbits, tbits_cap, plans[c]);
+        for (PassPlan& pp : plans[c]) {
+            if (pp.single) return fail(YAO_ERR_UNSUPPORTED, "a gate of the batch does not fit a tile");
+            plan_segments(pp, rb);
+        }
+        maxpasses = std::max(maxpasses, plans[c].size());
+    }
+    // entries level-major, ops / segments / coefficients concatenated
+    std::vector<BatchEntry> entries;
+    std::vector<TOp> ops;
+    std::vector<TSeg> segs;
+    std::vector<C> coef;
+    uint64_t njobs = 0;
+    for (size_t level = 0; level < maxpasses; level++)
+        for (size_t c = 0; c < progs.size(); c++) {
+            if (level >= plans[c].size()) continue;
+            const PassPlan& pp = plans[c][level];
+            BatchEntry e;
+            memset(&e, 0, sizeof(e));
+            e.hdr = pp.hdr;
+            e.state = (uint64_t)(uintptr_t)regs[c]->d;
+            e.job_start = njobs;
+            e.circuit = (uint32_t)c;
+            e.pass = (uint32_t)level;
+            e.ops_off = (int32_t)ops.size();
+            e.segs_off = (int32_t)segs.size();
+            e.coef_off = (int32_t)coef.size();
+            ops.insert(ops.end(), pp.ops.begin(), pp.ops.end());
+            segs.insert(segs.end(), pp.segs.begin(), pp.segs.end());
+            for (const Cx& x : pp.coef) {
+                C cc;
+                if (sizeof(V) == 16) {
+                    *(double2*)&cc = make_double2(x.re, x.im);
+                } else {
+                    float hr = (float)x.re, hi = (float)x.im;
+                    *(float4*)&cc = make_float4(hr, hi, (float)(x.re - (double)hr), (float)(x.im - (double)hi));
+                }
+                coef.push_back(cc);
+            }
+            entries.push_back(e);
+            njobs += pp.hdr.ntiles;
+        }
+    if (njobs == 0) return YAO_OK;
+    if (coef.empty()) coef.resize(1);
+    if (ops.empty()) ops.resize(1);
+    if (segs.empty()) segs.resize(1);
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t b_ent = al(entries.size() * sizeof(BatchEntry)), b_ops = al(ops.size() * sizeof(TOp)),
+                 b_seg = al(segs.size() * sizeof(TSeg)), b_coef = al(coef.size() * sizeof(C)),
+                 b_ctr = al(sizeof(unsigned long long) + sizeof(int) + progs.size() * sizeof(unsigned int));
+    char* buf = nullptr;
+    YAO_CUDA(cudaMallocAsync((void**)&buf, b_ent + b_ops + b_seg + b_coef + b_ctr, ctx->stream));
+    char* p = buf;
+    BatchEntry* d_ent = (BatchEntry*)p;
+    p += b_ent;
+    TOp* d_ops = (TOp*)p;
+    p += b_ops;
+    TSeg* d_seg = (TSeg*)p;
+    p += b_seg;
+    C* d_coef = (C*)p;
+    p += b_coef;
+    unsigned long long* d_next = (unsigned long long*)p;
+    int* d_err = (int*)(p + sizeof(unsigned long long));
+    unsigned int* d_done = (unsigned int*)(p + sizeof(unsigned long long) + sizeof(int));
+    YAO_CUDA(cudaMemcpyAsync(d_ent, entries.data(), entries.size() * sizeof(BatchEntry), cudaMemcpyHostToDevice, ctx->stream));
+    YAO_CUDA(cudaMemcpyAsync(d_ops, ops.data(), ops.size() * sizeof(TOp), cudaMemcpyHostToDevice, ctx->stream));
+    YAO_CUDA(cudaMemcpyAsync(d_seg, segs.data(), segs.size() * sizeof(TSeg), cudaMemcpyHostToDevice, ctx->stream));
+    YAO_CUDA(cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(C), cudaMemcpyHostToDevice, ctx->stream));
+    YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+    // every entry's description is staged in shared memory when the largest fits
+    size_t max_stg = 0;
+    std::vector<int32_t> ncoefs(entries.size());
+    {
+        // coefficient counts per entry (entries are laid out in order)
+        for (size_t i = 0; i < entries.size(); i++) {
+            int32_t end = (i + 1 < entries.size()) ? entries[i + 1].coef_off : (int32_t)coef.size();
+            ncoefs[i] = end - entries[i].coef_off;
+            max_stg = std::max(max_stg, staged_bytes(entries[i].hdr.nops, entries[i].hdr.nsegs, ncoefs[i], sizeof(C)));
+        }
+        const int st = max_stg <= kMaxStagedBytes ? 1 : 0;
+        for (size_t i = 0; i < entries.size(); i++) {
+            entries[i].hdr.ncoef = ncoefs[i];
+            entries[i].hdr.staged = st;
+        }
+        YAO_CUDA(cudaMemcpyAsync(d_ent, entries.data(), entries.size() * sizeof(BatchEntry), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (!st) max_stg = 0;
+    }
+    const size_t smem = ((size_t)1 << tbits_cap) * sizeof(V) + max_stg;
+    auto kern = exact ? k_batch_tiles<V, true, 3> : k_batch_tiles<V, false, 3>;
+    YAO_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    YAO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileThreads, smem));
+    const unsigned grid = (unsigned)std::max(1, per_sm) * (unsigned)ctx->num_sms;
+    // capture: reset the queue and counters, run the persistent kernel
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    YAO_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(d_next, 0, b_ctr, ctx->stream);
+    kern<<<grid, kTileThreads, smem, ctx->stream>>>(d_ent, (int)entries.size(), njobs, d_next, d_done, d_err, d_ops,
+                                                    d_seg, d_coef);
+    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+    if (ce != cudaSuccess) return cuda_fail(ce, "capture of the batch launch");
+    YAO_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    {
+        double bytes = 0;
+        for (const BatchEntry& e : entries) bytes += (double)e.hdr.ntiles * (double)(1u << e.hdr.tbits) * 2.0 * sizeof(V);
+        ProfScope prof(ctx, exact ? "batch_tiles_exact" : "batch_tiles_fused", bytes);
+        YAO_CUDA(cudaGraphLaunch(exec, ctx->stream));
+    }
+    ctx->launches++;
+    int herr = 0;
+    YAO_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    YAO_CUDA(cudaFreeAsync(buf, ctx->stream));
+    if (herr) return fail(YAO_ERR_TIMEOUT, "batched launch: a job waited too long for its circuit's previous pass");
+    return YAO_OK;
+}
+
+int launch_batch(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs, const std::vector<Reg*>& regs,
+                 int32_t mode, int32_t k) {
+    if (regs.empty()) return YAO_OK;
+    if (regs[0]->precision == YAO_C128) return batch_t<double2>(ctx, progs, regs, mode, k);
+    return batch_t<float2>(ctx, progs, regs, mode, k);
 }
 
 }  // namespace yao

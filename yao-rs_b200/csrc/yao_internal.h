@@ -179,6 +179,10 @@ struct DM {
 // All launchers enqueue on ctx->stream and return YAO_OK or an error.
 int launch_gate(Ctx* ctx, void* state, int32_t precision, uint32_t nbits, const LGate& g);
 int launch_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k);
+// Many circuits (one register each, same context and precision) in one
+// persistent, graph-captured launch (TILED or FUSED forms).
+int launch_batch(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs, const std::vector<Reg*>& regs,
+                 int32_t mode, int32_t k);
 
 int launch_fill_zero_state(Ctx* ctx, Reg* r, uint64_t basis);
 int launch_uniform_state(Ctx* ctx, Reg* r);
@@ -206,6 +210,13 @@ int expect_terms(Ctx* ctx, const Reg* r, const std::vector<MonoTerm>& terms, std
 // The allocation-free expectation value (static device scratch), sv_reduce.cu.
 int expect_noalloc(Ctx* ctx, const Reg* r, const yao_term* terms, size_t nterms, double* out);
 int build_lambda(Ctx* ctx, const Reg* psi, const std::vector<MonoTerm>& terms, Reg* lambda);
+int build_lambda_sets(Ctx* ctx, const void* psi_d, void* lam_d, uint32_t nbits, uint64_t nsets,
+                      const std::vector<MonoTerm>& terms);
+// A gate on nsets complex128 registers of nbits qubits stored back to back.
+int launch_gate_sets(Ctx* ctx, void* state, uint32_t nbits, const LGate& g, uint64_t nsets);
+// Energies and adjoint gradients of nsets parameter vectors of one circuit.
+int expect_grad_batch(Ctx* ctx, const std::vector<MonoTerm>& terms, const Circuit* c, const double* params,
+                      size_t nsets, const Reg* psi0, double* values, double* grads);
 int adjoint_step(Ctx* ctx, Reg* psi, Reg* lambda, const LGate* gen, const std::vector<LGate>& dag,
                  Cx* dot_out);
 

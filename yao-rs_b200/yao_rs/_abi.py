@@ -146,6 +146,7 @@ SIGNATURES = {
     "yao_measure_with_postprocess": (C.c_int, [vp, u32p, u32, i32, u64, C.c_double,
                                                C.POINTER(C.c_uint8), pp]),
     "yao_batch_apply": (C.c_int, [pp, pp, sz, i32, i32]),
+    "yao_expect_grad_batch": (C.c_int, [C.POINTER(yao_term), sz, vp, dptr, sz, vp, dptr, dptr]),
 }
 
 _lib = None

@@ -60,6 +60,19 @@ def expect_grad(observable, circuit, psi0: ArrayReg):
     return val.value, [grad[i] for i in range(n)]
 
 
+def expect_grad_batch(observable, circuit, params, psi0: ArrayReg):
+    """expect_grad for many parameter vectors (rows of `params`) of one
+    circuit in one batched sweep; returns (energies[nsets], grads[nsets, np])."""
+    P = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1, circuit.num_params()))
+    nsets = P.shape[0]
+    arr, keep = observable.terms_array()
+    vals = np.zeros(nsets)
+    grads = np.zeros((nsets, circuit.num_params()))
+    A.check(A.lib().yao_expect_grad_batch(arr, len(observable), circuit.handle, P.ctypes.data_as(A.dptr), nsets,
+                                          psi0.handle, vals.ctypes.data_as(A.dptr), grads.ctypes.data_as(A.dptr)))
+    return vals, grads
+
+
 def probs(state, locs=None) -> np.ndarray:
     """probs (src/measure.rs:82-87) for an ArrayReg or a DensityMatrix."""
     n = state.nbits()
