@@ -450,15 +450,19 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
     # the 40 layers as one Circuit: tiles and fused blocks span layers
     whole = Y.Circuit.qubits(n, [el for l in range(LAYERS) for el in layer_elements(Y, n, l)])
     ref = Y.ArrayReg.zero_state(n, device=dev)
-    # warm the tiled path (plan + first launches) on a throwaway pass
+    # warm-up: the autotuner picks the tile shape on a prefix of the circuit
+    # (scratch copy of the register), then one throwaway layer
+    chosen = {"tiled": Y.autotune(whole, ref, Y.MODE_TILED)}
     Y.apply_inplace(circuits[0], ref, Y.MODE_TILED)
     del ref
     ref = Y.ArrayReg.zero_state(n, device=dev)
     t_tiled = timed(lambda: Y.apply_inplace(whole, ref, Y.MODE_TILED))
     out["s_per_circuit_tiled"] = t_tiled
     forms = {}
-    for name, prec, k in (("fused_f64_k5", Y.C128, 5), ("fused_c64_k5", Y.C64, 5), ("fused_c64_k4", Y.C64, 4)):
+    for name, prec, k in (("fused_f64_k5", Y.C128, 5), ("fused_c64_k5", Y.C64, 5), ("fused_c64_k4", Y.C64, 4),
+                          ("fused_c64_auto", Y.C64, 0), ("fused_f64_auto", Y.C128, 0)):
         r = Y.ArrayReg.zero_state(n, prec, device=dev)
+        chosen[name] = Y.autotune(whole, r, Y.MODE_FUSED, k)
         Y.apply_inplace(circuits[0], r, Y.MODE_FUSED, k)
         del r
         r = Y.ArrayReg.zero_state(n, prec, device=dev)
@@ -468,6 +472,7 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
                        "max_abs_err": ref.max_abs_diff(r)}
         del r
     out["fused"] = forms
+    out["autotuned"] = chosen
     del ref
     # VQE: n=24, 8 layers of Ry.Rz on every qubit + CNOT ring, TFIM
     nv, lv = 24, 8
@@ -533,8 +538,13 @@ def batch_extra(Y, A, torch, stream, dev, timed):
     ref = [Y.ArrayReg.zero_state(n, device=dev) for n, _ in draws]
     res["s_plain"] = timed(lambda: Y.batch_apply(circuits, ref, Y.MODE_PLAIN))
     forms = {}
-    for name, mode, prec, k in (("tiled_c128", Y.MODE_TILED, Y.C128, 0), ("fused_c128_k4", Y.MODE_FUSED, Y.C128, 4),
-                                ("fused_c64_k4", Y.MODE_FUSED, Y.C64, 4)):
+    for name, mode, prec, k in (("tiled_c128", Y.MODE_TILED, Y.C128, 0), ("fused_c128_auto", Y.MODE_FUSED, Y.C128, 0),
+                                ("fused_c64_auto", Y.MODE_FUSED, Y.C64, 0), ("fused_c64_k2", Y.MODE_FUSED, Y.C64, 2)):
+        # warm-up on 64 of the circuits (the batch autotuner runs here)
+        wi = [max(range(len(draws)), key=lambda i: draws[i][0])] + list(range(63))
+        warm = [Y.ArrayReg.zero_state(draws[i][0], prec, device=dev) for i in wi]
+        Y.batch_apply([circuits[i] for i in wi], warm, mode, k)
+        del warm
         regs = [Y.ArrayReg.zero_state(n, prec, device=dev) for n, _ in draws]
         t0 = time.perf_counter()
         t = timed(lambda: Y.batch_apply(circuits, regs, mode, k))
@@ -546,6 +556,22 @@ def batch_extra(Y, A, torch, stream, dev, timed):
         del regs
     res["forms"] = forms
     del ref
+    # CPU: the oracle (single thread) on 16 of the circuits with n <= 16,
+    # extrapolated to the batch by amplitude-gate updates
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    rng = np.random.default_rng(7)
+    small = [i for i, (nq, _) in enumerate(draws) if nq <= 16]
+    pick = sorted(rng.choice(small, size=min(16, len(small)), replace=False).tolist())
+    t0 = time.perf_counter()
+    for i in pick:
+        z = np.zeros(1 << draws[i][0], complex)
+        z[0] = 1
+        O.apply_circuit(circuits[i], z)
+    t_s = time.perf_counter() - t0
+    work = lambda idx: sum(len(circuits[i].elements) * (1 << draws[i][0]) for i in idx)
+    res["cpu_oracle_sample"] = {"circuits": len(pick), "s": t_s, "threads": 1,
+                                "s_batch_extrapolated": t_s * work(range(len(circuits))) / work(pick)}
     return res
 
 
@@ -572,9 +598,19 @@ def vqe_batch_extra(Y, A, torch, stream, dev, timed):
         err_v = max(err_v, abs(v - vals[s]))
         err_g = max(err_g, float(np.max(np.abs(np.array(g) - grads[s]))))
     ts = (time.perf_counter() - t0) / ns
+    # CPU: the oracle's expect_grad (single thread) on set 0
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    c.dispatch(list(sets[0]))
+    z0 = np.zeros(1 << n, complex)
+    z0[0] = 1
+    t0 = time.perf_counter()
+    vo, go = O.expect_grad(op, c, z0)
+    t_cpu = time.perf_counter() - t0
     return {"qubits": n, "params": int(sets.shape[1]), "sets": nsets, "batched_grads_per_s": nsets / tb,
             "batched_s": tb, "single_grads_per_s": 1.0 / ts, "speedup": ts * nsets / tb,
-            "max_energy_diff": err_v, "max_grad_diff": err_g}
+            "max_energy_diff": err_v, "max_grad_diff": err_g, "cpu_oracle_s_per_grad": t_cpu,
+            "max_grad_diff_vs_oracle": float(np.max(np.abs(np.asarray(go) - grads[0])))}
 
 
 def qft_circuit(Y, n):

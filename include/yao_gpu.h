@@ -102,7 +102,9 @@ enum yao_precision { YAO_C128 = 0, YAO_C64 = 1 };
  *   FUSED     gates multiplied into dense k-qubit blocks on the host (FP64),
  *             each block one tiled pass; not bit-exact, report 1 - fidelity.
  *             On a YAO_C64 register the blocks are applied with split
- *             (hi + lo) FP32 products accumulated in FP32. */
+ *             (hi + lo) FP32 products accumulated in FP32, and when every
+ *             gate is unitary the input's FP64 norm is restored at the end
+ *             (yao_apply_inplace_mode; the batched form does not). */
 enum yao_apply_mode { YAO_MODE_PLAIN = 0, YAO_MODE_TILED = 1, YAO_MODE_FUSED = 2 };
 
 /* One circuit element: PositionedGate (src/circuit.rs:103-109),
@@ -219,6 +221,14 @@ int yao_apply(const yao_circuit* c, const yao_reg* r, yao_reg** out);
 /* The same with an explicit execution form (enum yao_apply_mode); k is the
  * fusion width of YAO_MODE_FUSED (1..6; 0 = autotuned). */
 int yao_apply_inplace_mode(const yao_circuit* c, yao_reg* r, int32_t mode, int32_t k);
+/* Autotuner of the TILED / FUSED forms (no yao-rs counterpart): times tile
+ * shapes (and, for FUSED with k = 0, fusion widths 2..6) on a prefix of c
+ * applied to a scratch copy of r (r is not changed) and records the fastest
+ * for r's qubit count, precision and mode; later apply calls with the same
+ * (qubits, precision, mode, k) use it.  choice[3] = {k, tile bits, register
+ * bits}.  Apply calls tune on first use by themselves unless YAO_AUTOTUNE=0;
+ * YAO_TUNE_CACHE=<file> keeps the choices across processes. */
+int yao_autotune(const yao_circuit* c, yao_reg* r, int32_t mode, int32_t k, int32_t* choice);
 
 /* ---------------------------------------------------------- DensityMatrix */
 /* DensityMatrix::from_reg / zero_state / mixed (src/density_matrix.rs:19-57). */

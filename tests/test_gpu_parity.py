@@ -148,6 +148,39 @@ def test_fused_fp64_and_c64(n):
     assert 1 - abs(np.vdot(ref, out)) ** 2 < 1e-6
 
 
+def test_autotune_and_tile_shapes(monkeypatch):
+    """The autotuner's choice is a valid shape, leaves the register alone, and
+    every tile shape it can pick keeps TILED bit-exact and FUSED in bounds."""
+    rng = np.random.default_rng(99)
+    n = 15
+    c = random_circuit(rng, n, 150, max_ctrl=2)
+    psi = random_state(rng, n)
+    ref = O.apply_circuit(c, psi)
+    r = Y.ArrayReg.from_vec(n, psi)
+    ch = Y.autotune(c, r, Y.MODE_TILED)
+    assert 10 <= ch["tile_bits"] <= 12 and 2 <= ch["reg_bits"] <= 3
+    assert maxdiff(r.state_vec(), psi) == 0.0
+    Y.apply_inplace(c, r, Y.MODE_TILED)
+    assert maxdiff(r.state_vec(), ref) == 0.0
+    r = Y.ArrayReg.from_vec(n, psi)
+    ch = Y.autotune(c, r, Y.MODE_FUSED, 0)
+    assert 2 <= ch["k"] <= 6
+    Y.apply_inplace(c, r, Y.MODE_FUSED, 0)
+    assert maxdiff(r.state_vec(), ref) < 1e-10
+    for tb, rb in ((10, 2), (11, 2), (11, 3), (12, 3), (12, 2), (9, 1)):
+        monkeypatch.setenv("YAO_TILE_BITS", str(tb))
+        monkeypatch.setenv("YAO_REG_BITS", str(rb))
+        assert maxdiff(gpu_apply(c, psi, Y.MODE_TILED), ref) == 0.0, (tb, rb)
+        assert maxdiff(gpu_apply(c, psi, Y.MODE_FUSED, 4), ref) < 1e-10, (tb, rb)
+    for tb, rb in ((13, 4), (12, 4), (11, 2), (12, 3)):
+        monkeypatch.setenv("YAO_TILE_BITS", str(tb))
+        monkeypatch.setenv("YAO_REG_BITS", str(rb))
+        r = Y.ArrayReg.from_vec(n, psi).to_precision(Y.C64)
+        Y.apply_inplace(c, r, Y.MODE_FUSED, 5)
+        out = r.state_vec().astype(np.complex128)
+        assert 1 - abs(np.vdot(ref, out)) ** 2 < 1e-6, (tb, rb)
+
+
 def test_batched_launch():
     """Uneven circuits (3..14 qubits, 1..6 layers) in one persistent launch:
     TILED is bit-exact against the oracle, FUSED (c128 and c64) within its
@@ -507,3 +540,26 @@ def test_density_matrix_purity_large():
     assert abs(d.purity() - O.dm_purity(d.state_data(), n)) < 1e-12
     mixed = Y.DensityMatrix.mixed([0.5, 0.5], [Y.ArrayReg.zero_state(1), Y.ArrayReg.product_state([1])])
     assert abs(mixed.purity() - 0.5) < 1e-12
+
+
+def test_batch_bounded_wait_reports_timeout(monkeypatch):
+    """The batched launch's dependency wait is bounded: with circuit 0's
+    second pass made to wait for a count that never comes (test hook), the
+    wait gives up after 0.2 s, the call fails with YAO_ERR_TIMEOUT, and the
+    context keeps working."""
+    from yao_rs import _abi as A
+    rng = np.random.default_rng(5)
+    circuits = [layered_circuit(8, 3, seed=11), layered_circuit(8, 2, seed=12)]
+    states = [random_state(rng, 8) for _ in circuits]
+    monkeypatch.setenv("YAO_TILE_BITS", "6")
+    monkeypatch.setenv("YAO_AUTOTUNE", "0")
+    monkeypatch.setenv("YAO_TEST_BATCH_STALL", "1")
+    regs = [Y.ArrayReg.from_vec(8, s) for s in states]
+    with pytest.raises(Y.YaoError) as ei:
+        Y.batch_apply(circuits, regs, Y.MODE_TILED)
+    assert ei.value.status == A.YAO_ERR_TIMEOUT
+    monkeypatch.delenv("YAO_TEST_BATCH_STALL")
+    regs = [Y.ArrayReg.from_vec(8, s) for s in states]
+    Y.batch_apply(circuits, regs, Y.MODE_TILED)
+    for c, s, r in zip(circuits, states, regs):
+        assert maxdiff(r.state_vec(), O.apply_circuit(c, s)) == 0.0

@@ -62,7 +62,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, force, verbose), srcs))
     if force or _stale(OUT, objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", str(OUT), *map(str, objs), "-cudart", "static"]
+        cmd = [NVCC, *ARCH, "-shared", "-o", str(OUT), *map(str, objs), "-cudart", "static", "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -765,6 +765,31 @@ int yao_reg_max_abs_diff(const yao_reg* a, const yao_reg* b, double* out) {
 }
 
 // --------------------------------------------------------------------- apply
+// Every lowered gate is unitary to 1e-12 (named gates are; a Custom matrix
+// is checked).
+static bool program_is_unitary(const std::vector<LGate>& prog) {
+    for (const LGate& g : prog) {
+        if (g.cls == GC_X || g.cls == GC_SWAP) continue;
+        const size_t d = (size_t)1 << g.k;
+        if (g.cls == GC_DIAG) {
+            for (const Cx& x : g.m)
+                if (std::fabs(x.re * x.re + x.im * x.im - 1.0) > 1e-12) return false;
+            continue;
+        }
+        for (size_t i = 0; i < d; i++)
+            for (size_t j = 0; j < d; j++) {
+                double re = 0, im = 0;
+                for (size_t r = 0; r < d; r++) {
+                    const Cx a = g.m[r * d + i], b = g.m[r * d + j];
+                    re += a.re * b.re + a.im * b.im;
+                    im += a.re * b.im - a.im * b.re;
+                }
+                if (std::fabs(re - (i == j ? 1.0 : 0.0)) > 1e-12 || std::fabs(im) > 1e-12) return false;
+            }
+    }
+    return true;
+}
+
 int yao_apply_inplace_mode(const yao_circuit* cc, yao_reg* r, int32_t mode, int32_t k) {
     CHECK_NULL(cc);
     CHECK_NULL(r);
@@ -775,10 +800,35 @@ int yao_apply_inplace_mode(const yao_circuit* cc, yao_reg* r, int32_t mode, int3
     if (mode < YAO_MODE_PLAIN || mode > YAO_MODE_FUSED) return fail(YAO_ERR_INVALID_ARGUMENT, "unknown apply mode");
     YAO_CUDA(cudaSetDevice(r->ctx->device));
     const std::vector<LGate>& prog = lowered(c);
+    // FUSED on complex64: the FP32 arithmetic drifts the norm by a few 1e-7
+    // over thousands of gates; a unitary circuit keeps the input's norm, so
+    // the FP64 norm of the input is restored afterwards.
+    const bool renorm = mode == YAO_MODE_FUSED && r->precision == YAO_C64 && !prog.empty() && program_is_unitary(prog);
+    double n0 = 0.0;
+    if (renorm && (s = reduce_norm_sqr(r->ctx, r, &n0))) return s;
     s = launch_program(r->ctx, r, prog, mode, k);
     if (s) return s;
+    if (renorm && n0 > 0.0) {
+        double n1 = 0.0;
+        if ((s = reduce_norm_sqr(r->ctx, r, &n1))) return s;
+        if (n1 > 0.0 && (s = launch_scale(r->ctx, r, std::sqrt(n1 / n0)))) return s;
+    }
     YAO_CUDA(cudaGetLastError());
     return YAO_OK;
+}
+
+int yao_autotune(const yao_circuit* cc, yao_reg* r, int32_t mode, int32_t k, int32_t* choice) {
+    CHECK_NULL(cc);
+    CHECK_NULL(r);
+    CHECK_NULL(choice);
+    clear_error();
+    yao_circuit* c = const_cast<yao_circuit*>(cc);
+    int s = check_apply(c, r);
+    if (s) return s;
+    if (mode != YAO_MODE_TILED && mode != YAO_MODE_FUSED)
+        return fail(YAO_ERR_INVALID_ARGUMENT, "autotuning applies to the TILED and FUSED modes");
+    YAO_CUDA(cudaSetDevice(r->ctx->device));
+    return autotune_program(r->ctx, r, lowered(c), mode, k, choice);
 }
 
 int yao_apply_inplace(const yao_circuit* c, yao_reg* r) { return yao_apply_inplace_mode(c, r, YAO_MODE_PLAIN, 0); }

@@ -20,7 +20,13 @@
 //    FP32 (a two-term compensated product).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <map>
+#include <mutex>
 #include <set>
+#include <string>
+#include <thread>
+#include <atomic>
 #include <vector>
 
 #include "device_common.cuh"
@@ -43,14 +49,15 @@ struct TOp {
     int32_t k;
     int8_t tl[kMaxTargets];  // local target positions (-1 = outside the tile, DIAG only)
     int8_t tg[kMaxTargets];  // global target positions
-    int32_t all_local;
+    int8_t rp[kMaxTargets];  // register segments: target positions among the segment's register bits
+    int8_t ts[kMaxTargets];  // wide ops: local target positions, ascending
     uint32_t lcmask, lcval;  // in-tile controls (local bit positions)
     uint64_t gcmask, gcval;  // out-of-tile controls (global bit positions)
     uint64_t active;         // DIAG: non-unit entries
     int32_t moff;            // first coefficient in the pass's coefficient array
-    int8_t rp[kMaxTargets];  // register segments: target positions among the segment's register bits
-    int8_t pad[2];
+    int32_t all_local;
 };
+static_assert(sizeof(TOp) % 8 == 0, "TOp is copied as 32-bit words and read as 64-bit fields");
 
 // Coefficient types: double2 for C128, float4 {hi.re, hi.im, lo.re, lo.im}
 // for C64 (split coefficient).
@@ -113,7 +120,6 @@ __device__ __forceinline__ bool coef_is_one<float2, float4>(float4 c) {
 }
 
 constexpr int kTileThreads = 512;
-constexpr int kMaxItems = 16;  // outputs per thread in a wide op (2^RB <= 16)
 constexpr size_t kMaxStagedBytes = 48 * 1024;  // pass description staged in shared memory
 
 // A pass is cut into segments.  In a register segment every thread owns
@@ -133,11 +139,23 @@ struct TSeg {
 __device__ __forceinline__ uint32_t swz(uint32_t l, double2*) { return l ^ ((l >> 3) & 7); }
 __device__ __forceinline__ uint32_t swz(uint32_t l, float2*) { return l ^ ((l >> 4) & 15); }
 
-template <typename V>
-__device__ __forceinline__ uint64_t tile_global(uint64_t base, uint32_t l, const TileHdr& hdr) {
-    uint64_t gi = base | (l & ((1u << hdr.m) - 1));
-    for (int j = hdr.m; j < hdr.tbits; j++) gi |= (uint64_t)((l >> j) & 1) << hdr.tb[j];
-    return gi;
+// Global index of tile position l: the low m positions are the low bits
+// themselves; the rest scatter to the tile's higher bits through a table of
+// 2^(tbits - m) offsets built once per pass in shared memory.
+constexpr int kMaxScatterBits = 9;
+
+__device__ __forceinline__ void tile_offsets(const TileHdr& hdr, uint64_t* hoff) {
+    const uint32_t nh = 1u << (hdr.tbits - hdr.m);
+    for (uint32_t h = threadIdx.x; h < nh; h += blockDim.x) {
+        uint64_t o = 0;
+        for (int j = hdr.m; j < hdr.tbits; j++) o |= (uint64_t)((h >> (j - hdr.m)) & 1) << hdr.tb[j];
+        hoff[h] = o;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ uint64_t tile_global(uint64_t base, uint32_t l, int m, const uint64_t* hoff) {
+    return base | (l & ((1u << m) - 1)) | hoff[l >> m];
 }
 
 // 1-qubit op (X or dense) on register bit P
@@ -235,27 +253,21 @@ __device__ __forceinline__ void reg2_at(int p0, int p1, V (&v)[1 << RB], const u
 __device__ __forceinline__ double2 ld_l2(const double2* p) { return __ldcg(p); }
 __device__ __forceinline__ float2 ld_l2(const float2* p) { return __ldcg(p); }
 
-// One tile of one pass: load, every segment, store.  COHERENT loads bypass
-// L1 (the tile may have been written by another SM during the same launch).
-template <typename V, bool EXACT, int RB, bool COHERENT>
-__device__ __forceinline__ void tile_body(V* __restrict__ st, const TileHdr& hdr, uint64_t t,
-                                          const TOp* __restrict__ ops, const TSeg* __restrict__ segs,
-                                          const typename CoefT<V>::C* __restrict__ coef, V* s) {
+// The segments of one pass on one tile held in shared memory `s` (the tile
+// at `base`).  Ends with the tile updated in `s` and a __syncthreads().
+template <typename V, bool EXACT, int RB>
+__device__ __forceinline__ void tile_compute(const TileHdr& hdr, uint64_t base, const TOp* __restrict__ ops,
+                                             const TSeg* __restrict__ segs,
+                                             const typename CoefT<V>::C* __restrict__ coef, V* s) {
     typedef typename CoefT<V>::C C;
     constexpr int NA = 1 << RB;
     V* tag = nullptr;  // selects the swizzle overload
     const uint32_t T = 1u << hdr.tbits;
-    const int nt = blockDim.x;
-    {
-        const uint64_t base = insert_zeros(t, hdr.tb, hdr.tbits);
-        for (uint32_t l = threadIdx.x; l < T; l += nt) {
-            const V* src = &st[tile_global<V>(base, l, hdr)];
-            s[swz(l, tag)] = COHERENT ? ld_l2(src) : *src;
-        }
-        __syncthreads();
-        for (int si = 0; si < hdr.nsegs; si++) {
-            const TSeg sg = segs[si];
-            if (!sg.wide && threadIdx.x < (T >> RB)) {
+    const uint32_t nt = blockDim.x;
+    for (int si = 0; si < hdr.nsegs; si++) {
+        const TSeg sg = segs[si];
+        if (!sg.wide) {
+            if (threadIdx.x < (T >> RB)) {
                 uint32_t lbase = threadIdx.x;
 #pragma unroll
                 for (int i = 0; i < RB; i++) lbase = ins0(lbase, sg.rbs[i]);
@@ -274,17 +286,19 @@ __device__ __forceinline__ void tile_body(V* __restrict__ st, const TileHdr& hdr
                     if ((base & op.gcmask) != op.gcval) continue;  // uniform over the tile
                     const C* m = coef + op.moff;
                     if (op.cls == GC_DIAG) {
+                        // entry index: out-of-tile target bits come from the
+                        // tile base, in-tile ones from the amplitude's position
+                        uint32_t dl0 = 0;
+                        if (!op.all_local)
+                            for (int i = 0; i < op.k; i++)
+                                if (op.tl[i] < 0) dl0 |= (uint32_t)((base >> op.tg[i]) & 1) << i;
 #pragma unroll
                         for (int j = 0; j < NA; j++) {
                             const uint32_t l = lbase | roff[j];
                             if ((l & op.lcmask) != op.lcval) continue;
-                            uint32_t dl = 0;
-                            if (op.all_local) {
-                                for (int i = 0; i < op.k; i++) dl |= ((l >> op.tl[i]) & 1) << i;
-                            } else {
-                                const uint64_t gi = tile_global<V>(base, l, hdr);
-                                for (int i = 0; i < op.k; i++) dl |= (uint32_t)((gi >> op.tg[i]) & 1) << i;
-                            }
+                            uint32_t dl = dl0;
+                            for (int i = 0; i < op.k; i++)
+                                if (op.tl[i] >= 0) dl |= ((l >> op.tl[i]) & 1) << i;
                             if ((op.active >> dl) & 1) v[j] = cmulassign_c<EXACT>(v[j], m[dl]);
                         }
                     } else if (op.k == 1) {
@@ -295,54 +309,126 @@ __device__ __forceinline__ void tile_body(V* __restrict__ st, const TileHdr& hdr
                 }
 #pragma unroll
                 for (int j = 0; j < NA; j++) s[swz(lbase | roff[j], tag)] = v[j];
-            } else if (sg.wide) {
-                // one dense op on k >= 3 targets: item = (group, row); outputs
-                // stay in registers until every thread has read its inputs
-                const TOp& op = ops[sg.op_begin];
-                const bool on = (base & op.gcmask) == op.gcval;
-                const C* m = coef + op.moff;
-                const int k = op.k, nl = 1 << k;
-                int sorted[kMaxTargets];
-                for (int i = 0; i < k; i++) sorted[i] = op.tl[i];
-                for (int i = 1; i < k; i++)
-                    for (int j = i; j > 0 && sorted[j - 1] > sorted[j]; j--) {
-                        int tmp = sorted[j];
-                        sorted[j] = sorted[j - 1];
-                        sorted[j - 1] = tmp;
-                    }
-                V outv[kMaxItems];
-                uint32_t outi[kMaxItems];
-                int cnt = 0;
-                for (uint32_t it = threadIdx.x; on && it < T; it += nt) {
-                    uint32_t g = it >> k, row = it & (nl - 1);
-                    uint32_t b = g;
-                    for (int i = 0; i < k; i++) b = ins0(b, sorted[i]);
-                    const bool act = (b & op.lcmask) == op.lcval;
-                    uint32_t ro = 0;
-                    for (int i = 0; i < k; i++) ro |= ((row >> i) & 1) << op.tl[i];
-                    V acc = VecT<V>::zero();
-                    if (act) {
-                        const C* mr = m + (size_t)row * nl;
-                        for (int c = 0; c < nl; c++) {
-                            uint32_t co = 0;
-                            for (int i = 0; i < k; i++) co |= ((c >> i) & 1) << op.tl[i];
-                            acc = cfma_c<EXACT>(acc, mr[c], s[swz(b | co, tag)]);
-                        }
-                    }
-                    outv[cnt] = acc;
-                    outi[cnt] = act ? (b | ro) : 0xffffffffu;
-                    cnt++;
-                }
-                __syncthreads();
-                for (int i = 0; i < cnt; i++)
-                    if (outi[i] != 0xffffffffu) s[swz(outi[i], tag)] = outv[i];
+            }
+        } else {
+            // one dense op on k >= 3 targets (a 2^k x 2^k matrix times the
+            // G = T / 2^k groups of the tile).  Item it = (row, group) with
+            // the group index fastest, so a warp reads one matrix row
+            // (broadcast) against 32 groups.  When G divides the thread
+            // count, a thread's NA items share one group and every amplitude
+            // it loads serves NA rows.  Outputs stay in registers until
+            // every thread has read its inputs.
+            __shared__ uint32_t wco[1 << kMaxTargets];  // local offset of column / row c
+            const TOp& op = ops[sg.op_begin];
+            const bool on = (base & op.gcmask) == op.gcval;
+            const C* m = coef + op.moff;
+            const int k = op.k, nl = 1 << k;
+            const uint32_t G = T >> k;
+            for (int c = threadIdx.x; c < nl; c += nt) {
+                uint32_t co = 0;
+                for (int q = 0; q < k; q++) co |= (uint32_t)((c >> q) & 1) << op.tl[q];
+                wco[c] = co;
             }
             __syncthreads();
+            V outv[NA];
+            uint32_t outi[NA];
+#pragma unroll
+            for (int i = 0; i < NA; i++) {
+                outi[i] = 0xffffffffu;
+                outv[i] = VecT<V>::zero();
+            }
+            if (on && G <= nt) {
+                const uint32_t g = threadIdx.x & (G - 1);
+                uint32_t b = g;
+                for (int q = 0; q < k; q++) b = ins0(b, op.ts[q]);
+                const uint32_t row0 = threadIdx.x / G, rstep = nt / G;
+                if ((b & op.lcmask) == op.lcval) {
+                    for (int c = 0; c < nl; c++) {
+                        const V x = s[swz(b | wco[c], tag)];
+#pragma unroll
+                        for (int i = 0; i < NA; i++) {
+                            const uint32_t row = row0 + (uint32_t)i * rstep;
+                            if (row < (uint32_t)nl) outv[i] = cfma_c<EXACT>(outv[i], m[(size_t)row * nl + c], x);
+                        }
+                    }
+#pragma unroll
+                    for (int i = 0; i < NA; i++) {
+                        const uint32_t row = row0 + (uint32_t)i * rstep;
+                        if (row < (uint32_t)nl) outi[i] = b | wco[row];
+                    }
+                }
+            } else if (on) {
+#pragma unroll
+                for (int i = 0; i < NA; i++) {
+                    const uint32_t it = threadIdx.x + (uint32_t)i * nt;
+                    if (it >= T) continue;
+                    const uint32_t g = it & (G - 1), row = it / G;
+                    uint32_t b = g;
+                    for (int q = 0; q < k; q++) b = ins0(b, op.ts[q]);
+                    if ((b & op.lcmask) != op.lcval) continue;
+                    V acc = VecT<V>::zero();
+                    const C* mr = m + (size_t)row * nl;
+                    for (int c = 0; c < nl; c++) acc = cfma_c<EXACT>(acc, mr[c], s[swz(b | wco[c], tag)]);
+                    outv[i] = acc;
+                    outi[i] = b | wco[row];
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < NA; i++)
+                if (outi[i] != 0xffffffffu) s[swz(outi[i], tag)] = outv[i];
         }
-        for (uint32_t l = threadIdx.x; l < T; l += nt) st[tile_global<V>(base, l, hdr)] = s[swz(l, tag)];
-        if (COHERENT) __threadfence();  // the stores are visible device-wide before the tile is marked done
         __syncthreads();
     }
+}
+
+// Plain (synchronous) tile load and store.  COHERENT loads bypass L1 (the
+// tile may have been written by another SM during the same launch).
+template <typename V, bool COHERENT>
+__device__ __forceinline__ void tile_load(const V* __restrict__ st, const TileHdr& hdr, const uint64_t* hoff,
+                                          uint64_t base, V* s) {
+    V* tag = nullptr;
+    const uint32_t T = 1u << hdr.tbits;
+    const int m = hdr.m;
+    for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) {
+        const V* src = &st[tile_global(base, l, m, hoff)];
+        s[swz(l, tag)] = COHERENT ? ld_l2(src) : *src;
+    }
+    __syncthreads();
+}
+
+template <typename V>
+__device__ __forceinline__ void tile_store(V* __restrict__ st, const TileHdr& hdr, const uint64_t* hoff,
+                                           uint64_t base, const V* s) {
+    const V* tag = nullptr;
+    const uint32_t T = 1u << hdr.tbits;
+    const int m = hdr.m;
+    for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) st[tile_global(base, l, m, hoff)] = s[swz(l, (V*)tag)];
+}
+
+// Asynchronous tile load (cp.async, no register staging): the copies of one
+// call form one commit group.
+__device__ __forceinline__ void cp_async_amp(double2* dst, const double2* src) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_amp(float2* dst, const float2* src) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <typename V>
+__device__ __forceinline__ void tile_load_async(const V* __restrict__ st, const TileHdr& hdr, const uint64_t* hoff,
+                                                uint64_t base, V* s) {
+    V* tag = nullptr;
+    const uint32_t T = 1u << hdr.tbits;
+    const int m = hdr.m;
+    for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) cp_async_amp(&s[swz(l, tag)], &st[tile_global(base, l, m, hoff)]);
 }
 
 // Bytes of shared memory that hold a staged pass description.
@@ -355,12 +441,12 @@ __host__ __device__ inline size_t staged_bytes(int nops, int nsegs, int ncoef, s
 // shared memory when the host marked it `staged`; returns the pointers the
 // tile body reads.
 template <typename V>
-__device__ __forceinline__ void stage_pass(const TileHdr& hdr, unsigned char* smem, const TOp*& ops, const TSeg*& segs,
-                                           const typename CoefT<V>::C*& coef) {
+__device__ __forceinline__ void stage_pass(const TileHdr& hdr, unsigned char* smem, int nbuf, const TOp*& ops,
+                                           const TSeg*& segs, const typename CoefT<V>::C*& coef) {
     typedef typename CoefT<V>::C C;
     if (!hdr.staged) return;
     auto a16 = [](size_t x) { return (x + 15) / 16 * 16; };
-    unsigned char* p = smem + ((size_t)1 << hdr.tbits) * sizeof(V);
+    unsigned char* p = smem + (size_t)nbuf * ((size_t)1 << hdr.tbits) * sizeof(V);
     TOp* so = (TOp*)p;
     p += a16((size_t)hdr.nops * sizeof(TOp));
     TSeg* ss = (TSeg*)p;
@@ -381,35 +467,66 @@ __device__ __forceinline__ void stage_pass(const TileHdr& hdr, unsigned char* sm
     coef = sc;
 }
 
+// One pass over every tile.  Two tile buffers: while a CTA works on one
+// tile, the next tile it owns streams into the other buffer (cp.async), so
+// HBM traffic overlaps the arithmetic even with one CTA per SM.
 template <typename V, bool EXACT, int RB>
 __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
-    k_tile_pass(V* __restrict__ st, const TileHdr hdr, const TOp* __restrict__ gops, const TSeg* __restrict__ gsegs,
+    k_tile_pass(V* __restrict__ st, const TileHdr phdr, const TOp* __restrict__ gops, const TSeg* __restrict__ gsegs,
                 const typename CoefT<V>::C* __restrict__ gcoef) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ TileHdr hdr;  // indexed with run-time subscripts: keep it out of the parameter space
+    if (threadIdx.x == 0) hdr = phdr;
+    __syncthreads();
     const TOp* ops = gops;
     const TSeg* segs = gsegs;
     const typename CoefT<V>::C* coef = gcoef;
-    stage_pass<V>(hdr, smem_raw, ops, segs, coef);
-    for (uint64_t t = blockIdx.x; t < hdr.ntiles; t += gridDim.x)
-        tile_body<V, EXACT, RB, false>(st, hdr, t, ops, segs, coef, (V*)smem_raw);
+    __shared__ uint64_t hoff[1 << kMaxScatterBits];
+    stage_pass<V>(hdr, smem_raw, 2, ops, segs, coef);
+    tile_offsets(hdr, hoff);
+    const uint32_t T = 1u << hdr.tbits;
+    V* cur = (V*)smem_raw;
+    V* nxt = cur + T;
+    uint64_t t = blockIdx.x;
+    if (t < hdr.ntiles) tile_load_async<V>(st, hdr, hoff, insert_zeros(t, hdr.tb, hdr.tbits), cur);
+    cp_async_commit();
+    for (; t < hdr.ntiles; t += gridDim.x) {
+        const uint64_t tn = t + gridDim.x;
+        if (tn < hdr.ntiles) tile_load_async<V>(st, hdr, hoff, insert_zeros(tn, hdr.tb, hdr.tbits), nxt);
+        cp_async_commit();
+        cp_async_wait<1>();  // this thread's copies into `cur` have landed
+        __syncthreads();     // ... and every other thread's
+        const uint64_t base = insert_zeros(t, hdr.tb, hdr.tbits);
+        tile_compute<V, EXACT, RB>(hdr, base, ops, segs, coef, cur);
+        tile_store<V>(st, hdr, hoff, base, cur);
+        __syncthreads();  // `cur` is read out before it receives tile t + 2 * gridDim.x
+        V* tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+    }
+    cp_async_wait<0>();
 }
 
 // ------------------------------------------------------------- batches
 //
 // Many circuits (uneven sizes) in one persistent launch.  Every (circuit,
-// pass) is an entry; its tiles are jobs.  Entries are ordered level-major
-// (every circuit's pass 0, then every circuit's pass 1, ...), jobs are taken
-// from a global counter in that order, and a job first waits until all tiles
-// of its circuit's previous passes are done (`done[circuit]` counts finished
-// tiles).  A job only waits on jobs taken before it, by CTAs that are
-// running, so the waits end; each wait is still bounded in time, and a wait
-// that gives up sets `*err` and lets the job (and its circuit) fail.
+// pass) is an entry; its tiles are cut into chunks of consecutive tiles.
+// Entries are ordered level-major (every circuit's pass 0, then every
+// circuit's pass 1, ...), chunks are taken from a global counter in that
+// order, and a chunk first waits until all tiles of its circuit's previous
+// passes are done (`done[circuit]` counts finished tiles).  A chunk only
+// waits on chunks taken before it, by CTAs that are running, so the waits
+// end; each wait is still bounded in time, and a wait that gives up sets
+// `*err` (the host reports the batch as failed).
 struct BatchEntry {
     TileHdr hdr;
-    uint64_t state;      // device address of the circuit's state
-    uint64_t job_start;  // first job id of this entry
+    uint64_t state;  // device address of the circuit's state
     uint32_t circuit, pass;
     int32_t ops_off, segs_off, coef_off, pad;
+};
+
+struct BatchChunk {
+    uint32_t entry, tile0, ntile, pad;
 };
 
 __device__ __forceinline__ uint64_t global_ns() {
@@ -422,35 +539,32 @@ constexpr uint64_t kBatchWaitNs = 2000000000ull;  // 2 s
 
 template <typename V, bool EXACT, int RB>
 __global__ void __launch_bounds__(kTileThreads, 1)
-    k_batch_tiles(const BatchEntry* __restrict__ entries, int nentries, uint64_t njobs,
+    k_batch_tiles(const BatchEntry* __restrict__ entries, const BatchChunk* __restrict__ chunks, uint64_t nchunks,
                   unsigned long long* __restrict__ next, unsigned int* __restrict__ done, int* __restrict__ err,
                   const TOp* __restrict__ ops, const TSeg* __restrict__ segs,
-                  const typename CoefT<V>::C* __restrict__ coef) {
+                  const typename CoefT<V>::C* __restrict__ coef, uint64_t wait_ns) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long sj;
-    __shared__ int se, sskip;
+    __shared__ int sskip;
+    __shared__ uint64_t hoff[1 << kMaxScatterBits];
+    int staged = -1;  // entry whose pass description and offsets are in shared memory
+    const TOp* o = ops;
+    const TSeg* sgs = segs;
+    const typename CoefT<V>::C* cf = coef;
     for (;;) {
         if (threadIdx.x == 0) sj = atomicAdd(next, 1ull);
         __syncthreads();
-        const uint64_t j = sj;
-        if (j >= njobs) break;
+        const uint64_t c = sj;
+        if (c >= nchunks) break;
+        const BatchChunk ch = chunks[c];
+        const BatchEntry& e = entries[ch.entry];
         if (threadIdx.x == 0) {
-            int lo = 0, hi = nentries - 1;  // last entry with job_start <= j
-            while (lo < hi) {
-                int mid = (lo + hi + 1) >> 1;
-                if (entries[mid].job_start <= j)
-                    lo = mid;
-                else
-                    hi = mid - 1;
-            }
-            se = lo;
-            const BatchEntry& e = entries[lo];
             const unsigned int need = (unsigned int)(e.pass * e.hdr.ntiles);
             int skip = 0;
             if (need > 0) {
                 const uint64_t t0 = global_ns();
                 while (*((volatile unsigned int*)&done[e.circuit]) < need) {
-                    if (global_ns() - t0 > kBatchWaitNs) {
+                    if (global_ns() - t0 > wait_ns) {
                         atomicExch(err, 1);
                         skip = 1;
                         break;
@@ -462,17 +576,28 @@ __global__ void __launch_bounds__(kTileThreads, 1)
             sskip = skip;
         }
         __syncthreads();
-        const BatchEntry& e = entries[se];
         if (!sskip) {
-            const TOp* o = ops + e.ops_off;
-            const TSeg* sgs = segs + e.segs_off;
-            const typename CoefT<V>::C* cf = coef + e.coef_off;
-            stage_pass<V>(e.hdr, smem_raw, o, sgs, cf);
-            tile_body<V, EXACT, RB, true>((V*)e.state, e.hdr, j - e.job_start, o, sgs, cf, (V*)smem_raw);
+            if ((int)ch.entry != staged) {
+                o = ops + e.ops_off;
+                sgs = segs + e.segs_off;
+                cf = coef + e.coef_off;
+                stage_pass<V>(e.hdr, smem_raw, 1, o, sgs, cf);
+                tile_offsets(e.hdr, hoff);
+                staged = (int)ch.entry;
+            }
+            for (uint32_t t = ch.tile0; t < ch.tile0 + ch.ntile; t++) {
+                const uint64_t base = insert_zeros(t, e.hdr.tb, e.hdr.tbits);
+                tile_load<V, true>((V*)e.state, e.hdr, hoff, base, (V*)smem_raw);
+                tile_compute<V, EXACT, RB>(e.hdr, base, o, sgs, cf, (V*)smem_raw);
+                tile_store<V>((V*)e.state, e.hdr, hoff, base, (V*)smem_raw);
+                __syncthreads();
+            }
+            __threadfence();  // the stores are visible device-wide before the tiles are counted done
+            __syncthreads();
         }
         if (threadIdx.x == 0) {
             __threadfence();
-            atomicAdd(&done[e.circuit], 1u);
+            atomicAdd(&done[e.circuit], ch.ntile);
         }
         __syncthreads();
     }
@@ -501,6 +626,9 @@ constexpr int max_reg_bits() {
 // tile bits fit in rb register bits share a register segment; a dense op on
 // three or more targets is a wide segment of its own.
 static void plan_segments(PassPlan& pp, int rb) {
+    // every non-wide op must fit one register segment
+    for (const TOp& op : pp.ops)
+        if (op.cls != GC_DIAG && !(op.cls == GC_DENSE && op.k >= 3)) rb = std::max(rb, (int)op.k);
     pp.rb = rb;
     pp.segs.clear();
     const int tbits = pp.hdr.tbits;
@@ -609,7 +737,9 @@ static void plan_passes(const std::vector<LGate>& prog, uint32_t nbits, int tbit
                 op.tg[q] = (int8_t)g->tb[q];
                 op.tl[q] = (int8_t)local_of(g->tb[q]);
                 if (op.tl[q] < 0) op.all_local = 0;
+                op.ts[q] = op.tl[q];
             }
+            std::sort(op.ts, op.ts + g->k);
             for (int c = 0; c < g->nc; c++) {
                 int lb = local_of(g->cb[c]);
                 if (lb >= 0) {
@@ -639,51 +769,52 @@ static void plan_passes(const std::vector<LGate>& prog, uint32_t nbits, int tbit
 
 // ------------------------------------------------------------- fusion
 
-// Apply an LGate to a small dense vector over the block's local bits
-// (host, FP64) -- used to multiply gates into fused block matrices.
-static void host_apply(const LGate& g, const std::vector<int>& local_of_bit, std::vector<Cx>& v) {
-    const size_t n = v.size();
-    auto lb = [&](int gb) { return local_of_bit[gb]; };
+// Left-multiply a block matrix (d x d over the block's local bits, row
+// index = local output index) by an LGate whose bits are all block bits:
+// M <- G M, column by column (host, FP64).
+static void apply_gate_to_block(const LGate& g, const int* local_of_bit, size_t d, Cx* M) {
     uint64_t cm = 0, cvv = 0;
     for (int c = 0; c < g.nc; c++) {
-        cm |= (uint64_t)1 << lb(g.cb[c]);
-        if (g.cv[c]) cvv |= (uint64_t)1 << lb(g.cb[c]);
+        cm |= (uint64_t)1 << local_of_bit[g.cb[c]];
+        if (g.cv[c]) cvv |= (uint64_t)1 << local_of_bit[g.cb[c]];
     }
-    uint64_t tmask = 0;
-    for (int q = 0; q < g.k; q++) tmask |= (uint64_t)1 << lb(g.tb[q]);
     const int nl = 1 << g.k;
-    std::vector<Cx> old(nl);
-    for (size_t b = 0; b < n; b++) {
+    uint64_t tmask = 0;
+    size_t sc[1 << kMaxTargets];
+    for (int l = 0; l < nl; l++) {
+        size_t o = 0;
+        for (int q = 0; q < g.k; q++)
+            if ((l >> q) & 1) o |= (size_t)1 << local_of_bit[g.tb[q]];
+        sc[l] = o;
+    }
+    for (int q = 0; q < g.k; q++) tmask |= (uint64_t)1 << local_of_bit[g.tb[q]];
+    Cx old[1 << kMaxTargets];
+    for (size_t b = 0; b < d; b++) {
         if (b & tmask) continue;
         if ((b & cm) != cvv) continue;
-        std::vector<size_t> idx(nl);
-        for (int l = 0; l < nl; l++) {
-            size_t o = b;
-            for (int q = 0; q < g.k; q++)
-                if ((l >> q) & 1) o |= (size_t)1 << lb(g.tb[q]);
-            idx[l] = o;
-            old[l] = v[o];
-        }
-        if (g.cls == GC_X) {
-            v[idx[0]] = old[1];
-            v[idx[1]] = old[0];
-        } else if (g.cls == GC_SWAP) {
-            v[idx[1]] = old[2];
-            v[idx[2]] = old[1];
-        } else if (g.cls == GC_DIAG) {
-            for (int l = 0; l < nl; l++) {
-                Cx a = old[l], d = g.m[l];
-                v[idx[l]] = Cx{a.re * d.re - a.im * d.im, a.re * d.im + a.im * d.re};
-            }
-        } else {
-            for (int r = 0; r < nl; r++) {
-                Cx acc{0, 0};
-                for (int c = 0; c < nl; c++) {
-                    Cx m = g.m[(size_t)r * nl + c], x = old[c];
-                    acc.re += m.re * x.re - m.im * x.im;
-                    acc.im += m.re * x.im + m.im * x.re;
+        for (size_t col = 0; col < d; col++) {
+            for (int l = 0; l < nl; l++) old[l] = M[(b | sc[l]) * d + col];
+            if (g.cls == GC_X) {
+                M[(b | sc[0]) * d + col] = old[1];
+                M[(b | sc[1]) * d + col] = old[0];
+            } else if (g.cls == GC_SWAP) {
+                M[(b | sc[1]) * d + col] = old[2];
+                M[(b | sc[2]) * d + col] = old[1];
+            } else if (g.cls == GC_DIAG) {
+                for (int l = 0; l < nl; l++) {
+                    const Cx a = old[l], e = g.m[l];
+                    M[(b | sc[l]) * d + col] = Cx{a.re * e.re - a.im * e.im, a.re * e.im + a.im * e.re};
                 }
-                v[idx[r]] = acc;
+            } else {
+                for (int r = 0; r < nl; r++) {
+                    Cx acc{0, 0};
+                    for (int c = 0; c < nl; c++) {
+                        const Cx m = g.m[(size_t)r * nl + c], x = old[c];
+                        acc.re += m.re * x.re - m.im * x.im;
+                        acc.im += m.re * x.im + m.im * x.re;
+                    }
+                    M[(b | sc[r]) * d + col] = acc;
+                }
             }
         }
     }
@@ -724,15 +855,10 @@ static void block_extend(Block& b, const std::vector<int>& add) {
 }
 
 static void block_mul_gate(Block& b, const LGate& g, uint32_t nbits) {
-    std::vector<int> local_of_bit(nbits, -1);
+    int local_of_bit[64];
+    for (uint32_t i = 0; i < nbits && i < 64; i++) local_of_bit[i] = -1;
     for (size_t i = 0; i < b.bits.size(); i++) local_of_bit[b.bits[i]] = (int)i;
-    size_t d = (size_t)1 << b.bits.size();
-    std::vector<Cx> col(d);
-    for (size_t c = 0; c < d; c++) {
-        for (size_t r = 0; r < d; r++) col[r] = b.m[r * d + c];
-        host_apply(g, local_of_bit, col);
-        for (size_t r = 0; r < d; r++) b.m[r * d + c] = col[r];
-    }
+    apply_gate_to_block(g, local_of_bit, (size_t)1 << b.bits.size(), b.m.data());
 }
 
 // Greedy fusion into blocks of at most k qubits.  A gate joins the most
@@ -801,30 +927,41 @@ static void fuse_blocks(const std::vector<LGate>& prog, uint32_t nbits, int k, s
 
 // ------------------------------------------------------------ execution
 
+// Persistent launch: as many CTAs as fit on the SMs at once (each loops
+// over its tiles with the next one in flight), never more than tiles.
 template <typename V, bool EXACT, int RB>
-static int launch_tile_rb(unsigned grid, unsigned threads, size_t smem, cudaStream_t s, V* st, const TileHdr& hdr,
+static int launch_tile_rb(int num_sms, unsigned threads, size_t smem, cudaStream_t s, V* st, const TileHdr& hdr,
                           const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef) {
     static bool attr = false;
     if (!attr) {
+        int dev = 0, optin = 0;
+        YAO_CUDA(cudaGetDevice(&dev));
+        YAO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        cudaFuncAttributes fa;
+        YAO_CUDA(cudaFuncGetAttributes(&fa, k_tile_pass<V, EXACT, RB>));
         YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      160 * 1024));
+                                      optin - (int)fa.sharedSizeBytes));
         YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                       cudaSharedmemCarveoutMaxShared));
         attr = true;
     }
+    int per_sm = 0;
+    YAO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_pass<V, EXACT, RB>, (int)threads, smem));
+    if (per_sm < 1) return fail(YAO_ERR_UNSUPPORTED, "tile pass does not fit on an SM");
+    const unsigned grid = (unsigned)std::min<uint64_t>(hdr.ntiles, (uint64_t)per_sm * (uint64_t)num_sms);
     k_tile_pass<V, EXACT, RB><<<grid, threads, smem, s>>>(st, hdr, ops, segs, coef);
     return YAO_OK;
 }
 
 template <typename V, bool EXACT>
-static int launch_tile(int rb, unsigned grid, unsigned threads, size_t smem, cudaStream_t s, V* st,
+static int launch_tile(int rb, int num_sms, unsigned threads, size_t smem, cudaStream_t s, V* st,
                        const TileHdr& hdr, const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef) {
     switch (rb) {
-    case 1: return launch_tile_rb<V, EXACT, 1>(grid, threads, smem, s, st, hdr, ops, segs, coef);
-    case 2: return launch_tile_rb<V, EXACT, 2>(grid, threads, smem, s, st, hdr, ops, segs, coef);
-    case 3: return launch_tile_rb<V, EXACT, 3>(grid, threads, smem, s, st, hdr, ops, segs, coef);
+    case 1: return launch_tile_rb<V, EXACT, 1>(num_sms, threads, smem, s, st, hdr, ops, segs, coef);
+    case 2: return launch_tile_rb<V, EXACT, 2>(num_sms, threads, smem, s, st, hdr, ops, segs, coef);
+    case 3: return launch_tile_rb<V, EXACT, 3>(num_sms, threads, smem, s, st, hdr, ops, segs, coef);
     case 4:
-        if constexpr (sizeof(V) == 8) return launch_tile_rb<V, EXACT, 4>(grid, threads, smem, s, st, hdr, ops, segs, coef);
+        if constexpr (sizeof(V) == 8) return launch_tile_rb<V, EXACT, 4>(num_sms, threads, smem, s, st, hdr, ops, segs, coef);
         break;
     default: break;
     }
@@ -856,24 +993,253 @@ static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
     YAO_CUDA(cudaMemcpyAsync((char*)dbuf + cb_off, hc.data(), cb, cudaMemcpyHostToDevice, ctx->stream));
     TileHdr hdr = pp.hdr;
     hdr.ncoef = (int32_t)hc.size();
+    if (hdr.tbits - hdr.m > kMaxScatterBits) return fail(YAO_ERR_UNSUPPORTED, "tile has too many scattered bits");
     const size_t tile_bytes = ((size_t)1 << hdr.tbits) * sizeof(V);
     const size_t stg = staged_bytes(hdr.nops, hdr.nsegs, hdr.ncoef, sizeof(C));
     hdr.staged = stg <= kMaxStagedBytes ? 1 : 0;
-    const size_t smem = tile_bytes + (hdr.staged ? stg : 0);
+    const size_t smem = 2 * tile_bytes + (hdr.staged ? stg : 0);
     const unsigned threads = (unsigned)(((uint32_t)1 << pp.hdr.tbits) >> pp.rb);
-    const unsigned grid = (unsigned)std::min<uint64_t>(pp.hdr.ntiles, (uint64_t)ctx->num_sms * 4);
     const TOp* dops = (const TOp*)dbuf;
     const TSeg* dsegs = (const TSeg*)((char*)dbuf + sb_off);
     const C* dcoef = (const C*)((char*)dbuf + cb_off);
     {
         ProfScope prof(ctx, EXACT ? "tile_pass_exact" : "tile_pass_fused",
                        (double)pp.hdr.ntiles * (double)((uint64_t)1 << pp.hdr.tbits) * 2.0 * sizeof(V));
-        int s = launch_tile<V, EXACT>(pp.rb, grid, threads, smem, ctx->stream, st, hdr, dops, dsegs, dcoef);
+        int s = launch_tile<V, EXACT>(pp.rb, ctx->num_sms, threads, smem, ctx->stream, st, hdr, dops, dsegs, dcoef);
         if (s) return s;
     }
     ctx->launches++;
     YAO_CUDA(cudaGetLastError());
     YAO_CUDA(cudaFreeAsync(dbuf, ctx->stream));
+    return YAO_OK;
+}
+
+// Execution choice of a TILED / FUSED run: fusion width k (FUSED), tile
+// bits and register bits per thread.
+struct TileConfig {
+    int k = 0;
+    int tbits = 0;
+    int rb = 0;
+};
+
+template <typename V>
+static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, const std::vector<LGate>& prog,
+                           int32_t mode, const TileConfig& cfg) {
+    std::vector<LGate> work;
+    const bool exact = (mode == YAO_MODE_TILED) && sizeof(V) == 16;
+    if (mode == YAO_MODE_FUSED)
+        fuse_blocks(prog, nbits, std::min(cfg.k, kMaxTargets), work);
+    else
+        work = prog;
+    std::vector<PassPlan> passes;
+    plan_passes(work, nbits, cfg.tbits, passes);
+    for (PassPlan& pp : passes)
+        if (!pp.single) {
+            // at most kTileThreads threads per tile
+            const int tb = (int)pp.hdr.tbits;
+            const int rb = std::max(tb - 9, std::min(cfg.rb, tb));
+            plan_segments(pp, std::min(rb, max_reg_bits<V>()));
+        }
+    for (const PassPlan& pp : passes) {
+        int s;
+        if (pp.single)
+            s = launch_gate(ctx, st, precision, nbits, pp.gate);
+        else if (exact)
+            s = run_pass<V, true>(ctx, st, nbits, pp);
+        else
+            s = run_pass<V, false>(ctx, st, nbits, pp);
+        if (s) return s;
+    }
+    return YAO_OK;
+}
+
+// ------------------------------------------------------------ autotuner
+//
+// The tile shape (tile bits, register bits) and, for FUSED with k = 0, the
+// fusion width are picked by timing candidates on the device: a prefix of
+// the program (at most 2^38 amplitude-gate updates, at least 64 gates) runs
+// on a scratch copy of the register for every candidate, and the fastest is
+// kept per (device, qubits, precision, mode, requested k).  Choices live in
+// memory and, when YAO_TUNE_CACHE names a file, in that file (one
+// "key k tbits rb" line per entry).  YAO_TILE_BITS / YAO_REG_BITS pin the
+// shape and YAO_AUTOTUNE=0 turns tuning off (defaults below).
+
+static std::mutex g_tune_mu;
+static std::map<std::string, TileConfig> g_tune;
+static bool g_tune_loaded = false;
+
+static std::string tune_key(int device, uint32_t nbits, int32_t prec, int32_t mode, int32_t kreq, const char* what) {
+    char b[128];
+    snprintf(b, sizeof(b), "%s/dev%d/n%u/p%d/m%d/k%d", what, device, nbits, prec, mode, kreq);
+    return b;
+}
+
+static void tune_load_locked() {
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* path = getenv("YAO_TUNE_CACHE");
+    if (!path || !*path) return;
+    FILE* f = fopen(path, "r");
+    if (!f) return;
+    char key[128];
+    TileConfig c;
+    while (fscanf(f, "%127s %d %d %d", key, &c.k, &c.tbits, &c.rb) == 4) g_tune[key] = c;
+    fclose(f);
+}
+
+static void tune_store_locked() {
+    const char* path = getenv("YAO_TUNE_CACHE");
+    if (!path || !*path) return;
+    FILE* f = fopen(path, "w");
+    if (!f) return;
+    for (const auto& kv : g_tune) fprintf(f, "%s %d %d %d\n", kv.first.c_str(), kv.second.k, kv.second.tbits, kv.second.rb);
+    fclose(f);
+}
+
+static bool env_int(const char* name, int lo, int hi, int* out) {
+    const char* e = getenv(name);
+    if (!e || !*e) return false;
+    int v = atoi(e);
+    if (v < lo || v > hi) return false;
+    *out = v;
+    return true;
+}
+
+template <typename V>
+static TileConfig default_config(int32_t mode, int32_t kreq) {
+    TileConfig c;
+    c.k = mode == YAO_MODE_FUSED ? (kreq > 0 ? std::min(kreq, kMaxTargets) : 4) : 0;
+    c.tbits = 11;
+    c.rb = 2;
+    env_int("YAO_TILE_BITS", 6, sizeof(V) == 16 ? 12 : 13, &c.tbits);
+    env_int("YAO_REG_BITS", 1, max_reg_bits<V>(), &c.rb);
+    return c;
+}
+
+template <typename V>
+static void tile_candidates(uint32_t nbits, std::vector<TileConfig>& out) {
+    const int tmax = sizeof(V) == 16 ? 12 : 13;
+    std::set<std::pair<int, int>> seen;
+    for (int tb = tmax - 2; tb <= tmax; tb++)
+        for (int rb = 2; rb <= max_reg_bits<V>(); rb++) {
+            const int etb = std::min<int>(tb, (int)nbits);
+            if (etb - rb > 9) continue;  // 2^(etb - rb) threads: at most kTileThreads
+            if (!seen.insert({etb, rb}).second) continue;
+            TileConfig c;
+            c.tbits = tb;
+            c.rb = rb;
+            out.push_back(c);
+        }
+}
+
+// Time every candidate on a scratch copy of the state; *best receives the
+// fastest (left at the default when no scratch memory is available).
+template <typename V>
+static int tune_program(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t kreq,
+                        TileConfig* best, double* best_ms) {
+    *best = default_config<V>(mode, kreq);
+    *best_ms = -1.0;
+    const uint32_t n = r->nbits;
+    const size_t cap = std::max<size_t>(64, (size_t)1 << std::max(0, 38 - (int)n));
+    std::vector<LGate> sample(prog.begin(), prog.begin() + std::min(prog.size(), cap));
+    if (sample.empty()) return YAO_OK;
+    const size_t bytes = ((size_t)1 << n) * sizeof(V);
+    V* scratch = nullptr;
+    if (cudaMallocAsync((void**)&scratch, bytes, ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return YAO_OK;
+    }
+    YAO_CUDA(cudaMemcpyAsync(scratch, r->d, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    const bool prof = ctx->prof;
+    ctx->prof = false;
+    cudaEvent_t a, b;
+    YAO_CUDA(cudaEventCreate(&a));
+    YAO_CUDA(cudaEventCreate(&b));
+    int st = YAO_OK;
+    auto timed = [&](const TileConfig& c, float* ms) -> int {
+        YAO_CUDA(cudaEventRecord(a, ctx->stream));
+        int s = run_program_cfg<V>(ctx, scratch, n, r->precision, sample, mode, c);
+        if (s) return s;
+        YAO_CUDA(cudaEventRecord(b, ctx->stream));
+        YAO_CUDA(cudaEventSynchronize(b));
+        YAO_CUDA(cudaEventElapsedTime(ms, a, b));
+        return YAO_OK;
+    };
+    std::vector<TileConfig> shapes;
+    tile_candidates<V>(n, shapes);
+    TileConfig cur = *best;
+    float ms = 0.f, bms = 0.f;
+    // warm-up (first launches of each kernel variant carry one-time costs)
+    for (const TileConfig& sc : shapes) {
+        TileConfig c = cur;
+        c.tbits = sc.tbits;
+        c.rb = sc.rb;
+        if ((st = timed(c, &ms))) break;
+    }
+    bool have = false;
+    for (size_t i = 0; !st && i < shapes.size(); i++) {
+        TileConfig c = cur;
+        c.tbits = shapes[i].tbits;
+        c.rb = shapes[i].rb;
+        if ((st = timed(c, &ms))) break;
+        if (!have || ms < bms) {
+            bms = ms;
+            *best = c;
+            have = true;
+        }
+    }
+    if (!st && mode == YAO_MODE_FUSED && kreq <= 0) {
+        const TileConfig shape = *best;
+        for (int k = 2; k <= kMaxTargets; k++) {
+            if (k == shape.k) continue;
+            TileConfig c = shape;
+            c.k = k;
+            if ((st = timed(c, &ms))) break;
+            if (ms < bms) {
+                bms = ms;
+                *best = c;
+            }
+        }
+    }
+    ctx->prof = prof;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFreeAsync(scratch, ctx->stream);
+    if (!st) *best_ms = bms;
+    return st;
+}
+
+template <typename V>
+static int choose_config(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t kreq,
+                         bool force, TileConfig* out) {
+    *out = default_config<V>(mode, kreq);
+    if (!force) {
+        int pinned = 0;
+        if (env_int("YAO_TILE_BITS", 6, 13, &pinned) || env_int("YAO_REG_BITS", 1, 4, &pinned)) return YAO_OK;
+        const char* at = getenv("YAO_AUTOTUNE");
+        if (at && at[0] == '0') return YAO_OK;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    YAO_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return YAO_OK;  // no synchronising while a graph is captured
+    const std::string key = tune_key(ctx->device, r->nbits, r->precision, mode, kreq, "prog");
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        tune_load_locked();
+        auto it = g_tune.find(key);
+        if (it != g_tune.end() && !force) {
+            *out = it->second;
+            return YAO_OK;
+        }
+    }
+    double ms;
+    int s = tune_program<V>(ctx, r, prog, mode, kreq, out, &ms);
+    if (s) return s;
+    if (ms >= 0) {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        g_tune[key] = *out;
+        tune_store_locked();
+    }
     return YAO_OK;
 }
 
@@ -887,49 +1253,10 @@ static int run_program_t(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32
         }
         return YAO_OK;
     }
-    // tile size: 2^12 complex128 (64 KiB) or 2^13 complex64 (64 KiB) per CTA
-    // tile: 2^tbits amplitudes per CTA (shared memory = 2^tbits * sizeof(V));
-    // YAO_TILE_BITS overrides the default for tuning runs
-    int tbits = sizeof(V) == 16 ? 12 : 13;
-    if (const char* e = getenv("YAO_TILE_BITS")) {
-        int v = atoi(e);
-        if (v >= 6 && v <= (sizeof(V) == 16 ? 12 : 13)) tbits = v;
-    }
-    std::vector<LGate> work;
-    bool exact = (mode == YAO_MODE_TILED) && sizeof(V) == 16;
-    if (mode == YAO_MODE_FUSED) {
-        int kk = k > 0 ? std::min(k, kMaxTargets) : 5;
-        fuse_blocks(prog, r->nbits, kk, work);
-    } else {
-        work = prog;
-    }
-    std::vector<PassPlan> passes;
-    plan_passes(work, r->nbits, tbits, passes);
-    // register bits: 3 (8 amplitudes per thread) unless YAO_REG_BITS says
-    // otherwise, more only when the tile would need more than kTileThreads
-    // threads
-    int rb_pref = 3;
-    if (const char* e = getenv("YAO_REG_BITS")) {
-        int v = atoi(e);
-        if (v >= 1 && v <= 4) rb_pref = v;
-    }
-    for (PassPlan& pp : passes)
-        if (!pp.single) {
-            int tb = (int)pp.hdr.tbits;
-            int rb = std::max(tb - 9, std::min(rb_pref, tb));
-            plan_segments(pp, std::min(rb, max_reg_bits<V>()));
-        }
-    for (const PassPlan& pp : passes) {
-        int s;
-        if (pp.single)
-            s = launch_gate(ctx, st, r->precision, r->nbits, pp.gate);
-        else if (exact)
-            s = run_pass<V, true>(ctx, st, r->nbits, pp);
-        else
-            s = run_pass<V, false>(ctx, st, r->nbits, pp);
-        if (s) return s;
-    }
-    return YAO_OK;
+    TileConfig cfg;
+    int s = choose_config<V>(ctx, r, prog, mode, k, false, &cfg);
+    if (s) return s;
+    return run_program_cfg<V>(ctx, st, r->nbits, r->precision, prog, mode, cfg);
 }
 
 int launch_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k) {
@@ -937,37 +1264,69 @@ int launch_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mod
     return run_program_t<float2>(ctx, r, prog, mode, k);
 }
 
+int autotune_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k, int32_t out[3]) {
+    TileConfig c;
+    int s = r->precision == YAO_C128 ? choose_config<double2>(ctx, r, prog, mode, k, true, &c)
+                                     : choose_config<float2>(ctx, r, prog, mode, k, true, &c);
+    if (s) return s;
+    out[0] = c.k;
+    out[1] = c.tbits;
+    out[2] = c.rb;
+    return YAO_OK;
+}
+
 // ------------------------------------------------------------ batch host
 
 template <typename V>
 static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs, const std::vector<Reg*>& regs,
-                   int32_t mode, int32_t k) {
+                   int32_t mode, const TileConfig& cfg) {
     typedef typename CoefT<V>::C C;
-    const int tbits_cap = 12, rb = 3;
+    const int tbits_cap = std::min(cfg.tbits, 12), rb = 3;
+    const int k = cfg.k;
     const bool exact = mode == YAO_MODE_TILED && sizeof(V) == 16;
-    // plan every circuit
+    // plan every circuit (independent: spread over host threads)
     std::vector<std::vector<PassPlan>> plans(progs.size());
-    size_t maxpasses = 0;
-    for (size_t c = 0; c < progs.size(); c++) {
+    for (size_t c = 0; c < progs.size(); c++)
         if (regs[c]->nbits < 3) return fail(YAO_ERR_UNSUPPORTED, "batched circuits need at least 3 qubits");
+    std::vector<int> bad(progs.size(), 0);
+    auto plan_one = [&](size_t c) {
         std::vector<LGate> work;
         if (mode == YAO_MODE_FUSED)
-            fuse_blocks(*progs[c], regs[c]->nbits, k > 0 ? std::min(k, kMaxTargets) : 2, work);
+            fuse_blocks(*progs[c], regs[c]->nbits, std::max(1, std::min(k, kMaxTargets)), work);
         else
             work = *progs[c];
         plan_passes(work, regs[c]->nbits, tbits_cap, plans[c]);
         for (PassPlan& pp : plans[c]) {
-            if (pp.single) return fail(YAO_ERR_UNSUPPORTED, "a gate of the batch does not fit a tile");
-            plan_segments(pp, rb);
+            if (pp.single) bad[c] = 1;
+            else if (pp.hdr.tbits - pp.hdr.m > kMaxScatterBits) bad[c] = 2;
+            else plan_segments(pp, rb);
         }
+    };
+    {
+        const size_t nth = std::max<size_t>(1, std::min<size_t>({(size_t)std::thread::hardware_concurrency(),
+                                                                  (size_t)32, progs.size() / 8 + 1}));
+        std::atomic<size_t> nextc(0);
+        auto worker = [&]() {
+            for (size_t c; (c = nextc.fetch_add(1)) < progs.size();) plan_one(c);
+        };
+        std::vector<std::thread> pool;
+        for (size_t t = 1; t < nth; t++) pool.emplace_back(worker);
+        worker();
+        for (std::thread& th : pool) th.join();
+    }
+    size_t maxpasses = 0;
+    for (size_t c = 0; c < progs.size(); c++) {
+        if (bad[c] == 1) return fail(YAO_ERR_UNSUPPORTED, "a gate of the batch does not fit a tile");
+        if (bad[c] == 2) return fail(YAO_ERR_UNSUPPORTED, "tile has too many scattered bits");
         maxpasses = std::max(maxpasses, plans[c].size());
     }
     // entries level-major, ops / segments / coefficients concatenated
     std::vector<BatchEntry> entries;
+    std::vector<BatchChunk> chunks;
     std::vector<TOp> ops;
     std::vector<TSeg> segs;
     std::vector<C> coef;
-    uint64_t njobs = 0;
+    size_t max_stg = 0;
     for (size_t level = 0; level < maxpasses; level++)
         for (size_t c = 0; c < progs.size(); c++) {
             if (level >= plans[c].size()) continue;
@@ -976,7 +1335,6 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
             memset(&e, 0, sizeof(e));
             e.hdr = pp.hdr;
             e.state = (uint64_t)(uintptr_t)regs[c]->d;
-            e.job_start = njobs;
             e.circuit = (uint32_t)c;
             e.pass = (uint32_t)level;
             e.ops_off = (int32_t)ops.size();
@@ -994,22 +1352,51 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
                 }
                 coef.push_back(cc);
             }
+            e.hdr.ncoef = (int32_t)pp.coef.size();
+            const size_t stg = staged_bytes(e.hdr.nops, e.hdr.nsegs, e.hdr.ncoef, sizeof(C));
+            e.hdr.staged = stg <= kMaxStagedBytes ? 1 : 0;
+            if (e.hdr.staged) max_stg = std::max(max_stg, stg);
+            // chunks of consecutive tiles: about 32 per pass of a large
+            // circuit, at most 16 tiles each
+            const uint32_t nt = (uint32_t)pp.hdr.ntiles;
+            const uint32_t per = std::max<uint32_t>(1, std::min<uint32_t>(16, nt / 32));
+            for (uint32_t t0 = 0; t0 < nt; t0 += per) {
+                BatchChunk ch;
+                ch.entry = (uint32_t)entries.size();
+                ch.tile0 = t0;
+                ch.ntile = std::min(per, nt - t0);
+                ch.pad = 0;
+                chunks.push_back(ch);
+            }
             entries.push_back(e);
-            njobs += pp.hdr.ntiles;
         }
-    if (njobs == 0) return YAO_OK;
+    if (chunks.empty()) return YAO_OK;
+    // YAO_TEST_BATCH_STALL=1 (failure-path test): circuit 0's second pass
+    // waits for a tile count that is never reached, with a 0.2 s limit, so
+    // the bounded wait runs out and the call reports YAO_ERR_TIMEOUT
+    uint64_t wait_ns = kBatchWaitNs;
+    if (const char* e = getenv("YAO_TEST_BATCH_STALL"))
+        if (e[0] == '1')
+            for (BatchEntry& be : entries)
+                if (be.circuit == 0 && be.pass == 1) {
+                    be.pass = 1u << 20;
+                    wait_ns = 200000000ull;
+                }
     if (coef.empty()) coef.resize(1);
     if (ops.empty()) ops.resize(1);
     if (segs.empty()) segs.resize(1);
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-    const size_t b_ent = al(entries.size() * sizeof(BatchEntry)), b_ops = al(ops.size() * sizeof(TOp)),
-                 b_seg = al(segs.size() * sizeof(TSeg)), b_coef = al(coef.size() * sizeof(C)),
+    const size_t b_ent = al(entries.size() * sizeof(BatchEntry)), b_chk = al(chunks.size() * sizeof(BatchChunk)),
+                 b_ops = al(ops.size() * sizeof(TOp)), b_seg = al(segs.size() * sizeof(TSeg)),
+                 b_coef = al(coef.size() * sizeof(C)),
                  b_ctr = al(sizeof(unsigned long long) + sizeof(int) + progs.size() * sizeof(unsigned int));
     char* buf = nullptr;
-    YAO_CUDA(cudaMallocAsync((void**)&buf, b_ent + b_ops + b_seg + b_coef + b_ctr, ctx->stream));
+    YAO_CUDA(cudaMallocAsync((void**)&buf, b_ent + b_chk + b_ops + b_seg + b_coef + b_ctr, ctx->stream));
     char* p = buf;
     BatchEntry* d_ent = (BatchEntry*)p;
     p += b_ent;
+    BatchChunk* d_chk = (BatchChunk*)p;
+    p += b_chk;
     TOp* d_ops = (TOp*)p;
     p += b_ops;
     TSeg* d_seg = (TSeg*)p;
@@ -1020,30 +1407,11 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
     int* d_err = (int*)(p + sizeof(unsigned long long));
     unsigned int* d_done = (unsigned int*)(p + sizeof(unsigned long long) + sizeof(int));
     YAO_CUDA(cudaMemcpyAsync(d_ent, entries.data(), entries.size() * sizeof(BatchEntry), cudaMemcpyHostToDevice, ctx->stream));
+    YAO_CUDA(cudaMemcpyAsync(d_chk, chunks.data(), chunks.size() * sizeof(BatchChunk), cudaMemcpyHostToDevice, ctx->stream));
     YAO_CUDA(cudaMemcpyAsync(d_ops, ops.data(), ops.size() * sizeof(TOp), cudaMemcpyHostToDevice, ctx->stream));
     YAO_CUDA(cudaMemcpyAsync(d_seg, segs.data(), segs.size() * sizeof(TSeg), cudaMemcpyHostToDevice, ctx->stream));
     YAO_CUDA(cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(C), cudaMemcpyHostToDevice, ctx->stream));
     YAO_CUDA(cudaStreamSynchronize(ctx->stream));
-    // every entry's description is staged in shared memory when the largest fits
-    size_t max_stg = 0;
-    std::vector<int32_t> ncoefs(entries.size());
-    {
-        // coefficient counts per entry (entries are laid out in order)
-        for (size_t i = 0; i < entries.size(); i++) {
-            int32_t end = (i + 1 < entries.size()) ? entries[i + 1].coef_off : (int32_t)coef.size();
-            ncoefs[i] = end - entries[i].coef_off;
-            max_stg = std::max(max_stg, staged_bytes(entries[i].hdr.nops, entries[i].hdr.nsegs, ncoefs[i], sizeof(C)));
-        }
-        const int st = max_stg <= kMaxStagedBytes ? 1 : 0;
-        for (size_t i = 0; i < entries.size(); i++) {
-            entries[i].hdr.ncoef = ncoefs[i];
-            entries[i].hdr.staged = st;
-        }
-        YAO_CUDA(cudaMemcpyAsync(d_ent, entries.data(), entries.size() * sizeof(BatchEntry), cudaMemcpyHostToDevice,
-                                 ctx->stream));
-        YAO_CUDA(cudaStreamSynchronize(ctx->stream));
-        if (!st) max_stg = 0;
-    }
     const size_t smem = ((size_t)1 << tbits_cap) * sizeof(V) + max_stg;
     auto kern = exact ? k_batch_tiles<V, true, 3> : k_batch_tiles<V, false, 3>;
     YAO_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1055,8 +1423,8 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
     cudaGraphExec_t exec = nullptr;
     YAO_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     cudaMemsetAsync(d_next, 0, b_ctr, ctx->stream);
-    kern<<<grid, kTileThreads, smem, ctx->stream>>>(d_ent, (int)entries.size(), njobs, d_next, d_done, d_err, d_ops,
-                                                    d_seg, d_coef);
+    kern<<<grid, kTileThreads, smem, ctx->stream>>>(d_ent, d_chk, (uint64_t)chunks.size(), d_next, d_done, d_err,
+                                                    d_ops, d_seg, d_coef, wait_ns);
     cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
     if (ce != cudaSuccess) return cuda_fail(ce, "capture of the batch launch");
     YAO_CUDA(cudaGraphInstantiate(&exec, graph, 0));
@@ -1073,15 +1441,144 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
     YAO_CUDA(cudaFreeAsync(buf, ctx->stream));
-    if (herr) return fail(YAO_ERR_TIMEOUT, "batched launch: a job waited too long for its circuit's previous pass");
+    if (herr) return fail(YAO_ERR_TIMEOUT, "batched launch: a chunk waited too long for its circuit's previous pass");
     return YAO_OK;
+}
+
+// Batch autotuner: tile bits (10..12) and, for FUSED with k = 0, the fusion
+// width (2..6), timed on up to 64 of the batch's circuits (evenly spaced)
+// run on scratch copies of their registers; kept per (device, largest
+// qubit count, precision, mode, requested k) like the single-circuit choice.
+template <typename V>
+static int tune_batch(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs, const std::vector<Reg*>& regs,
+                      int32_t mode, int32_t kreq, TileConfig* best, bool* tuned) {
+    *tuned = false;
+    const size_t ns = std::min<size_t>(64, regs.size());
+    std::vector<const std::vector<LGate>*> sp(ns);
+    std::vector<Reg> sr(ns);
+    std::vector<Reg*> srp(ns);
+    size_t total = 0;
+    for (size_t i = 0; i < ns; i++) {
+        const size_t c = i * regs.size() / ns;
+        sp[i] = progs[c];
+        sr[i] = *regs[c];
+        total += (regs[c]->bytes() + 255) / 256 * 256;
+    }
+    char* scratch = nullptr;
+    if (cudaMallocAsync((void**)&scratch, total, ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return YAO_OK;
+    }
+    size_t off = 0;
+    for (size_t i = 0; i < ns; i++) {
+        YAO_CUDA(cudaMemcpyAsync(scratch + off, sr[i].d, sr[i].bytes(), cudaMemcpyDeviceToDevice, ctx->stream));
+        sr[i].d = scratch + off;
+        srp[i] = &sr[i];
+        off += (sr[i].bytes() + 255) / 256 * 256;
+    }
+    const bool prof = ctx->prof;
+    ctx->prof = false;
+    cudaEvent_t a, b;
+    YAO_CUDA(cudaEventCreate(&a));
+    YAO_CUDA(cudaEventCreate(&b));
+    auto timed = [&](const TileConfig& c, float* ms) -> int {
+        YAO_CUDA(cudaEventRecord(a, ctx->stream));
+        int s = batch_t<V>(ctx, sp, srp, mode, c);
+        if (s) return s;
+        YAO_CUDA(cudaEventRecord(b, ctx->stream));
+        YAO_CUDA(cudaEventSynchronize(b));
+        YAO_CUDA(cudaEventElapsedTime(ms, a, b));
+        return YAO_OK;
+    };
+    int st = YAO_OK;
+    float ms = 0.f, bms = 0.f;
+    bool have = false;
+    TileConfig cur = *best;
+    for (int tb = 10; !st && tb <= 12; tb++) {
+        TileConfig c = cur;
+        c.tbits = tb;
+        if ((st = timed(c, &ms))) break;  // warm-up of this shape
+        if ((st = timed(c, &ms))) break;
+        if (!have || ms < bms) {
+            bms = ms;
+            *best = c;
+            have = true;
+        }
+    }
+    if (!st && mode == YAO_MODE_FUSED && kreq <= 0) {
+        const TileConfig shape = *best;
+        for (int k = 2; k <= kMaxTargets; k++) {
+            if (k == shape.k) continue;
+            TileConfig c = shape;
+            c.k = k;
+            if ((st = timed(c, &ms))) break;
+            if (ms < bms) {
+                bms = ms;
+                *best = c;
+            }
+        }
+    }
+    ctx->prof = prof;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFreeAsync(scratch, ctx->stream);
+    *tuned = !st;
+    return st;
+}
+
+template <typename V>
+static int batch_choose(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs, const std::vector<Reg*>& regs,
+                        int32_t mode, int32_t kreq, TileConfig* out) {
+    *out = default_config<V>(mode, kreq);
+    out->tbits = 12;
+    if (mode == YAO_MODE_FUSED && kreq <= 0) out->k = 2;
+    int pinned = 0;
+    if (env_int("YAO_TILE_BITS", 6, 12, &pinned)) {
+        out->tbits = pinned;
+        return YAO_OK;
+    }
+    const char* at = getenv("YAO_AUTOTUNE");
+    if (at && at[0] == '0') return YAO_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    YAO_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return YAO_OK;
+    uint32_t nmax = 0;
+    for (const Reg* r : regs) nmax = std::max(nmax, r->nbits);
+    const std::string key = tune_key(ctx->device, nmax, regs[0]->precision, mode, kreq, "batch");
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        tune_load_locked();
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+            *out = it->second;
+            return YAO_OK;
+        }
+    }
+    bool tuned = false;
+    int s = tune_batch<V>(ctx, progs, regs, mode, kreq, out, &tuned);
+    if (s) return s;
+    if (tuned) {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        g_tune[key] = *out;
+        tune_store_locked();
+    }
+    return YAO_OK;
+}
+
+template <typename V>
+static int batch_entry(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs, const std::vector<Reg*>& regs,
+                       int32_t mode, int32_t k) {
+    TileConfig cfg;
+    int s = batch_choose<V>(ctx, progs, regs, mode, k, &cfg);
+    if (s) return s;
+    return batch_t<V>(ctx, progs, regs, mode, cfg);
 }
 
 int launch_batch(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs, const std::vector<Reg*>& regs,
                  int32_t mode, int32_t k) {
     if (regs.empty()) return YAO_OK;
-    if (regs[0]->precision == YAO_C128) return batch_t<double2>(ctx, progs, regs, mode, k);
-    return batch_t<float2>(ctx, progs, regs, mode, k);
+    if (regs[0]->precision == YAO_C128) return batch_entry<double2>(ctx, progs, regs, mode, k);
+    return batch_entry<float2>(ctx, progs, regs, mode, k);
 }
 
 }  // namespace yao

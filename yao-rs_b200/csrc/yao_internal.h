@@ -179,6 +179,9 @@ struct DM {
 // All launchers enqueue on ctx->stream and return YAO_OK or an error.
 int launch_gate(Ctx* ctx, void* state, int32_t precision, uint32_t nbits, const LGate& g);
 int launch_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k);
+// Time TILED / FUSED candidates for this program and register (always
+// re-tunes); out = {k, tile bits, register bits}.
+int autotune_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k, int32_t out[3]);
 // Many circuits (one register each, same context and precision) in one
 // persistent, graph-captured launch (TILED or FUSED forms).
 int launch_batch(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs, const std::vector<Reg*>& regs,

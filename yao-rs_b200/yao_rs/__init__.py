@@ -13,7 +13,7 @@ from .circuit import (Circuit, PositionedAnnotation, PositionedChannel, Position
 from .gate import Gate
 from .noise import NoiseChannel
 from .operator import Op, OperatorPolynomial, OperatorString, op_matrix
-from .ops import (MeasureResult, PostProcess, apply, apply_inplace, batch_apply, expect_arrayreg, expect_dm, expect_grad_batch,
+from .ops import (MeasureResult, PostProcess, apply, apply_inplace, autotune, batch_apply, expect_arrayreg, expect_dm, expect_grad_batch,
                   expect_grad, measure_with_postprocess, probs)
 from .register import ArrayReg, DensityMatrix, Register, density_matrix_from_reg
 
@@ -21,7 +21,7 @@ __all__ = [
     "ArrayReg", "C64", "C128", "Circuit", "CircuitError", "DensityMatrix", "Gate", "MODE_FUSED", "MODE_PLAIN",
     "MODE_TILED", "MeasureResult", "NoiseChannel", "Op", "OperatorPolynomial", "OperatorString",
     "PositionedAnnotation", "PositionedChannel", "PositionedGate", "PostProcess", "Register", "YaoError",
-    "apply", "apply_inplace", "batch_apply", "channel", "context", "control", "density_matrix_from_reg",
+    "apply", "apply_inplace", "autotune", "batch_apply", "channel", "context", "control", "density_matrix_from_reg",
     "elements_array", "expect_arrayreg", "expect_dm", "expect_grad", "expect_grad_batch", "label", "launch_count",
     "measure_with_postprocess", "op_matrix", "probs", "put",
 ]

@@ -27,6 +27,14 @@ def apply(circuit, reg: ArrayReg, mode: int = A.MODE_PLAIN, k: int = 0) -> Array
     return out
 
 
+def autotune(circuit, reg: ArrayReg, mode: int = A.MODE_FUSED, k: int = 0) -> dict:
+    """Time the TILED / FUSED execution choices for this circuit on a scratch
+    copy of `reg` and keep the fastest for later calls; returns the choice."""
+    out = (C.c_int32 * 3)()
+    A.check(A.lib().yao_autotune(circuit.handle, reg.handle, mode, k, out))
+    return {"k": out[0], "tile_bits": out[1], "reg_bits": out[2]}
+
+
 def batch_apply(circuits, regs, mode: int = A.MODE_PLAIN, k: int = 0):
     cs = (C.c_void_p * max(1, len(circuits)))(*[c.handle for c in circuits])
     rs = (C.c_void_p * max(1, len(regs)))(*[r.handle for r in regs])
