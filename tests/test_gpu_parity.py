@@ -563,3 +563,31 @@ def test_batch_bounded_wait_reports_timeout(monkeypatch):
     Y.batch_apply(circuits, regs, Y.MODE_TILED)
     for c, s, r in zip(circuits, states, regs):
         assert maxdiff(r.state_vec(), O.apply_circuit(c, s)) == 0.0
+
+
+@pytest.mark.parametrize("n", [13, 16])
+def test_tensor_core_blocks(monkeypatch, n):
+    """Dense 5-qubit blocks of complex64 FUSED runs on the tensor cores
+    (3 x TF32 products, FP32 accumulation in tensor memory) agree with the
+    oracle to 1 - F <= 1e-6 and with the CUDA-core form to 1e-6 relative."""
+    rng = np.random.default_rng(500 + n)
+    c = layered_circuit(n, 6, seed=n)
+    psi = random_state(rng, n)
+    ref = O.apply_circuit(c, psi)
+    monkeypatch.setenv("YAO_TILE_BITS", "12")
+    monkeypatch.setenv("YAO_REG_BITS", "3")
+    outs = {}
+    from yao_rs import _abi as A
+    for tc in ("1", "0"):
+        monkeypatch.setenv("YAO_TC", tc)
+        r = Y.ArrayReg.from_vec(n, psi).to_precision(Y.C64)
+        A.profile(True)
+        Y.apply_inplace(c, r, Y.MODE_FUSED, 5)
+        kernels = {p["kernel"] for p in A.profile_report()}
+        A.profile(False)
+        assert ("tile_pass_tc" in kernels) == (tc == "1"), kernels
+        outs[tc] = r.state_vec().astype(np.complex128)
+        assert 1 - abs(np.vdot(ref, outs[tc])) ** 2 < 1e-6, tc
+    scale = np.max(np.abs(ref))
+    assert np.max(np.abs(outs["1"] - outs["0"])) < 1e-5 * scale
+    assert np.max(np.abs(outs["1"] - ref)) < 1e-5 * scale

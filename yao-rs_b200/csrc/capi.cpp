@@ -351,6 +351,7 @@ int yao_ctx_destroy(yao_ctx* c) {
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     if (c->scratch) cudaFree(c->scratch);
+    if (c->d_err) cudaFree(c->d_err);
     if (c->host_pinned) cudaFreeHost(c->host_pinned);
     cudaStreamDestroy(c->stream);
     delete c;

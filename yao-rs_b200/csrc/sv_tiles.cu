@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <set>
@@ -30,6 +31,7 @@
 #include <vector>
 
 #include "device_common.cuh"
+#include "tc_sm100.cuh"
 
 namespace yao {
 
@@ -42,6 +44,8 @@ struct TileHdr {
     uint64_t ntiles;
     int32_t ncoef;
     int32_t staged;  // op table, segments and coefficients are copied to shared memory
+    int32_t mma;     // some wide op of the pass runs on the tensor cores
+    int32_t pad;
 };
 
 struct TOp {
@@ -56,6 +60,8 @@ struct TOp {
     uint64_t active;         // DIAG: non-unit entries
     int32_t moff;            // first coefficient in the pass's coefficient array
     int32_t all_local;
+    int32_t mma;             // tensor-core op: offset of its operand matrices (floats), else -1
+    int32_t mpad;
 };
 static_assert(sizeof(TOp) % 8 == 0, "TOp is copied as 32-bit words and read as 64-bit fields");
 
@@ -253,12 +259,152 @@ __device__ __forceinline__ void reg2_at(int p0, int p1, V (&v)[1 << RB], const u
 __device__ __forceinline__ double2 ld_l2(const double2* p) { return __ldcg(p); }
 __device__ __forceinline__ float2 ld_l2(const float2* p) { return __ldcg(p); }
 
+// ------------------------------------------------------- tensor-core ops
+//
+// A dense 5-qubit block on complex64 data in a 4096-amplitude tile runs on
+// the tensor cores as one real GEMM: the tile's G = 128 groups are the rows
+// of X (K = 64 reals per group: re, im of local index 0, 1, ...), the block's
+// real form B (64 x 64: rows 2i, 2i+1 = re, im of output i) is the second
+// operand, D = X B^T (128 x 64, FP32) accumulates in tensor memory.  FP32
+// accuracy comes from three TF32 products, D = Xh Bh + Xh Bl + Xl Bh, where
+// Xh = tf32(X), Xl = X - Xh (and Bh / Bl likewise, prepared on the host).
+// Operands are K-major in the no-swizzle canonical layout: element (r, k) at
+// byte (r / 8) * 2048 + (k / 4) * 128 + (r % 8) * 16 + (k % 4) * 4.
+constexpr int kTcK = 5;                 // qubits of a tensor-core block
+constexpr int kTcTileBits = 12;         // tile of a tensor-core pass (2^12 complex64)
+constexpr int kTcRows = 128;            // groups per tile = MMA M
+constexpr int kTcN = 64;                // real outputs = MMA N
+constexpr int kTcKr = 64;               // real inputs = reduction length
+constexpr int kTcOpFloats = 2 * kTcN * kTcKr;  // Bh then Bl
+constexpr uint32_t kTcSbo = (kTcKr / 4) * 128;  // bytes between 8-row groups
+constexpr size_t kTcSmemBytes = 2 * (size_t)kTcRows * kTcKr * 4 + 2 * (size_t)kTcN * kTcKr * 4;  // Xh, Xl, Bh, Bl
+constexpr uint64_t kTcWaitNs = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ uint64_t global_ns_tc() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+struct TcCtx {
+    uint32_t tmem;       // accumulator (64 columns)
+    uint64_t* bar;       // MMA completion barrier
+    uint32_t phase;      // parity of the next completion
+    float* xh;           // operands in shared memory (1 KiB aligned)
+    float* xl;
+    float* bh;
+    float* bl;
+    const float* mmat;   // every tensor-core op's Bh, Bl of the pass (global)
+    int loaded;          // op offset whose B operands are in shared memory
+    int failed;          // a completion wait ran out (results of the pass are void)
+    int* err;
+};
+
+__device__ __forceinline__ uint32_t tc_off(uint32_t r, uint32_t k) {
+    return (r >> 3) * kTcSbo + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4;
+}
+
+template <typename V>
+__device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
+    if constexpr (sizeof(V) == 8) {
+        float2* t = (float2*)s;
+        const uint32_t nt = blockDim.x, tid = threadIdx.x;
+        __shared__ uint32_t co[1 << kTcK];  // tile offset of local index c
+        if (tid < (1u << kTcK)) {
+            uint32_t o = 0;
+#pragma unroll
+            for (int q = 0; q < kTcK; q++) o |= (uint32_t)((tid >> q) & 1) << op.tl[q];
+            co[tid] = o;
+        }
+        __syncthreads();
+        // 1. X: 128 groups x 16 pairs of local indices -> 16-byte chunks
+        for (uint32_t it = tid; it < (uint32_t)kTcRows * 16; it += nt) {
+            const uint32_t g = it & (kTcRows - 1), jp = it >> 7;
+            uint32_t b = g;
+#pragma unroll
+            for (int q = 0; q < kTcK; q++) b = ins0(b, op.ts[q]);
+            const float2 v0 = t[swz(b | co[2 * jp], (float2*)nullptr)];
+            const float2 v1 = t[swz(b | co[2 * jp + 1], (float2*)nullptr)];
+            const float4 x = make_float4(v0.x, v0.y, v1.x, v1.y);
+            const float4 h = make_float4(tc::to_tf32(x.x), tc::to_tf32(x.y), tc::to_tf32(x.z), tc::to_tf32(x.w));
+            const float4 l = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
+            const uint32_t off = tc_off(g, 4 * jp);
+            *(float4*)((char*)tc.xh + off) = h;
+            *(float4*)((char*)tc.xl + off) = l;
+        }
+        // 2. B: this op's operands (kept while consecutive tiles reuse them)
+        if (tc.loaded != op.mma) {
+            const float4* src = (const float4*)(tc.mmat + op.mma);
+            float4* dh = (float4*)tc.bh;
+            float4* dl = (float4*)tc.bl;
+            constexpr int n4 = kTcN * kTcKr / 4;
+            for (int i = tid; i < n4; i += nt) {
+                dh[i] = src[i];
+                dl[i] = src[n4 + i];
+            }
+            tc.loaded = op.mma;
+        }
+        tc::fence_proxy_async();
+        tc::fence_before_sync();
+        __syncthreads();
+        // 3. one thread issues the MMAs: 8 K-steps x 3 products
+        if (tid == 0) {
+            tc::fence_after_sync();
+            constexpr uint32_t idesc = tc::idesc_tf32(kTcRows, kTcN);
+            const uint32_t xh = tc::smem_u32(tc.xh), xl = tc::smem_u32(tc.xl);
+            const uint32_t bh = tc::smem_u32(tc.bh), bl = tc::smem_u32(tc.bl);
+#pragma unroll
+            for (int k8 = 0; k8 < kTcKr / 8; k8++) {
+                const uint32_t o = (uint32_t)k8 * 256;
+                tc::mma_tf32(tc.tmem, tc::smem_desc(xh + o, 128, kTcSbo), tc::smem_desc(bh + o, 128, kTcSbo), idesc,
+                             k8 > 0);
+                tc::mma_tf32(tc.tmem, tc::smem_desc(xh + o, 128, kTcSbo), tc::smem_desc(bl + o, 128, kTcSbo), idesc, 1);
+                tc::mma_tf32(tc.tmem, tc::smem_desc(xl + o, 128, kTcSbo), tc::smem_desc(bh + o, 128, kTcSbo), idesc, 1);
+            }
+            tc::commit(tc.bar);
+        }
+        // 4. every thread waits for completion (bounded)
+        bool done = false;
+        const uint64_t t0 = global_ns_tc();
+        while (!(done = tc::mbar_try_wait(tc.bar, tc.phase))) {
+            if (global_ns_tc() - t0 > kTcWaitNs) break;
+        }
+        tc.phase ^= 1u;
+        if (!done) {
+            tc.failed = 1;
+            if (tid == 0) atomicExch(tc.err, 1);
+        }
+        tc::fence_after_sync();
+        // 5. warps 0-3 read their 32 accumulator lanes (lane = group) and
+        // write the block's 32 outputs of that group into the tile
+        if (done && tid < (uint32_t)kTcRows) {
+            const uint32_t g = tid;
+            uint32_t b = g;
+#pragma unroll
+            for (int q = 0; q < kTcK; q++) b = ins0(b, op.ts[q]);
+            const uint32_t lane_base = (tid & ~31u) << 16;
+#pragma unroll
+            for (int half = 0; half < 2; half++) {
+                uint32_t r[32];
+                tc::tmem_ld32(tc.tmem + lane_base + (uint32_t)half * 32, r);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int i = 0; i < 16; i++)
+                    t[swz(b | co[half * 16 + i], (float2*)nullptr)] =
+                        make_float2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
+            }
+        }
+        tc::fence_before_sync();
+    }
+}
+
 // The segments of one pass on one tile held in shared memory `s` (the tile
 // at `base`).  Ends with the tile updated in `s` and a __syncthreads().
-template <typename V, bool EXACT, int RB>
+template <typename V, bool EXACT, int RB, bool TC = false>
 __device__ __forceinline__ void tile_compute(const TileHdr& hdr, uint64_t base, const TOp* __restrict__ ops,
                                              const TSeg* __restrict__ segs,
-                                             const typename CoefT<V>::C* __restrict__ coef, V* s) {
+                                             const typename CoefT<V>::C* __restrict__ coef, V* s,
+                                             TcCtx* tcx = nullptr) {
     typedef typename CoefT<V>::C C;
     constexpr int NA = 1 << RB;
     V* tag = nullptr;  // selects the swizzle overload
@@ -321,6 +467,13 @@ __device__ __forceinline__ void tile_compute(const TileHdr& hdr, uint64_t base, 
             __shared__ uint32_t wco[1 << kMaxTargets];  // local offset of column / row c
             const TOp& op = ops[sg.op_begin];
             const bool on = (base & op.gcmask) == op.gcval;
+            if constexpr (TC) {
+                if (op.mma >= 0) {  // no controls, 5 targets, 2^12 tile (host-checked)
+                    wide_tc<V>(op, s, *tcx);
+                    __syncthreads();
+                    continue;
+                }
+            }
             const C* m = coef + op.moff;
             const int k = op.k, nl = 1 << k;
             const uint32_t G = T >> k;
@@ -473,17 +626,47 @@ __device__ __forceinline__ void stage_pass(const TileHdr& hdr, unsigned char* sm
 template <typename V, bool EXACT, int RB>
 __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
     k_tile_pass(V* __restrict__ st, const TileHdr phdr, const TOp* __restrict__ gops, const TSeg* __restrict__ gsegs,
-                const typename CoefT<V>::C* __restrict__ gcoef) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+                const typename CoefT<V>::C* __restrict__ gcoef, const float* __restrict__ mmat, int* __restrict__ err) {
+    constexpr bool TC = sizeof(V) == 8 && !EXACT;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ TileHdr hdr;  // indexed with run-time subscripts: keep it out of the parameter space
+    __shared__ uint64_t hoff[1 << kMaxScatterBits];
+    __shared__ uint64_t tc_bar;
+    __shared__ uint32_t tc_tmem;
     if (threadIdx.x == 0) hdr = phdr;
     __syncthreads();
     const TOp* ops = gops;
     const TSeg* segs = gsegs;
     const typename CoefT<V>::C* coef = gcoef;
-    __shared__ uint64_t hoff[1 << kMaxScatterBits];
     stage_pass<V>(hdr, smem_raw, 2, ops, segs, coef);
     tile_offsets(hdr, hoff);
+    TcCtx tcx;
+    const bool use_tc = TC && hdr.mma;
+    if (use_tc) {
+        // operands after the two tiles and the staged pass description (1 KiB aligned)
+        size_t off = 2 * ((size_t)1 << hdr.tbits) * sizeof(V);
+        if (hdr.staged) off += staged_bytes(hdr.nops, hdr.nsegs, hdr.ncoef, sizeof(typename CoefT<V>::C));
+        off = (off + 1023) & ~(size_t)1023;
+        tcx.xh = (float*)(smem_raw + off);
+        tcx.xl = tcx.xh + kTcRows * kTcKr;
+        tcx.bh = tcx.xl + kTcRows * kTcKr;
+        tcx.bl = tcx.bh + kTcN * kTcKr;
+        tcx.mmat = mmat;
+        tcx.loaded = -1;
+        tcx.failed = 0;
+        tcx.err = err;
+        tcx.phase = 0;
+        tcx.bar = &tc_bar;
+        if (threadIdx.x == 0) tc::mbar_init(&tc_bar, 1);
+        if (threadIdx.x < 32) {
+            tc::tmem_alloc(&tc_tmem, kTcN);
+            tc::tmem_relinquish();
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        tcx.tmem = tc_tmem;
+    }
     const uint32_t T = 1u << hdr.tbits;
     V* cur = (V*)smem_raw;
     V* nxt = cur + T;
@@ -497,7 +680,10 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         cp_async_wait<1>();  // this thread's copies into `cur` have landed
         __syncthreads();     // ... and every other thread's
         const uint64_t base = insert_zeros(t, hdr.tb, hdr.tbits);
-        tile_compute<V, EXACT, RB>(hdr, base, ops, segs, coef, cur);
+        if (use_tc)
+            tile_compute<V, EXACT, RB, TC>(hdr, base, ops, segs, coef, cur, &tcx);
+        else
+            tile_compute<V, EXACT, RB, false>(hdr, base, ops, segs, coef, cur);
         tile_store<V>(st, hdr, hoff, base, cur);
         __syncthreads();  // `cur` is read out before it receives tile t + 2 * gridDim.x
         V* tmp = cur;
@@ -505,6 +691,21 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         nxt = tmp;
     }
     cp_async_wait<0>();
+    if (use_tc) {
+        // an MMA still in flight after a wait that gave up: wait for it
+        // again (bounded) before the accumulator is freed
+        if (tcx.failed) {
+            const uint64_t t0 = global_ns_tc();
+            while (!tc::mbar_try_wait(tcx.bar, tcx.phase ^ 1u) && global_ns_tc() - t0 < kTcWaitNs) {
+            }
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            tc::fence_after_sync();
+            tc::tmem_dealloc(tcx.tmem, kTcN);
+        }
+    }
 }
 
 // ------------------------------------------------------------- batches
@@ -543,7 +744,7 @@ __global__ void __launch_bounds__(kTileThreads, 1)
                   unsigned long long* __restrict__ next, unsigned int* __restrict__ done, int* __restrict__ err,
                   const TOp* __restrict__ ops, const TSeg* __restrict__ segs,
                   const typename CoefT<V>::C* __restrict__ coef, uint64_t wait_ns) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ unsigned long long sj;
     __shared__ int sskip;
     __shared__ uint64_t hoff[1 << kMaxScatterBits];
@@ -613,6 +814,7 @@ struct PassPlan {
     std::vector<TSeg> segs;
     std::vector<Cx> coef;
     int rb = 0;           // register bits per thread in register segments
+    std::vector<float> mmat;  // tensor-core operands (Bh, Bl per op, canonical layout)
 };
 
 // Largest number of register bits per thread (512 threads own a 2^12
@@ -733,6 +935,7 @@ static void plan_passes(const std::vector<LGate>& prog, uint32_t nbits, int tbit
             op.cls = g->cls;
             op.k = g->k;
             op.all_local = 1;
+            op.mma = -1;
             for (int q = 0; q < g->k; q++) {
                 op.tg[q] = (int8_t)g->tb[q];
                 op.tl[q] = (int8_t)local_of(g->tb[q]);
@@ -931,7 +1134,8 @@ static void fuse_blocks(const std::vector<LGate>& prog, uint32_t nbits, int k, s
 // over its tiles with the next one in flight), never more than tiles.
 template <typename V, bool EXACT, int RB>
 static int launch_tile_rb(int num_sms, unsigned threads, size_t smem, cudaStream_t s, V* st, const TileHdr& hdr,
-                          const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef) {
+                          const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef, const float* mmat,
+                          int* err) {
     static bool attr = false;
     if (!attr) {
         int dev = 0, optin = 0;
@@ -949,19 +1153,21 @@ static int launch_tile_rb(int num_sms, unsigned threads, size_t smem, cudaStream
     YAO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_pass<V, EXACT, RB>, (int)threads, smem));
     if (per_sm < 1) return fail(YAO_ERR_UNSUPPORTED, "tile pass does not fit on an SM");
     const unsigned grid = (unsigned)std::min<uint64_t>(hdr.ntiles, (uint64_t)per_sm * (uint64_t)num_sms);
-    k_tile_pass<V, EXACT, RB><<<grid, threads, smem, s>>>(st, hdr, ops, segs, coef);
+    k_tile_pass<V, EXACT, RB><<<grid, threads, smem, s>>>(st, hdr, ops, segs, coef, mmat, err);
     return YAO_OK;
 }
 
 template <typename V, bool EXACT>
 static int launch_tile(int rb, int num_sms, unsigned threads, size_t smem, cudaStream_t s, V* st,
-                       const TileHdr& hdr, const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef) {
+                       const TileHdr& hdr, const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef,
+                       const float* mmat, int* err) {
     switch (rb) {
-    case 1: return launch_tile_rb<V, EXACT, 1>(num_sms, threads, smem, s, st, hdr, ops, segs, coef);
-    case 2: return launch_tile_rb<V, EXACT, 2>(num_sms, threads, smem, s, st, hdr, ops, segs, coef);
-    case 3: return launch_tile_rb<V, EXACT, 3>(num_sms, threads, smem, s, st, hdr, ops, segs, coef);
+    case 1: return launch_tile_rb<V, EXACT, 1>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
+    case 2: return launch_tile_rb<V, EXACT, 2>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
+    case 3: return launch_tile_rb<V, EXACT, 3>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
     case 4:
-        if constexpr (sizeof(V) == 8) return launch_tile_rb<V, EXACT, 4>(num_sms, threads, smem, s, st, hdr, ops, segs, coef);
+        if constexpr (sizeof(V) == 8)
+            return launch_tile_rb<V, EXACT, 4>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
         break;
     default: break;
     }
@@ -982,30 +1188,42 @@ static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
             *p = make_float4(hr, hi, (float)(pp.coef[i].re - (double)hr), (float)(pp.coef[i].im - (double)hi));
         }
     }
-    // one device buffer: ops | segments | coefficients (256-byte aligned parts)
-    size_t ob = pp.ops.size() * sizeof(TOp), sb = pp.segs.size() * sizeof(TSeg), cb = hc.size() * sizeof(C);
-    size_t sb_off = (ob + 255) / 256 * 256;
-    size_t cb_off = sb_off + (sb + 255) / 256 * 256;
+    // one device buffer: ops | segments | coefficients | tensor-core operands
+    // (256-byte aligned parts)
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    size_t ob = pp.ops.size() * sizeof(TOp), sb = pp.segs.size() * sizeof(TSeg), cb = hc.size() * sizeof(C),
+           mb = pp.mmat.size() * sizeof(float);
+    size_t sb_off = al(ob);
+    size_t cb_off = sb_off + al(sb);
+    size_t mb_off = cb_off + al(cb);
     void* dbuf = nullptr;
-    YAO_CUDA(cudaMallocAsync(&dbuf, cb_off + cb, ctx->stream));
+    YAO_CUDA(cudaMallocAsync(&dbuf, mb_off + mb, ctx->stream));
     YAO_CUDA(cudaMemcpyAsync(dbuf, pp.ops.data(), ob, cudaMemcpyHostToDevice, ctx->stream));
     YAO_CUDA(cudaMemcpyAsync((char*)dbuf + sb_off, pp.segs.data(), sb, cudaMemcpyHostToDevice, ctx->stream));
     YAO_CUDA(cudaMemcpyAsync((char*)dbuf + cb_off, hc.data(), cb, cudaMemcpyHostToDevice, ctx->stream));
+    if (mb) YAO_CUDA(cudaMemcpyAsync((char*)dbuf + mb_off, pp.mmat.data(), mb, cudaMemcpyHostToDevice, ctx->stream));
     TileHdr hdr = pp.hdr;
     hdr.ncoef = (int32_t)hc.size();
     if (hdr.tbits - hdr.m > kMaxScatterBits) return fail(YAO_ERR_UNSUPPORTED, "tile has too many scattered bits");
     const size_t tile_bytes = ((size_t)1 << hdr.tbits) * sizeof(V);
     const size_t stg = staged_bytes(hdr.nops, hdr.nsegs, hdr.ncoef, sizeof(C));
     hdr.staged = stg <= kMaxStagedBytes ? 1 : 0;
-    const size_t smem = 2 * tile_bytes + (hdr.staged ? stg : 0);
+    size_t smem = 2 * tile_bytes + (hdr.staged ? stg : 0);
+    if (hdr.mma) smem = ((smem + 1023) & ~(size_t)1023) + kTcSmemBytes;
     const unsigned threads = (unsigned)(((uint32_t)1 << pp.hdr.tbits) >> pp.rb);
     const TOp* dops = (const TOp*)dbuf;
     const TSeg* dsegs = (const TSeg*)((char*)dbuf + sb_off);
     const C* dcoef = (const C*)((char*)dbuf + cb_off);
+    const float* dmmat = (const float*)((char*)dbuf + mb_off);
+    if (hdr.mma && !ctx->d_err) {
+        YAO_CUDA(cudaMalloc((void**)&ctx->d_err, sizeof(int)));
+        YAO_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    }
     {
-        ProfScope prof(ctx, EXACT ? "tile_pass_exact" : "tile_pass_fused",
+        ProfScope prof(ctx, hdr.mma ? "tile_pass_tc" : (EXACT ? "tile_pass_exact" : "tile_pass_fused"),
                        (double)pp.hdr.ntiles * (double)((uint64_t)1 << pp.hdr.tbits) * 2.0 * sizeof(V));
-        int s = launch_tile<V, EXACT>(pp.rb, ctx->num_sms, threads, smem, ctx->stream, st, hdr, dops, dsegs, dcoef);
+        int s = launch_tile<V, EXACT>(pp.rb, ctx->num_sms, threads, smem, ctx->stream, st, hdr, dops, dsegs, dcoef,
+                                      dmmat, ctx->d_err);
         if (s) return s;
     }
     ctx->launches++;
@@ -1021,6 +1239,46 @@ struct TileConfig {
     int tbits = 0;
     int rb = 0;
 };
+
+// FP32 -> TF32, round to nearest even (low 13 mantissa bits cleared)
+static float host_tf32(float f) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    u += 0xFFFu + ((u >> 13) & 1u);
+    u &= 0xFFFFE000u;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+// Mark the dense 5-qubit ops of a complex64 pass with a 2^12 tile for the
+// tensor cores and append their operands: the block's real form
+// B[2i+q][2j+p] (re/im of output i against re/im of input j), split into
+// TF32 high and low parts, in the canonical K-major layout.
+static void tc_prepare(PassPlan& pp) {
+    if (pp.hdr.tbits != kTcTileBits) return;
+    for (TOp& op : pp.ops) {
+        if (op.cls != GC_DENSE || op.k != kTcK || op.lcmask != 0 || op.gcmask != 0) continue;
+        op.mma = (int32_t)pp.mmat.size();
+        pp.mmat.resize(pp.mmat.size() + kTcOpFloats, 0.f);
+        float* bh = pp.mmat.data() + op.mma;
+        float* bl = bh + kTcN * kTcKr;
+        const int nl = 1 << kTcK;
+        for (int i = 0; i < nl; i++)
+            for (int j = 0; j < nl; j++) {
+                const Cx u = pp.coef[(size_t)op.moff + (size_t)i * nl + j];
+                const double v[2][2] = {{u.re, -u.im}, {u.im, u.re}};  // [q][p]
+                for (int q = 0; q < 2; q++)
+                    for (int p2 = 0; p2 < 2; p2++) {
+                        const uint32_t o = 2 * i + q, kk = 2 * j + p2;
+                        const size_t at = ((o >> 3) * kTcSbo + (kk >> 2) * 128 + (o & 7) * 16 + (kk & 3) * 4) / 4;
+                        const float h = host_tf32((float)v[q][p2]);
+                        bh[at] = h;
+                        bl[at] = host_tf32((float)(v[q][p2] - (double)h));
+                    }
+            }
+        pp.hdr.mma = 1;
+    }
+}
 
 template <typename V>
 static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, const std::vector<LGate>& prog,
@@ -1040,6 +1298,18 @@ static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, c
             const int rb = std::max(tb - 9, std::min(cfg.rb, tb));
             plan_segments(pp, std::min(rb, max_reg_bits<V>()));
         }
+    // dense 5-qubit blocks of complex64 FUSED runs go to the tensor cores
+    // (YAO_TC=0 keeps them on the CUDA cores)
+    bool any_tc = false;
+    if (sizeof(V) == 8 && mode == YAO_MODE_FUSED) {
+        const char* e = getenv("YAO_TC");
+        if (!(e && e[0] == '0'))
+            for (PassPlan& pp : passes)
+                if (!pp.single) {
+                    tc_prepare(pp);
+                    any_tc |= pp.hdr.mma != 0;
+                }
+    }
     for (const PassPlan& pp : passes) {
         int s;
         if (pp.single)
@@ -1049,6 +1319,15 @@ static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, c
         else
             s = run_pass<V, false>(ctx, st, nbits, pp);
         if (s) return s;
+    }
+    if (any_tc) {
+        int herr = 0;
+        YAO_CUDA(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (herr) {
+            YAO_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+            return fail(YAO_ERR_TIMEOUT, "tensor-core pass: an MMA completion wait gave up");
+        }
     }
     return YAO_OK;
 }

@@ -131,6 +131,8 @@ struct Ctx {
     void* host_pinned = nullptr;
     size_t host_pinned_bytes = 0;
     uint64_t launches = 0;
+    // device word a kernel sets when one of its bounded waits gave up
+    int* d_err = nullptr;
     int ensure_scratch(size_t bytes);
     int ensure_host_pinned(size_t bytes);
     // optional per-launch timing (CUDA events on `stream` around each launch)
