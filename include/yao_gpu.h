@@ -102,9 +102,11 @@ enum yao_precision { YAO_C128 = 0, YAO_C64 = 1 };
  *   FUSED     gates multiplied into dense k-qubit blocks on the host (FP64),
  *             each block one tiled pass; not bit-exact, report 1 - fidelity.
  *             On a YAO_C64 register the blocks are applied with split
- *             (hi + lo) FP32 products accumulated in FP32, and when every
- *             gate is unitary the input's FP64 norm is restored at the end
- *             (yao_apply_inplace_mode; the batched form does not). */
+ *             (hi + lo) FP32 products accumulated in FP32 (dense 3..5-qubit
+ *             blocks: three TF32 tensor-core products), and when every gate
+ *             is unitary and the circuit has 256 gates or more, the input's
+ *             FP64 norm is restored at the end (yao_apply_inplace_mode; the
+ *             batched form does not). */
 enum yao_apply_mode { YAO_MODE_PLAIN = 0, YAO_MODE_TILED = 1, YAO_MODE_FUSED = 2 };
 
 /* One circuit element: PositionedGate (src/circuit.rs:103-109),
@@ -229,6 +231,11 @@ int yao_apply_inplace_mode(const yao_circuit* c, yao_reg* r, int32_t mode, int32
  * bits}.  Apply calls tune on first use by themselves unless YAO_AUTOTUNE=0;
  * YAO_TUNE_CACHE=<file> keeps the choices across processes. */
 int yao_autotune(const yao_circuit* c, yao_reg* r, int32_t mode, int32_t k, int32_t* choice);
+/* The TILED / FUSED plan of c for a given shape, computed on the host only
+ * (no device needed): info[7] = {passes, single-gate passes, ops,
+ * tensor-core ops, wide CUDA-core ops, register segments, fused blocks}. */
+int yao_plan_info(const yao_circuit* c, int32_t precision, int32_t mode, int32_t k, int32_t tile_bits,
+                  int32_t reg_bits, int64_t* info);
 
 /* ---------------------------------------------------------- DensityMatrix */
 /* DensityMatrix::from_reg / zero_state / mixed (src/density_matrix.rs:19-57). */

@@ -146,3 +146,27 @@ def test_operator_string_normalisation():
     p = Y.OperatorPolynomial.single(0, Y.Op.Z, 2.0) + Y.OperatorPolynomial.identity()
     assert len(p) == 2 and p.coeffs() == [2.0, 1.0]
     assert (-p).coeffs() == [-2.0, -1.0]
+
+
+def test_plan_info_host_only():
+    """The TILED / FUSED planner runs on the host: every gate lands in a pass,
+    fused blocks never outnumber the gates, tensor-core ops appear only for
+    complex64 FUSED plans with 2^12 tiles."""
+    from helpers import layered_circuit, random_circuit
+    rng = np.random.default_rng(3)
+    for n in (8, 14, 20):
+        c = random_circuit(rng, n, 200, max_ctrl=2)
+        tiled = Y.plan_info(c, Y.C128, Y.MODE_TILED, 0, 10, 2)
+        assert tiled["single_gate_passes"] == 0 and tiled["tensor_core_ops"] == 0
+        assert tiled["ops"] <= len(c.elements) and tiled["passes"] >= 1
+        for k in (2, 4, 5):
+            f = Y.plan_info(c, Y.C64, Y.MODE_FUSED, k, 12, 3)
+            assert f["blocks"] <= len(c.elements) and f["ops"] == f["blocks"]
+            f128 = Y.plan_info(c, Y.C128, Y.MODE_FUSED, k, 12, 3)
+            assert f128["tensor_core_ops"] == 0 and f128["blocks"] == f["blocks"]
+    c = layered_circuit(16, 10, seed=1)
+    f = Y.plan_info(c, Y.C64, Y.MODE_FUSED, 5, 12, 3)
+    assert f["tensor_core_ops"] > 0
+    assert Y.plan_info(c, Y.C64, Y.MODE_FUSED, 5, 11, 3)["tensor_core_ops"] == 0
+    with pytest.raises(Y.YaoError):
+        Y.plan_info(c, Y.C64, Y.MODE_PLAIN, 5, 12, 3)

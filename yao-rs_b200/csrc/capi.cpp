@@ -803,8 +803,10 @@ int yao_apply_inplace_mode(const yao_circuit* cc, yao_reg* r, int32_t mode, int3
     const std::vector<LGate>& prog = lowered(c);
     // FUSED on complex64: the FP32 arithmetic drifts the norm by a few 1e-7
     // over thousands of gates; a unitary circuit keeps the input's norm, so
-    // the FP64 norm of the input is restored afterwards.
-    const bool renorm = mode == YAO_MODE_FUSED && r->precision == YAO_C64 && !prog.empty() && program_is_unitary(prog);
+    // the FP64 norm of the input is restored afterwards (circuits of 256
+    // gates or more: shorter ones drift by less than an FP32 ulp).
+    const bool renorm =
+        mode == YAO_MODE_FUSED && r->precision == YAO_C64 && prog.size() >= 256 && program_is_unitary(prog);
     double n0 = 0.0;
     if (renorm && (s = reduce_norm_sqr(r->ctx, r, &n0))) return s;
     s = launch_program(r->ctx, r, prog, mode, k);
@@ -830,6 +832,23 @@ int yao_autotune(const yao_circuit* cc, yao_reg* r, int32_t mode, int32_t k, int
         return fail(YAO_ERR_INVALID_ARGUMENT, "autotuning applies to the TILED and FUSED modes");
     YAO_CUDA(cudaSetDevice(r->ctx->device));
     return autotune_program(r->ctx, r, lowered(c), mode, k, choice);
+}
+
+int yao_plan_info(const yao_circuit* cc, int32_t precision, int32_t mode, int32_t k, int32_t tile_bits,
+                  int32_t reg_bits, int64_t* info) {
+    CHECK_NULL(cc);
+    CHECK_NULL(info);
+    clear_error();
+    yao_circuit* c = const_cast<yao_circuit*>(cc);
+    if (!c->qubit_only) return fail(YAO_ERR_QUBIT_ONLY, "ArrayReg only supports qubit-only circuits");
+    int s = check_widths(c);
+    if (s) return s;
+    if (mode != YAO_MODE_TILED && mode != YAO_MODE_FUSED)
+        return fail(YAO_ERR_INVALID_ARGUMENT, "plans exist for the TILED and FUSED modes");
+    if (precision != YAO_C128 && precision != YAO_C64) return fail(YAO_ERR_INVALID_ARGUMENT, "unknown precision");
+    if (tile_bits < 6 || tile_bits > 13 || reg_bits < 1 || reg_bits > 4)
+        return fail(YAO_ERR_INVALID_ARGUMENT, "tile bits 6..13, register bits 1..4");
+    return plan_info(lowered(c), c->nbits, precision, mode, k, tile_bits, reg_bits, info);
 }
 
 int yao_apply_inplace(const yao_circuit* c, yao_reg* r) { return yao_apply_inplace_mode(c, r, YAO_MODE_PLAIN, 0); }

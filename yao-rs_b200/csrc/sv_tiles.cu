@@ -290,6 +290,8 @@ struct TcCtx {
     uint32_t tmem;       // accumulator (64 columns)
     uint64_t* bar;       // MMA completion barrier
     uint32_t phase;      // parity of the next completion
+    uint64_t* bbar;      // B operand copy barrier
+    uint32_t bphase;
     float* xh;           // operands in shared memory (1 KiB aligned)
     float* xl;
     float* bh;
@@ -310,6 +312,13 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
         float2* t = (float2*)s;
         const uint32_t nt = blockDim.x, tid = threadIdx.x;
         __shared__ uint32_t co[1 << kTcK];  // tile offset of local index c
+        // B operands of this op (Bh, Bl: 32 KiB contiguous): one bulk copy
+        // started now, waited for by the MMA-issuing thread
+        const bool need_b = tc.loaded != op.mma;
+        if (need_b && tid == 0) {
+            tc::mbar_arrive_expect_tx(tc.bbar, (uint32_t)kTcOpFloats * 4);
+            tc::bulk_g2s(tc.bh, tc.mmat + op.mma, (uint32_t)kTcOpFloats * 4, tc.bbar);
+        }
         if (tid < (1u << kTcK)) {
             uint32_t o = 0;
 #pragma unroll
@@ -317,38 +326,41 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
             co[tid] = o;
         }
         __syncthreads();
-        // 1. X: 128 groups x 16 pairs of local indices -> 16-byte chunks
-        for (uint32_t it = tid; it < (uint32_t)kTcRows * 16; it += nt) {
-            const uint32_t g = it & (kTcRows - 1), jp = it >> 7;
+        // 1. X: row g = tid % 128 (one group per thread), 16-byte chunks jp
+        {
+            const uint32_t g = tid & (kTcRows - 1);
             uint32_t b = g;
 #pragma unroll
             for (int q = 0; q < kTcK; q++) b = ins0(b, op.ts[q]);
-            const float2 v0 = t[swz(b | co[2 * jp], (float2*)nullptr)];
-            const float2 v1 = t[swz(b | co[2 * jp + 1], (float2*)nullptr)];
-            const float4 x = make_float4(v0.x, v0.y, v1.x, v1.y);
-            const float4 h = make_float4(tc::to_tf32(x.x), tc::to_tf32(x.y), tc::to_tf32(x.z), tc::to_tf32(x.w));
-            const float4 l = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
-            const uint32_t off = tc_off(g, 4 * jp);
-            *(float4*)((char*)tc.xh + off) = h;
-            *(float4*)((char*)tc.xl + off) = l;
-        }
-        // 2. B: this op's operands (kept while consecutive tiles reuse them)
-        if (tc.loaded != op.mma) {
-            const float4* src = (const float4*)(tc.mmat + op.mma);
-            float4* dh = (float4*)tc.bh;
-            float4* dl = (float4*)tc.bl;
-            constexpr int n4 = kTcN * kTcKr / 4;
-            for (int i = tid; i < n4; i += nt) {
-                dh[i] = src[i];
-                dl[i] = src[n4 + i];
+            for (uint32_t jp = tid >> 7; jp < 16; jp += nt >> 7) {
+                const float2 v0 = t[swz(b | co[2 * jp], (float2*)nullptr)];
+                const float2 v1 = t[swz(b | co[2 * jp + 1], (float2*)nullptr)];
+                const float4 h = make_float4(tc::to_tf32(v0.x), tc::to_tf32(v0.y), tc::to_tf32(v1.x), tc::to_tf32(v1.y));
+                const float4 l = make_float4(v0.x - h.x, v0.y - h.y, v1.x - h.z, v1.y - h.w);
+                const uint32_t off = tc_off(g, 4 * jp);
+                *(float4*)((char*)tc.xh + off) = h;
+                *(float4*)((char*)tc.xl + off) = l;
             }
-            tc.loaded = op.mma;
         }
         tc::fence_proxy_async();
         tc::fence_before_sync();
         __syncthreads();
-        // 3. one thread issues the MMAs: 8 K-steps x 3 products
-        if (tid == 0) {
+        // 2. one thread issues the MMAs: 8 K-steps x 3 products
+        bool b_ok = true;
+        if (need_b) {
+            tc.loaded = op.mma;
+            if (tid == 0) {
+                const uint64_t tb = global_ns_tc();
+                while (!(b_ok = tc::mbar_try_wait(tc.bbar, tc.bphase)))
+                    if (global_ns_tc() - tb > kTcWaitNs) break;
+            }
+            tc.bphase ^= 1u;
+        }
+        if (tid == 0 && !b_ok) {
+            tc.failed = 1;
+            atomicExch(tc.err, 1);
+            tc::commit(tc.bar);  // no MMA: the barrier completes right away
+        } else if (tid == 0) {
             tc::fence_after_sync();
             constexpr uint32_t idesc = tc::idesc_tf32(kTcRows, kTcN);
             const uint32_t xh = tc::smem_u32(tc.xh), xl = tc::smem_u32(tc.xl);
@@ -363,7 +375,7 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
             }
             tc::commit(tc.bar);
         }
-        // 4. every thread waits for completion (bounded)
+        // 3. every thread waits for completion (bounded)
         bool done = false;
         const uint64_t t0 = global_ns_tc();
         while (!(done = tc::mbar_try_wait(tc.bar, tc.phase))) {
@@ -375,22 +387,24 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
             if (tid == 0) atomicExch(tc.err, 1);
         }
         tc::fence_after_sync();
-        // 5. warps 0-3 read their 32 accumulator lanes (lane = group) and
-        // write the block's 32 outputs of that group into the tile
-        if (done && tid < (uint32_t)kTcRows) {
-            const uint32_t g = tid;
+        // 4. warp w reads accumulator lanes 32 (w % 4) .. + 31 (lane = group)
+        // and a quarter (16 warps) or half (8 warps) of the 64 columns, and
+        // writes those outputs of its group into the tile
+        const uint32_t warp = tid >> 5, nwarp = nt >> 5;
+        const uint32_t cpw = 64 / (nwarp >> 2);  // columns per warp (16 or 32)
+        if (done) {
+            const uint32_t g = ((warp & 3) << 5) | (tid & 31);
             uint32_t b = g;
 #pragma unroll
             for (int q = 0; q < kTcK; q++) b = ins0(b, op.ts[q]);
-            const uint32_t lane_base = (tid & ~31u) << 16;
-#pragma unroll
-            for (int half = 0; half < 2; half++) {
-                uint32_t r[32];
-                tc::tmem_ld32(tc.tmem + lane_base + (uint32_t)half * 32, r);
+            const uint32_t c0 = (warp >> 2) * cpw;
+            for (uint32_t c = c0; c < c0 + cpw; c += 16) {
+                uint32_t r[16];
+                tc::tmem_ld16(tc.tmem + (((warp & 3) << 5) << 16) + c, r);
                 tc::tmem_wait_ld();
 #pragma unroll
-                for (int i = 0; i < 16; i++)
-                    t[swz(b | co[half * 16 + i], (float2*)nullptr)] =
+                for (int i = 0; i < 8; i++)
+                    t[swz(b | co[(c >> 1) + i], (float2*)nullptr)] =
                         make_float2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
             }
         }
@@ -631,7 +645,7 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ TileHdr hdr;  // indexed with run-time subscripts: keep it out of the parameter space
     __shared__ uint64_t hoff[1 << kMaxScatterBits];
-    __shared__ uint64_t tc_bar;
+    __shared__ uint64_t tc_bar, tc_bbar;
     __shared__ uint32_t tc_tmem;
     if (threadIdx.x == 0) hdr = phdr;
     __syncthreads();
@@ -657,7 +671,12 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         tcx.err = err;
         tcx.phase = 0;
         tcx.bar = &tc_bar;
-        if (threadIdx.x == 0) tc::mbar_init(&tc_bar, 1);
+        tcx.bphase = 0;
+        tcx.bbar = &tc_bbar;
+        if (threadIdx.x == 0) {
+            tc::mbar_init(&tc_bar, 1);
+            tc::mbar_init(&tc_bbar, 1);
+        }
         if (threadIdx.x < 32) {
             tc::tmem_alloc(&tc_tmem, kTcN);
             tc::tmem_relinquish();
@@ -697,6 +716,9 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         if (tcx.failed) {
             const uint64_t t0 = global_ns_tc();
             while (!tc::mbar_try_wait(tcx.bar, tcx.phase ^ 1u) && global_ns_tc() - t0 < kTcWaitNs) {
+            }
+            while (tcx.loaded >= 0 && !tc::mbar_try_wait(tcx.bbar, tcx.bphase ^ 1u) &&
+                   global_ns_tc() - t0 < 2 * kTcWaitNs) {
             }
         }
         tc::fence_before_sync();
@@ -1250,14 +1272,28 @@ static float host_tf32(float f) {
     return f;
 }
 
-// Mark the dense 5-qubit ops of a complex64 pass with a 2^12 tile for the
-// tensor cores and append their operands: the block's real form
-// B[2i+q][2j+p] (re/im of output i against re/im of input j), split into
+// Mark the dense 3..5-qubit ops of a complex64 pass with a 2^12 tile for
+// the tensor cores and append their operands.  A block on k < 5 targets is
+// widened to 5 with the identity on 5 - k further tile bits (U x I), so every
+// tensor-core op is one 128 x 64 x 64 product.  Operand: the block's real
+// form B[2i+q][2j+p] (re/im of output i against re/im of input j), split into
 // TF32 high and low parts, in the canonical K-major layout.
 static void tc_prepare(PassPlan& pp) {
     if (pp.hdr.tbits != kTcTileBits) return;
     for (TOp& op : pp.ops) {
-        if (op.cls != GC_DENSE || op.k != kTcK || op.lcmask != 0 || op.gcmask != 0) continue;
+        if (op.cls != GC_DENSE || op.k < 3 || op.k > kTcK || op.lcmask != 0 || op.gcmask != 0) continue;
+        const int k0 = op.k, nl0 = 1 << k0;
+        // widen: local index bits k0..4 on tile positions outside the block
+        uint32_t used = 0;
+        for (int q = 0; q < k0; q++) used |= 1u << op.tl[q];
+        for (int q = k0, pos = 0; q < kTcK; q++) {
+            while (used & (1u << pos)) pos++;
+            op.tl[q] = (int8_t)pos;
+            used |= 1u << pos;
+        }
+        op.k = kTcK;
+        for (int q = 0; q < kTcK; q++) op.ts[q] = op.tl[q];
+        std::sort(op.ts, op.ts + kTcK);
         op.mma = (int32_t)pp.mmat.size();
         pp.mmat.resize(pp.mmat.size() + kTcOpFloats, 0.f);
         float* bh = pp.mmat.data() + op.mma;
@@ -1265,7 +1301,9 @@ static void tc_prepare(PassPlan& pp) {
         const int nl = 1 << kTcK;
         for (int i = 0; i < nl; i++)
             for (int j = 0; j < nl; j++) {
-                const Cx u = pp.coef[(size_t)op.moff + (size_t)i * nl + j];
+                const bool same_hi = (i >> k0) == (j >> k0);
+                const Cx u = same_hi ? pp.coef[(size_t)op.moff + (size_t)(i & (nl0 - 1)) * nl0 + (j & (nl0 - 1))]
+                                     : Cx{0.0, 0.0};
                 const double v[2][2] = {{u.re, -u.im}, {u.im, u.re}};  // [q][p]
                 for (int q = 0; q < 2; q++)
                     for (int p2 = 0; p2 < 2; p2++) {
@@ -1541,6 +1579,39 @@ static int run_program_t(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32
 int launch_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k) {
     if (r->precision == YAO_C128) return run_program_t<double2>(ctx, r, prog, mode, k);
     return run_program_t<float2>(ctx, r, prog, mode, k);
+}
+
+int plan_info(const std::vector<LGate>& prog, uint32_t nbits, int32_t precision, int32_t mode, int32_t k,
+              int32_t tbits, int32_t rb, int64_t info[7]) {
+    for (int i = 0; i < 7; i++) info[i] = 0;
+    std::vector<LGate> work;
+    if (mode == YAO_MODE_FUSED)
+        fuse_blocks(prog, nbits, std::max(1, std::min<int>(k, kMaxTargets)), work);
+    else
+        work = prog;
+    info[6] = (int64_t)work.size();
+    std::vector<PassPlan> passes;
+    plan_passes(work, nbits, tbits, passes);
+    const int maxrb = precision == YAO_C128 ? max_reg_bits<double2>() : max_reg_bits<float2>();
+    for (PassPlan& pp : passes) {
+        info[0]++;
+        if (pp.single) {
+            info[1]++;
+            continue;
+        }
+        const int tb = (int)pp.hdr.tbits;
+        plan_segments(pp, std::min(std::max(tb - 9, std::min<int>(rb, tb)), maxrb));
+        if (precision == YAO_C64 && mode == YAO_MODE_FUSED) tc_prepare(pp);
+        info[2] += (int64_t)pp.ops.size();
+        for (const TOp& op : pp.ops) {
+            if (op.mma >= 0)
+                info[3]++;
+            else if (op.cls == GC_DENSE && op.k >= 3)
+                info[4]++;
+        }
+        for (const TSeg& sg : pp.segs) info[5] += sg.wide ? 0 : 1;
+    }
+    return YAO_OK;
 }
 
 int autotune_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k, int32_t out[3]) {

@@ -14,7 +14,7 @@ from .gate import Gate
 from .noise import NoiseChannel
 from .operator import Op, OperatorPolynomial, OperatorString, op_matrix
 from .ops import (MeasureResult, PostProcess, apply, apply_inplace, autotune, batch_apply, expect_arrayreg, expect_dm, expect_grad_batch,
-                  expect_grad, measure_with_postprocess, probs)
+                  expect_grad, measure_with_postprocess, plan_info, probs)
 from .register import ArrayReg, DensityMatrix, Register, density_matrix_from_reg
 
 __all__ = [
@@ -23,5 +23,5 @@ __all__ = [
     "PositionedAnnotation", "PositionedChannel", "PositionedGate", "PostProcess", "Register", "YaoError",
     "apply", "apply_inplace", "autotune", "batch_apply", "channel", "context", "control", "density_matrix_from_reg",
     "elements_array", "expect_arrayreg", "expect_dm", "expect_grad", "expect_grad_batch", "label", "launch_count",
-    "measure_with_postprocess", "op_matrix", "probs", "put",
+    "measure_with_postprocess", "op_matrix", "plan_info", "probs", "put",
 ]

@@ -35,6 +35,14 @@ def autotune(circuit, reg: ArrayReg, mode: int = A.MODE_FUSED, k: int = 0) -> di
     return {"k": out[0], "tile_bits": out[1], "reg_bits": out[2]}
 
 
+def plan_info(circuit, precision=A.C128, mode=A.MODE_FUSED, k=5, tile_bits=12, reg_bits=3) -> dict:
+    """The host plan of a TILED / FUSED run (no device needed)."""
+    out = (C.c_int64 * 7)()
+    A.check(A.lib().yao_plan_info(circuit.handle, precision, mode, k, tile_bits, reg_bits, out))
+    keys = ("passes", "single_gate_passes", "ops", "tensor_core_ops", "wide_ops", "register_segments", "blocks")
+    return dict(zip(keys, [int(x) for x in out]))
+
+
 def batch_apply(circuits, regs, mode: int = A.MODE_PLAIN, k: int = 0):
     cs = (C.c_void_p * max(1, len(circuits)))(*[c.handle for c in circuits])
     rs = (C.c_void_p * max(1, len(regs)))(*[r.handle for r in regs])
