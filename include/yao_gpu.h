@@ -104,9 +104,9 @@ enum yao_precision { YAO_C128 = 0, YAO_C64 = 1 };
  *             On a YAO_C64 register the blocks are applied with split
  *             (hi + lo) FP32 products accumulated in FP32 (dense 3..5-qubit
  *             blocks: three TF32 tensor-core products), and when every gate
- *             is unitary and the circuit has 256 gates or more, the input's
- *             FP64 norm is restored at the end (yao_apply_inplace_mode; the
- *             batched form does not). */
+ *             is unitary and blocks ran on the tensor cores or the circuit
+ *             has 256 gates or more, the input's FP64 norm is restored at
+ *             the end (yao_apply_inplace_mode; the batched form does not). */
 enum yao_apply_mode { YAO_MODE_PLAIN = 0, YAO_MODE_TILED = 1, YAO_MODE_FUSED = 2 };
 
 /* One circuit element: PositionedGate (src/circuit.rs:103-109),

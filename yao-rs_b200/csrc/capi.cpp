@@ -802,16 +802,18 @@ int yao_apply_inplace_mode(const yao_circuit* cc, yao_reg* r, int32_t mode, int3
     YAO_CUDA(cudaSetDevice(r->ctx->device));
     const std::vector<LGate>& prog = lowered(c);
     // FUSED on complex64: the FP32 arithmetic drifts the norm by a few 1e-7
-    // over thousands of gates; a unitary circuit keeps the input's norm, so
-    // the FP64 norm of the input is restored afterwards (circuits of 256
-    // gates or more: shorter ones drift by less than an FP32 ulp).
-    const bool renorm =
-        mode == YAO_MODE_FUSED && r->precision == YAO_C64 && prog.size() >= 256 && program_is_unitary(prog);
+    // over thousands of gates, and the tensor cores' FP32 accumulation
+    // shrinks it by up to about 1e-7 per block; a unitary circuit keeps the
+    // input's norm, so the FP64 norm of the input is restored afterwards
+    // when blocks ran on the tensor cores or the circuit has 256 gates or
+    // more (shorter CUDA-core runs drift by less than an FP32 ulp).
+    const bool renorm = mode == YAO_MODE_FUSED && r->precision == YAO_C64 && program_is_unitary(prog);
     double n0 = 0.0;
     if (renorm && (s = reduce_norm_sqr(r->ctx, r, &n0))) return s;
+    r->ctx->tc_used = false;
     s = launch_program(r->ctx, r, prog, mode, k);
     if (s) return s;
-    if (renorm && n0 > 0.0) {
+    if (renorm && n0 > 0.0 && (r->ctx->tc_used || prog.size() >= 256)) {
         double n1 = 0.0;
         if ((s = reduce_norm_sqr(r->ctx, r, &n1))) return s;
         if (n1 > 0.0 && (s = launch_scale(r->ctx, r, std::sqrt(n1 / n0)))) return s;

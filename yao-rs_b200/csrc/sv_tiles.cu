@@ -1358,6 +1358,7 @@ static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, c
             s = run_pass<V, false>(ctx, st, nbits, pp);
         if (s) return s;
     }
+    ctx->tc_used = any_tc;
     if (any_tc) {
         int herr = 0;
         YAO_CUDA(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));

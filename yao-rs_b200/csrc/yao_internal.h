@@ -133,6 +133,8 @@ struct Ctx {
     uint64_t launches = 0;
     // device word a kernel sets when one of its bounded waits gave up
     int* d_err = nullptr;
+    // the last TILED / FUSED run put some blocks on the tensor cores
+    bool tc_used = false;
     int ensure_scratch(size_t bytes);
     int ensure_host_pinned(size_t bytes);
     // optional per-launch timing (CUDA events on `stream` around each launch)
