@@ -254,8 +254,8 @@ def main():
     ap.add_argument("--qubits", type=int, default=NQ)
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
-    ap.add_argument("--profile-case", default=None, choices=["plain", "tiled", "fused64", "fused32", "fused32_tc", "vqe",
-                                                             "dm", "batch", "vqe_batch"],
+    ap.add_argument("--profile-case", default=None, choices=["plain", "tiled", "fused64", "fused32", "fused32_tc", "pass1q",
+                                                             "vqe", "dm", "batch", "vqe_batch"],
                     help="run one small case of a kernel family (for ncu captures) and exit")
     args = ap.parse_args()
     if args.profile_case:
@@ -409,6 +409,14 @@ def profile_case(args):
         sets = rng.uniform(-math.pi, math.pi, size=(512, 2 * 16 * 2))
         c = vqe_circuit(Y, 16, 2, sets[0])
         Y.expect_grad_batch(tfim(Y, 16), c, sets, Y.ArrayReg.zero_state(16))
+    elif args.profile_case == "pass1q":
+        # one complex64 tile pass holding a single 1-qubit block (the bare
+        # load / store pipeline of a pass), run 4 times
+        os.environ.update(YAO_TILE_BITS="12", YAO_REG_BITS="3", YAO_AUTOTUNE="0")
+        c = Y.Circuit.qubits(n, [Y.put([0], Y.Gate.Ry(0.3))])
+        r = Y.ArrayReg.zero_state(n, Y.C64)
+        for _ in range(4):
+            Y.apply_inplace(c, r, Y.MODE_FUSED, 5)
     elif args.profile_case == "fused32_tc":
         # 8 layers as one circuit, dense 3..5-qubit blocks on the tensor cores
         os.environ.update(YAO_TILE_BITS="12", YAO_REG_BITS="3", YAO_AUTOTUNE="0")
