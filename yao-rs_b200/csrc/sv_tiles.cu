@@ -93,17 +93,19 @@ __device__ __forceinline__ double2 cmulassign_c(double2 x, double2 c) {
     if (EXACT) return cmulassign_x(x, c);
     return cmul_c<false>(c, x);
 }
-// split-coefficient products for complex64 data: hi*x + lo*x, FP32 accumulate
+// split-coefficient products for complex64 data: (hi + lo) * x as one FMA
+// chain per component, the small lo terms first, FP32 accumulate
 template <bool EXACT>
 __device__ __forceinline__ float2 cmul_c(float4 c, float2 x) {
-    float hr = fmaf(c.x, x.x, -c.y * x.y), hi = fmaf(c.x, x.y, c.y * x.x);
-    float lr = fmaf(c.z, x.x, -c.w * x.y), li = fmaf(c.z, x.y, c.w * x.x);
-    return make_float2(hr + lr, hi + li);
+    const float re = fmaf(c.x, x.x, fmaf(-c.y, x.y, fmaf(c.z, x.x, -c.w * x.y)));
+    const float im = fmaf(c.x, x.y, fmaf(c.y, x.x, fmaf(c.z, x.y, c.w * x.x)));
+    return make_float2(re, im);
 }
 template <bool EXACT>
 __device__ __forceinline__ float2 cfma_c(float2 acc, float4 c, float2 x) {
-    float2 p = cmul_c<EXACT>(c, x);
-    return make_float2(acc.x + p.x, acc.y + p.y);
+    const float re = fmaf(c.x, x.x, fmaf(-c.y, x.y, fmaf(c.z, x.x, fmaf(-c.w, x.y, acc.x))));
+    const float im = fmaf(c.x, x.y, fmaf(c.y, x.x, fmaf(c.z, x.y, fmaf(c.w, x.x, acc.y))));
+    return make_float2(re, im);
 }
 template <bool EXACT>
 __device__ __forceinline__ float2 cmulassign_c(float2 x, float4 c) {
@@ -160,6 +162,18 @@ __device__ __forceinline__ void tile_offsets(const TileHdr& hdr, uint64_t* hoff)
     __syncthreads();
 }
 
+// Base index of tile t (t's bits deposited on the positions outside the
+// tile): the deposit is linear over disjoint bit fields, so four 256-entry
+// tables of 8-bit chunks of t, built once per CTA, replace the loop.
+__device__ __forceinline__ void tile_base_tables(const TileHdr& hdr, uint64_t* bt) {
+    for (uint32_t e = threadIdx.x; e < 4 * 256; e += blockDim.x)
+        bt[e] = insert_zeros((uint64_t)(e & 255) << (8 * (e >> 8)), hdr.tb, hdr.tbits);
+    __syncthreads();
+}
+__device__ __forceinline__ uint64_t tile_base(uint64_t t, const uint64_t* bt) {
+    return bt[t & 255] | bt[256 + ((t >> 8) & 255)] | bt[512 + ((t >> 16) & 255)] | bt[768 + ((t >> 24) & 255)];
+}
+
 __device__ __forceinline__ uint64_t tile_global(uint64_t base, uint32_t l, int m, const uint64_t* hoff) {
     return base | (l & ((1u << m) - 1)) | hoff[l >> m];
 }
@@ -177,11 +191,12 @@ __device__ __forceinline__ void reg1(V (&v)[1 << RB], const uint32_t lbase, cons
         c = m[2];
         d = m[3];
     }
+    const bool ctl = op.lcmask != 0;  // in-tile controls: test every pair
 #pragma unroll
     for (int j = 0; j < (1 << RB); j++) {
         if (j & (1 << P)) continue;
         const int j1 = j | (1 << P);
-        if (((lbase | roff[j]) & op.lcmask) != op.lcval) continue;
+        if (ctl && ((lbase | roff[j]) & op.lcmask) != op.lcval) continue;
         V w = v[j], x = v[j1];
         if (isx) {
             v[j] = x;
@@ -637,16 +652,19 @@ __device__ __forceinline__ void stage_pass(const TileHdr& hdr, unsigned char* sm
 // One pass over every tile.  Two tile buffers: while a CTA works on one
 // tile, the next tile it owns streams into the other buffer (cp.async), so
 // HBM traffic overlaps the arithmetic even with one CTA per SM.
-template <typename V, bool EXACT, int RB>
+// TCK: the pass holds tensor-core ops (complex64 FUSED only); a separate
+// instantiation, so passes without them carry none of its state.
+template <typename V, bool EXACT, int RB, bool TCK>
 __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
     k_tile_pass(V* __restrict__ st, const TileHdr phdr, const TOp* __restrict__ gops, const TSeg* __restrict__ gsegs,
                 const typename CoefT<V>::C* __restrict__ gcoef, const float* __restrict__ mmat, int* __restrict__ err) {
-    constexpr bool TC = sizeof(V) == 8 && !EXACT;
+    constexpr bool TC = TCK && sizeof(V) == 8 && !EXACT;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ TileHdr hdr;  // indexed with run-time subscripts: keep it out of the parameter space
     __shared__ uint64_t hoff[1 << kMaxScatterBits];
     __shared__ uint64_t tc_bar, tc_bbar;
     __shared__ uint32_t tc_tmem;
+    __shared__ uint64_t bt[4 * 256];  // tile base tables
     if (threadIdx.x == 0) hdr = phdr;
     __syncthreads();
     const TOp* ops = gops;
@@ -654,9 +672,10 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
     const typename CoefT<V>::C* coef = gcoef;
     stage_pass<V>(hdr, smem_raw, 2, ops, segs, coef);
     tile_offsets(hdr, hoff);
+    tile_base_tables(hdr, bt);
     TcCtx tcx;
-    const bool use_tc = TC && hdr.mma;
-    if (use_tc) {
+    constexpr bool use_tc = TC;
+    if constexpr (use_tc) {
         // operands after the two tiles and the staged pass description (1 KiB aligned)
         size_t off = 2 * ((size_t)1 << hdr.tbits) * sizeof(V);
         if (hdr.staged) off += staged_bytes(hdr.nops, hdr.nsegs, hdr.ncoef, sizeof(typename CoefT<V>::C));
@@ -690,17 +709,17 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
     V* cur = (V*)smem_raw;
     V* nxt = cur + T;
     uint64_t t = blockIdx.x;
-    if (t < hdr.ntiles) tile_load_async<V>(st, hdr, hoff, insert_zeros(t, hdr.tb, hdr.tbits), cur);
+    if (t < hdr.ntiles) tile_load_async<V>(st, hdr, hoff, tile_base(t, bt), cur);
     cp_async_commit();
     for (; t < hdr.ntiles; t += gridDim.x) {
         const uint64_t tn = t + gridDim.x;
-        if (tn < hdr.ntiles) tile_load_async<V>(st, hdr, hoff, insert_zeros(tn, hdr.tb, hdr.tbits), nxt);
+        if (tn < hdr.ntiles) tile_load_async<V>(st, hdr, hoff, tile_base(tn, bt), nxt);
         cp_async_commit();
         cp_async_wait<1>();  // this thread's copies into `cur` have landed
         __syncthreads();     // ... and every other thread's
-        const uint64_t base = insert_zeros(t, hdr.tb, hdr.tbits);
-        if (use_tc)
-            tile_compute<V, EXACT, RB, TC>(hdr, base, ops, segs, coef, cur, &tcx);
+        const uint64_t base = tile_base(t, bt);
+        if constexpr (use_tc)
+            tile_compute<V, EXACT, RB, true>(hdr, base, ops, segs, coef, cur, &tcx);
         else
             tile_compute<V, EXACT, RB, false>(hdr, base, ops, segs, coef, cur);
         tile_store<V>(st, hdr, hoff, base, cur);
@@ -710,7 +729,7 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         nxt = tmp;
     }
     cp_async_wait<0>();
-    if (use_tc) {
+    if constexpr (use_tc) {
         // an MMA still in flight after a wait that gave up: wait for it
         // again (bounded) before the accumulator is freed
         if (tcx.failed) {
@@ -1154,29 +1173,39 @@ static void fuse_blocks(const std::vector<LGate>& prog, uint32_t nbits, int k, s
 
 // Persistent launch: as many CTAs as fit on the SMs at once (each loops
 // over its tiles with the next one in flight), never more than tiles.
-template <typename V, bool EXACT, int RB>
-static int launch_tile_rb(int num_sms, unsigned threads, size_t smem, cudaStream_t s, V* st, const TileHdr& hdr,
-                          const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef, const float* mmat,
-                          int* err) {
+template <typename V, bool EXACT, int RB, bool TCK>
+static int launch_tile_k(int num_sms, unsigned threads, size_t smem, cudaStream_t s, V* st, const TileHdr& hdr,
+                         const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef, const float* mmat,
+                         int* err) {
     static bool attr = false;
     if (!attr) {
         int dev = 0, optin = 0;
         YAO_CUDA(cudaGetDevice(&dev));
         YAO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
         cudaFuncAttributes fa;
-        YAO_CUDA(cudaFuncGetAttributes(&fa, k_tile_pass<V, EXACT, RB>));
-        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        YAO_CUDA(cudaFuncGetAttributes(&fa, k_tile_pass<V, EXACT, RB, TCK>));
+        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB, TCK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       optin - (int)fa.sharedSizeBytes));
-        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB, TCK>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                       cudaSharedmemCarveoutMaxShared));
         attr = true;
     }
     int per_sm = 0;
-    YAO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_pass<V, EXACT, RB>, (int)threads, smem));
+    YAO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_pass<V, EXACT, RB, TCK>, (int)threads, smem));
     if (per_sm < 1) return fail(YAO_ERR_UNSUPPORTED, "tile pass does not fit on an SM");
     const unsigned grid = (unsigned)std::min<uint64_t>(hdr.ntiles, (uint64_t)per_sm * (uint64_t)num_sms);
-    k_tile_pass<V, EXACT, RB><<<grid, threads, smem, s>>>(st, hdr, ops, segs, coef, mmat, err);
+    k_tile_pass<V, EXACT, RB, TCK><<<grid, threads, smem, s>>>(st, hdr, ops, segs, coef, mmat, err);
     return YAO_OK;
+}
+
+template <typename V, bool EXACT, int RB>
+static int launch_tile_rb(int num_sms, unsigned threads, size_t smem, cudaStream_t s, V* st, const TileHdr& hdr,
+                          const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef, const float* mmat,
+                          int* err) {
+    if constexpr (sizeof(V) == 8 && !EXACT) {
+        if (hdr.mma) return launch_tile_k<V, EXACT, RB, true>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
+    }
+    return launch_tile_k<V, EXACT, RB, false>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
 }
 
 template <typename V, bool EXACT>
@@ -1375,7 +1404,7 @@ static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, c
 //
 // The tile shape (tile bits, register bits) and, for FUSED with k = 0, the
 // fusion width are picked by timing candidates on the device: a prefix of
-// the program (at most 2^38 amplitude-gate updates, at least 64 gates) runs
+// the program (at most 2^39 amplitude-gate updates, at least 64 gates) runs
 // on a scratch copy of the register for every candidate, and the fastest is
 // kept per (device, qubits, precision, mode, requested k).  Choices live in
 // memory and, when YAO_TUNE_CACHE names a file, in that file (one
@@ -1458,7 +1487,7 @@ static int tune_program(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog, 
     *best = default_config<V>(mode, kreq);
     *best_ms = -1.0;
     const uint32_t n = r->nbits;
-    const size_t cap = std::max<size_t>(64, (size_t)1 << std::max(0, 38 - (int)n));
+    const size_t cap = std::max<size_t>(64, (size_t)1 << std::max(0, 39 - (int)n));
     std::vector<LGate> sample(prog.begin(), prog.begin() + std::min(prog.size(), cap));
     if (sample.empty()) return YAO_OK;
     const size_t bytes = ((size_t)1 << n) * sizeof(V);
@@ -1507,11 +1536,18 @@ static int tune_program(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog, 
         }
     }
     if (!st && mode == YAO_MODE_FUSED && kreq <= 0) {
+        // widths: each timed after a warm-up run (first-use costs), tensor-core
+        // widths with the 2^12 tile they need
         const TileConfig shape = *best;
         for (int k = 2; k <= kMaxTargets; k++) {
             if (k == shape.k) continue;
             TileConfig c = shape;
             c.k = k;
+            if (sizeof(V) == 8 && k >= 3 && k <= kTcK) {
+                c.tbits = kTcTileBits;
+                c.rb = 3;
+            }
+            if ((st = timed(c, &ms))) break;
             if ((st = timed(c, &ms))) break;
             if (ms < bms) {
                 bms = ms;
