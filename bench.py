@@ -511,8 +511,21 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
         fm = Y.expect_arrayreg(Y.apply(vqe_circuit(Y, nv, lv, pm), z), op).real
         fd = (fp - fm) / (2 * eps)
         fd_err = max(fd_err, abs(fd - g[i]) / max(1e-12, abs(g[i])))
+    # CPU: the oracle's expect_grad (one thread) on the same ansatz at n = 18,
+    # scaled by 2^(24 - 18) to n = 24 (every pass is linear in the amplitudes)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    nc = 18
+    cc = vqe_circuit(Y, nc, lv, rng.uniform(-math.pi, math.pi, size=2 * nc * lv))
+    zc = np.zeros(1 << nc, complex)
+    zc[0] = 1
+    t0 = time.perf_counter()
+    O.expect_grad(tfim(Y, nc), cc, zc)
+    t_cpu = time.perf_counter() - t0
     out["vqe"] = {"qubits": nv, "params": len(g), "gates": len(vc.elements), "grads_per_s": 1.0 / dt,
-                  "s_per_grad": dt, "energy": val, "fd_max_rel_err": fd_err}
+                  "s_per_grad": dt, "energy": val, "fd_max_rel_err": fd_err,
+                  "cpu_oracle_s_per_grad_n18": t_cpu,
+                  "cpu_oracle_s_per_grad_n24_extrapolated": t_cpu * (1 << (nv - nc))}
     del z
     out["qft20"] = qft_extra(Y, A, torch, stream, dev, timed)
     out["noisy_dm14"] = dm_extra(Y, A, torch, stream, dev, timed)
@@ -715,6 +728,16 @@ def dm_extra(Y, A, torch, stream, dev, timed):
     g = Y.DensityMatrix.zero_state(ns, device=dev)
     g.apply(cs)
     res["n8_max_abs_diff_vs_oracle"] = float(np.max(np.abs(g.state_data() - ref)))
+    # one layer at n = 10 on the CPU, scaled to n = 14 (4^4) and 20 layers
+    ns = 10
+    c1 = noisy_dm_circuit(Y, ns, 1)
+    rho0 = np.zeros(1 << (2 * ns), complex)
+    rho0[0] = 1
+    t0 = time.perf_counter()
+    O.dm_apply_circuit(c1, rho0)
+    t1 = time.perf_counter() - t0
+    res["cpu_s_one_layer_n10"] = t1
+    res["cpu_s_per_circuit_n14_extrapolated"] = t1 * layers * 4 ** (n - ns)
     del d
     return res
 
