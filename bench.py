@@ -720,6 +720,23 @@ def dm_extra(Y, A, torch, stream, dev, timed):
            "purity": d.purity(), "trace_re": d.trace().real, "z": zs,
            "kernels": [{"kernel": p["kernel"], "launches": p["launches"], "ms": round(p["ms"], 2),
                         "GBps": round(p["bytes"] / (p["ms"] / 1e3) / 1e9, 1)} for p in prof]}
+    # FUSED form: rho as a 28-qubit vector through the fused tile passes,
+    # channels as superoperators
+    f = Y.DensityMatrix.zero_state(n, device=dev)
+    f.apply(noisy_dm_circuit(Y, n, 1, seed=99), Y.MODE_FUSED)  # warm-up
+    del f
+    f = Y.DensityMatrix.zero_state(n, device=dev)
+    A.profile(True, dev)
+    tf = timed(lambda: f.apply(c, Y.MODE_FUSED))
+    prof = A.profile_report(dev)
+    A.profile(False, dev)
+    zf = [Y.expect_dm(f, Y.OperatorPolynomial.single(i, Y.Op.Z, 1.0)).real for i in range(n)]
+    res["fused_superop"] = {
+        "s_per_circuit": tf, "speedup_vs_plain": t / tf,
+        "max_z_diff": max(abs(a - b) for a, b in zip(zs, zf)), "purity_diff": abs(f.purity() - res["purity"]),
+        "kernels": [{"kernel": p["kernel"], "launches": p["launches"], "ms": round(p["ms"], 2),
+                     "GBps": round(p["bytes"] / (p["ms"] / 1e3) / 1e9, 1)} for p in prof]}
+    del f
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
     ns = 8

@@ -251,6 +251,13 @@ int yao_dm_to_host(const yao_dm* d, double* rho);
 /* Register::apply for DensityMatrix (src/density_matrix.rs:249-259):
  * gates rho -> U rho U^dagger, channels rho -> sum_i K_i rho K_i^dagger. */
 int yao_dm_apply(yao_dm* d, const yao_circuit* c);
+/* The same with an execution form: YAO_MODE_PLAIN (= yao_dm_apply, the exact
+ * Kraus sum of yao-rs) or YAO_MODE_FUSED: rho as a 2n-qubit vector, each
+ * gate as U on the row bits and conj(U) on the column bits, each channel as
+ * its superoperator sum_i K_i (x) conj(K_i) (a dense op on 2k bits), all run
+ * through the FUSED tile-pass engine in FP64 (not bit-identical; agrees to
+ * ~1e-14). */
+int yao_dm_apply_mode(yao_dm* d, const yao_circuit* c, int32_t mode);
 /* trace / purity / partial_tr (src/density_matrix.rs:63-112). */
 int yao_dm_trace(const yao_dm* d, double out[2]);
 int yao_dm_purity(const yao_dm* d, double* out);

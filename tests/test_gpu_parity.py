@@ -520,6 +520,23 @@ def test_density_matrix_bit_exact(n):
     assert maxdiff(Y.probs(d, [n - 1, 0] if n > 1 else [0]), O.dm_probs(ref, n, [n - 1, 0] if n > 1 else [0])) == 0.0
 
 
+@pytest.mark.parametrize("n", [1, 2, 5, 8])
+def test_density_matrix_superop_form(n):
+    """FUSED density-matrix form (rho as a 2n-qubit vector through the fused
+    tile passes, channels as superoperators) against the oracle's Kraus sums:
+    1e-12, trace preserved."""
+    rng = np.random.default_rng(700 + n)
+    c = random_noisy_circuit(rng, n, 25)
+    psi = random_state(rng, n)
+    ref = O.dm_apply_circuit(c, O.dm_from_reg(psi, n))
+    d = Y.DensityMatrix.from_reg(Y.ArrayReg.from_vec(n, psi))
+    d.apply(c, Y.MODE_FUSED)
+    assert maxdiff(d.state_data(), ref) < 1e-12
+    assert abs(d.trace() - O.dm_trace(ref, n)) < 1e-12
+    with pytest.raises(Y.YaoError):
+        d.apply(c, Y.MODE_TILED)
+
+
 def test_density_matrix_golden(golden):
     from test_oracle_golden import dm_cases
     for key, c, psi, n, exp in dm_cases(golden):

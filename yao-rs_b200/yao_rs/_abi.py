@@ -136,6 +136,7 @@ SIGNATURES = {
     "yao_dm_nbits": (C.c_int, [vp, u32p]),
     "yao_dm_to_host": (C.c_int, [vp, dptr]),
     "yao_dm_apply": (C.c_int, [vp, vp]),
+    "yao_dm_apply_mode": (C.c_int, [vp, vp, i32]),
     "yao_dm_trace": (C.c_int, [vp, dptr]),
     "yao_dm_purity": (C.c_int, [vp, dptr]),
     "yao_dm_partial_tr": (C.c_int, [vp, u32p, u32, pp]),

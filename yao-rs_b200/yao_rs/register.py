@@ -262,9 +262,13 @@ class DensityMatrix(Register):
         ev = ev[ev > 1e-15]
         return float(-np.sum(ev * np.log(ev)))
 
-    def apply(self, circuit):
-        """Register::apply for DensityMatrix (src/density_matrix.rs:249-259)."""
-        A.check(A.lib().yao_dm_apply(self._h, circuit.handle))
+    def apply(self, circuit, mode=A.MODE_PLAIN):
+        """Register::apply for DensityMatrix (src/density_matrix.rs:249-259).
+
+        mode=MODE_FUSED runs rho as a 2n-qubit vector through the fused
+        tile passes, channels as superoperators (not bit-identical to the
+        Kraus sums; ~1e-14)."""
+        A.check(A.lib().yao_dm_apply_mode(self._h, circuit.handle, mode))
         return self
 
     def __repr__(self):
