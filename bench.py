@@ -527,10 +527,10 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
                   "cpu_oracle_s_per_grad_n18": t_cpu,
                   "cpu_oracle_s_per_grad_n24_extrapolated": t_cpu * (1 << (nv - nc))}
     del z
+    out["batched_vqe"] = vqe_batch_extra(Y, A, torch, stream, dev, timed)
     out["qft20"] = qft_extra(Y, A, torch, stream, dev, timed)
     out["noisy_dm14"] = dm_extra(Y, A, torch, stream, dev, timed)
     out["batched_circuits"] = batch_extra(Y, A, torch, stream, dev, timed)
-    out["batched_vqe"] = vqe_batch_extra(Y, A, torch, stream, dev, timed)
     return out
 
 

@@ -232,6 +232,25 @@ static int launch_gate_n(Ctx* ctx, V* st, uint32_t nbits, const LGate& g, uint64
 // nsets > 1: the gate acts on nsets registers of nbits qubits stored back to
 // back; the register index sits above every locked bit, so the groups of all
 // registers are enumerated as one range.
+template <typename V, int U>
+static int launch_small(const LGate& g, unsigned grid, cudaStream_t s, V* st, uint64_t ngroups, const DOpT<V>& op) {
+    if (g.cls == GC_X)
+        k_gate_small<V, GC_X, 1, U><<<grid, 256, 0, s>>>(st, ngroups, op);
+    else if (g.cls == GC_SWAP)
+        k_gate_small<V, GC_SWAP, 2, U><<<grid, 256, 0, s>>>(st, ngroups, op);
+    else if (g.cls == GC_DIAG && g.k == 1)
+        k_gate_small<V, GC_DIAG, 1, U><<<grid, 256, 0, s>>>(st, ngroups, op);
+    else if (g.cls == GC_DIAG && g.k == 2)
+        k_gate_small<V, GC_DIAG, 2, U><<<grid, 256, 0, s>>>(st, ngroups, op);
+    else if (g.cls == GC_DENSE && g.k == 1)
+        k_gate_small<V, GC_DENSE, 1, U><<<grid, 256, 0, s>>>(st, ngroups, op);
+    else if (g.cls == GC_DENSE && g.k == 2)
+        k_gate_small<V, GC_DENSE, 2, U><<<grid, 256, 0, s>>>(st, ngroups, op);
+    else
+        return fail(YAO_ERR_INVALID_ARGUMENT, "unsupported gate class");
+    return YAO_OK;
+}
+
 template <typename V>
 static int launch_gate_t(Ctx* ctx, V* st, uint32_t nbits, const LGate& g, uint64_t nsets = 1) {
     DOpT<V> op;
@@ -257,8 +276,20 @@ static int launch_gate_t(Ctx* ctx, V* st, uint32_t nbits, const LGate& g, uint64
             if (!is_one(g.m[l])) op.active |= (uint64_t)1 << l;
         if (op.active == 0) return YAO_OK;  // identity
     }
-    const int U = 2;
-    unsigned grid = grid_for((ngroups + U - 1) / U, 256, ctx->num_sms);
+    // groups per thread per sweep (loads of all of them in flight together)
+    // and CTAs per SM of the grid; YAO_PLAIN_GROUPS / YAO_PLAIN_CTAS override
+    // the defaults for tuning runs
+    static const int U = [] {
+        const char* e = getenv("YAO_PLAIN_GROUPS");
+        const int v = e ? atoi(e) : 2;
+        return (v == 1 || v == 2 || v == 4) ? v : 2;
+    }();
+    static const int per_sm = [] {
+        const char* e = getenv("YAO_PLAIN_CTAS");
+        const int v = e ? atoi(e) : 48;
+        return (v >= 1 && v <= 64) ? v : 48;
+    }();
+    unsigned grid = grid_for((ngroups + U - 1) / U, 256, ctx->num_sms, per_sm);
     cudaStream_t s = ctx->stream;
     // algorithmic traffic: every touched amplitude is read and written once
     int touched = g.cls == GC_DIAG ? __builtin_popcountll(op.active) : (g.cls == GC_SWAP ? 2 : nl);
@@ -267,20 +298,14 @@ static int launch_gate_t(Ctx* ctx, V* st, uint32_t nbits, const LGate& g, uint64
                                       {"gate_diag1", "gate_diag1", "gate_diag2"},
                                       {"gate_dense1", "gate_dense1", "gate_dense2"}};
     ProfScope prof(ctx, names[g.cls][g.k], (double)ngroups * touched * 2.0 * sizeof(V));
-    if (g.cls == GC_X)
-        k_gate_small<V, GC_X, 1, U><<<grid, 256, 0, s>>>(st, ngroups, op);
-    else if (g.cls == GC_SWAP)
-        k_gate_small<V, GC_SWAP, 2, U><<<grid, 256, 0, s>>>(st, ngroups, op);
-    else if (g.cls == GC_DIAG && g.k == 1)
-        k_gate_small<V, GC_DIAG, 1, U><<<grid, 256, 0, s>>>(st, ngroups, op);
-    else if (g.cls == GC_DIAG && g.k == 2)
-        k_gate_small<V, GC_DIAG, 2, U><<<grid, 256, 0, s>>>(st, ngroups, op);
-    else if (g.cls == GC_DENSE && g.k == 1)
-        k_gate_small<V, GC_DENSE, 1, U><<<grid, 256, 0, s>>>(st, ngroups, op);
-    else if (g.cls == GC_DENSE && g.k == 2)
-        k_gate_small<V, GC_DENSE, 2, U><<<grid, 256, 0, s>>>(st, ngroups, op);
+    int st_ = 0;
+    if (U == 1)
+        st_ = launch_small<V, 1>(g, grid, s, st, ngroups, op);
+    else if (U == 4)
+        st_ = launch_small<V, 4>(g, grid, s, st, ngroups, op);
     else
-        return fail(YAO_ERR_INVALID_ARGUMENT, "unsupported gate class");
+        st_ = launch_small<V, 2>(g, grid, s, st, ngroups, op);
+    if (st_) return st_;
     ctx->launches++;
     YAO_CUDA(cudaGetLastError());
     return YAO_OK;
