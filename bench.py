@@ -323,11 +323,11 @@ def main():
     achieved = top["bytes"] / (top["ms"] / 1e3) / 1e9
     # DRAM traffic per launch of the dense 1-qubit kernel: ncu capture of
     # `bench.py --profile-case plain --qubits 27` (dram__bytes_read.sum +
-    # dram__bytes_write.sum = 2.1475 + 2.0905 GB for 2^27 amplitudes), scaled
+    # dram__bytes_write.sum = 2.1475 + 2.0884 GB for 2^27 amplitudes), scaled
     # by the amplitudes one launch processes here.
     traffic = None
     if top["kernel"] == "gate_dense1":
-        traffic = (2.1475e9 + 2.0905e9) * (1 << n) / (1 << 27)
+        traffic = (2.1475e9 + 2.0884e9) * (1 << n) / (1 << 27)
     roofline = {"bound": "hbm", "kernel": top["kernel"], "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
                 "bytes_per_launch": top["bytes"] / top["launches"], "launches": top["launches"],
