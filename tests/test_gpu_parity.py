@@ -609,3 +609,51 @@ def test_tensor_core_blocks(monkeypatch, n, k):
     scale = np.max(np.abs(ref))
     assert np.max(np.abs(outs["1"] - outs["0"])) < 1e-5 * scale
     assert np.max(np.abs(outs["1"] - ref)) < 1e-5 * scale
+
+
+def test_edge_cases_empty_and_tiny():
+    """Empty circuits, annotation-only circuits, 1- and 2-qubit registers in
+    every form, empty batches and empty operators behave like yao-rs."""
+    rng = np.random.default_rng(11)
+    for n in (1, 2, 3):
+        psi = random_state(rng, n)
+        empty = Y.Circuit.qubits(n, [])
+        for mode in (Y.MODE_PLAIN, Y.MODE_TILED, Y.MODE_FUSED):
+            assert maxdiff(gpu_apply(empty, psi, mode), psi) == 0.0
+        c = random_circuit(rng, n, 30, max_ctrl=min(2, n - 1))
+        ref = O.apply_circuit(c, psi)
+        assert maxdiff(gpu_apply(c, psi, Y.MODE_TILED), ref) == 0.0
+        assert maxdiff(gpu_apply(c, psi, Y.MODE_FUSED, 0), ref) < 1e-12
+        r = Y.ArrayReg.from_vec(n, psi).to_precision(Y.C64)
+        Y.apply_inplace(c, r, Y.MODE_FUSED, 0)
+        assert 1 - abs(np.vdot(ref, r.state_vec().astype(np.complex128))) ** 2 < 1e-6
+    c = Y.Circuit.qubits(2, [Y.label(0, "a"), Y.label(1, "b")])
+    r = Y.ArrayReg.zero_state(2)
+    Y.apply_inplace(c, r, Y.MODE_FUSED)
+    assert maxdiff(r.state_vec(), [1, 0, 0, 0]) == 0.0
+    Y.batch_apply([], [], Y.MODE_TILED)
+    assert Y.expect_arrayreg(Y.ArrayReg.zero_state(3), Y.OperatorPolynomial.zero()) == 0
+    v, g = Y.expect_grad(Y.OperatorPolynomial.single(0, Y.Op.Z, 1.0), Y.Circuit.qubits(1, [Y.put([0], Gate.H)]),
+                         Y.ArrayReg.zero_state(1))
+    assert abs(v) < 1e-15 and g == []
+
+
+def test_batched_fused_c64_norm_restored():
+    """Complex64 FUSED batches of circuits with 256 gates or more get their
+    FP64 input norm restored, like a single register: every circuit within
+    1 - F <= 1e-6 of the oracle, norm 1 to 1e-6, and close to the same
+    circuit applied alone."""
+    rng = np.random.default_rng(77)
+    circuits = [layered_circuit(n, 8, seed=n) for n in (12, 13, 14, 15, 12, 14)]
+    assert all(len(c.elements) >= 256 for c in circuits)
+    states = [random_state(rng, c.nbits) for c in circuits]
+    refs = [O.apply_circuit(c, s) for c, s in zip(circuits, states)]
+    regs = [Y.ArrayReg.from_vec(c.nbits, s).to_precision(Y.C64) for c, s in zip(circuits, states)]
+    Y.batch_apply(circuits, regs, Y.MODE_FUSED, 5)
+    for c, s, r, ref in zip(circuits, states, regs, refs):
+        out = r.state_vec().astype(np.complex128)
+        assert 1 - abs(np.vdot(ref, out)) ** 2 < 1e-6
+        assert abs(np.vdot(out, out).real - 1) < 1e-6
+        one = Y.ArrayReg.from_vec(c.nbits, s).to_precision(Y.C64)
+        Y.apply_inplace(c, one, Y.MODE_FUSED, 5)
+        assert np.max(np.abs(one.state_vec() - out)) < 1e-5 * np.max(np.abs(ref))

@@ -1425,7 +1425,38 @@ int yao_batch_apply(const yao_circuit* const* circuits, yao_reg* const* regs, si
         rs[i] = regs[i];
     }
     YAO_CUDA(cudaSetDevice(regs[0]->ctx->device));
-    return launch_batch(regs[0]->ctx, progs, rs, mode, k);
+    Ctx* ctx = regs[0]->ctx;
+    // the norm rule of yao_apply_inplace_mode, batched: the FP64 input norm
+    // of every unitary circuit's register is restored when blocks ran on the
+    // tensor cores or a circuit of the batch has 256 gates or more
+    std::vector<Reg*> nr;
+    bool long_prog = false;
+    if (mode == YAO_MODE_FUSED && regs[0]->precision == YAO_C64)
+        for (size_t i = 0; i < n; i++)
+            if (program_is_unitary(*progs[i])) {
+                nr.push_back(rs[i]);
+                long_prog |= progs[i]->size() >= 256;
+            }
+    double* d_norm = nullptr;
+    int s;
+    if (!nr.empty()) {
+        YAO_CUDA(cudaMallocAsync((void**)&d_norm, 2 * nr.size() * sizeof(double), ctx->stream));
+        if ((s = launch_batch_norm_sqr(ctx, nr, d_norm))) {
+            cudaFreeAsync(d_norm, ctx->stream);
+            return s;
+        }
+    }
+    ctx->tc_used = false;
+    s = launch_batch(ctx, progs, rs, mode, k);
+    if (!s && !nr.empty() && (ctx->tc_used || long_prog)) {
+        s = launch_batch_norm_sqr(ctx, nr, d_norm + nr.size());
+        if (!s) s = launch_batch_rescale(ctx, nr, d_norm, d_norm + nr.size());
+    }
+    if (d_norm) {
+        cudaFreeAsync(d_norm, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+    }
+    return s;
 }
 
 }  // extern "C"

@@ -1067,4 +1067,114 @@ int expect_noalloc(Ctx* ctx, const Reg* r, const yao_term* terms, size_t nterms,
     return YAO_OK;
 }
 
+// ------------------------------------------------ batched norm restore
+// FUSED complex64 batches: every register's squared norm in two launches
+// (chunk partials, then each register's partials in chunk order), and one
+// launch that divides each register by sqrt(n1 / n0).  Deterministic like the
+// single-register reductions; nothing returns to the host.
+
+constexpr uint32_t kNormChunk = 1u << 16;  // amplitudes per chunk
+
+struct NormChunk {
+    uint64_t p;     // first amplitude of the chunk
+    uint32_t len;   // amplitudes in the chunk
+    uint32_t slot;  // index of the register's norm
+};
+
+template <typename V>
+__global__ void __launch_bounds__(kRT) k_chunk_norm_sqr(const NormChunk* __restrict__ ch, double* __restrict__ part) {
+    __shared__ double sm[kRT / 32];
+    const NormChunk c = ch[blockIdx.x];
+    const V* st = (const V*)(uintptr_t)c.p;
+    double acc = 0.0;
+    for (uint32_t i = threadIdx.x; i < c.len; i += blockDim.x) {
+        double2 v = to_d2(st[i]);
+        acc += v.x * v.x + v.y * v.y;
+    }
+    block_sum_write(&acc, 1, sm, part + blockIdx.x);
+}
+
+__global__ void __launch_bounds__(kRT) k_slot_sums(const uint32_t* __restrict__ first, uint32_t nslots,
+                                                   const double* __restrict__ part, double* __restrict__ out) {
+    __shared__ double sm[kRT / 32];
+    for (uint32_t r = blockIdx.x; r < nslots; r += gridDim.x) {
+        double acc = 0.0;
+        for (uint32_t i = first[r] + threadIdx.x; i < first[r + 1]; i += blockDim.x) acc += part[i];
+        block_sum_write(&acc, 1, sm, out + r);
+    }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kRT) k_chunk_rescale(const NormChunk* __restrict__ ch, const double* __restrict__ n0,
+                                                       const double* __restrict__ n1) {
+    const NormChunk c = ch[blockIdx.x];
+    const double a = n0[c.slot], b = n1[c.slot];
+    if (!(a > 0.0 && b > 0.0)) return;
+    const double d = sqrt(b / a);
+    V* st = (V*)(uintptr_t)c.p;
+    for (uint32_t i = threadIdx.x; i < c.len; i += blockDim.x) {
+        double2 v = to_d2(st[i]);
+        st[i] = from_d2<V>(make_double2(__ddiv_rn(v.x, d), __ddiv_rn(v.y, d)));
+    }
+}
+
+static void norm_chunks(const std::vector<Reg*>& regs, std::vector<NormChunk>& ch, std::vector<uint32_t>& first) {
+    first.assign(1, 0);
+    for (size_t s = 0; s < regs.size(); s++) {
+        const uint64_t n = (uint64_t)1 << regs[s]->nbits, es = regs[s]->precision == YAO_C128 ? 16 : 8;
+        for (uint64_t o = 0; o < n; o += kNormChunk)
+            ch.push_back(NormChunk{(uint64_t)(uintptr_t)regs[s]->d + o * es, (uint32_t)std::min<uint64_t>(kNormChunk, n - o),
+                                   (uint32_t)s});
+        first.push_back((uint32_t)ch.size());
+    }
+}
+
+// out[s] (device) = squared norm of regs[s]; all registers share one precision
+int launch_batch_norm_sqr(Ctx* ctx, const std::vector<Reg*>& regs, double* out) {
+    if (regs.empty()) return YAO_OK;
+    std::vector<NormChunk> ch;
+    std::vector<uint32_t> first;
+    norm_chunks(regs, ch, first);
+    const size_t b_ch = (ch.size() * sizeof(NormChunk) + 255) / 256 * 256,
+                 b_first = (first.size() * sizeof(uint32_t) + 255) / 256 * 256;
+    char* buf = nullptr;
+    YAO_CUDA(cudaMallocAsync((void**)&buf, b_ch + b_first + ch.size() * sizeof(double), ctx->stream));
+    NormChunk* d_ch = (NormChunk*)buf;
+    uint32_t* d_first = (uint32_t*)(buf + b_ch);
+    double* d_part = (double*)(buf + b_ch + b_first);
+    YAO_CUDA(cudaMemcpyAsync(d_ch, ch.data(), ch.size() * sizeof(NormChunk), cudaMemcpyHostToDevice, ctx->stream));
+    YAO_CUDA(cudaMemcpyAsync(d_first, first.data(), first.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+    if (regs[0]->precision == YAO_C128)
+        k_chunk_norm_sqr<double2><<<(unsigned)ch.size(), kRT, 0, ctx->stream>>>(d_ch, d_part);
+    else
+        k_chunk_norm_sqr<float2><<<(unsigned)ch.size(), kRT, 0, ctx->stream>>>(d_ch, d_part);
+    const unsigned g = (unsigned)std::min<size_t>(regs.size(), (size_t)ctx->num_sms * 8);
+    k_slot_sums<<<g, kRT, 0, ctx->stream>>>(d_first, (uint32_t)regs.size(), d_part, out);
+    ctx->launches += 2;
+    YAO_CUDA(cudaGetLastError());
+    YAO_CUDA(cudaFreeAsync(buf, ctx->stream));
+    YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+    return YAO_OK;
+}
+
+// regs[s] /= sqrt(n1[s] / n0[s]) where both are positive (device arrays)
+int launch_batch_rescale(Ctx* ctx, const std::vector<Reg*>& regs, const double* n0, const double* n1) {
+    if (regs.empty()) return YAO_OK;
+    std::vector<NormChunk> ch;
+    std::vector<uint32_t> first;
+    norm_chunks(regs, ch, first);
+    NormChunk* d_ch = nullptr;
+    YAO_CUDA(cudaMallocAsync((void**)&d_ch, ch.size() * sizeof(NormChunk), ctx->stream));
+    YAO_CUDA(cudaMemcpyAsync(d_ch, ch.data(), ch.size() * sizeof(NormChunk), cudaMemcpyHostToDevice, ctx->stream));
+    if (regs[0]->precision == YAO_C128)
+        k_chunk_rescale<double2><<<(unsigned)ch.size(), kRT, 0, ctx->stream>>>(d_ch, n0, n1);
+    else
+        k_chunk_rescale<float2><<<(unsigned)ch.size(), kRT, 0, ctx->stream>>>(d_ch, n0, n1);
+    ctx->launches++;
+    YAO_CUDA(cudaGetLastError());
+    YAO_CUDA(cudaFreeAsync(d_ch, ctx->stream));
+    YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+    return YAO_OK;
+}
+
 }  // namespace yao
