@@ -626,7 +626,6 @@ template <typename V>
 __device__ __forceinline__ void stage_pass(const TileHdr& hdr, unsigned char* smem, int nbuf, const TOp*& ops,
                                            const TSeg*& segs, const typename CoefT<V>::C*& coef) {
     typedef typename CoefT<V>::C C;
-    if (!hdr.staged) return;
     auto a16 = [](size_t x) { return (x + 15) / 16 * 16; };
     unsigned char* p = smem + (size_t)nbuf * ((size_t)1 << hdr.tbits) * sizeof(V);
     TOp* so = (TOp*)p;
@@ -654,7 +653,10 @@ __device__ __forceinline__ void stage_pass(const TileHdr& hdr, unsigned char* sm
 // HBM traffic overlaps the arithmetic even with one CTA per SM.
 // TCK: the pass holds tensor-core ops (complex64 FUSED only); a separate
 // instantiation, so passes without them carry none of its state.
-template <typename V, bool EXACT, int RB, bool TCK>
+// STG: the pass description is copied to shared memory, unconditionally, so
+// every read of it compiles to a shared-memory load (a pointer chosen at run
+// time between global and shared memory would make them generic loads).
+template <typename V, bool EXACT, int RB, bool TCK, bool STG>
 __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
     k_tile_pass(V* __restrict__ st, const TileHdr phdr, const TOp* __restrict__ gops, const TSeg* __restrict__ gsegs,
                 const typename CoefT<V>::C* __restrict__ gcoef, const float* __restrict__ mmat, int* __restrict__ err) {
@@ -670,7 +672,7 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
     const TOp* ops = gops;
     const TSeg* segs = gsegs;
     const typename CoefT<V>::C* coef = gcoef;
-    stage_pass<V>(hdr, smem_raw, 2, ops, segs, coef);
+    if constexpr (STG) stage_pass<V>(hdr, smem_raw, 2, ops, segs, coef);
     tile_offsets(hdr, hoff);
     tile_base_tables(hdr, bt);
     TcCtx tcx;
@@ -678,7 +680,7 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
     if constexpr (use_tc) {
         // operands after the two tiles and the staged pass description (1 KiB aligned)
         size_t off = 2 * ((size_t)1 << hdr.tbits) * sizeof(V);
-        if (hdr.staged) off += staged_bytes(hdr.nops, hdr.nsegs, hdr.ncoef, sizeof(typename CoefT<V>::C));
+        if (STG) off += staged_bytes(hdr.nops, hdr.nsegs, hdr.ncoef, sizeof(typename CoefT<V>::C));
         off = (off + 1023) & ~(size_t)1023;
         tcx.xh = (float*)(smem_raw + off);
         tcx.xl = tcx.xh + kTcRows * kTcKr;
@@ -823,7 +825,7 @@ __global__ void __launch_bounds__(kTileThreads, 1)
                 o = ops + e.ops_off;
                 sgs = segs + e.segs_off;
                 cf = coef + e.coef_off;
-                stage_pass<V>(e.hdr, smem_raw, 1, o, sgs, cf);
+                if (e.hdr.staged) stage_pass<V>(e.hdr, smem_raw, 1, o, sgs, cf);
                 tile_offsets(e.hdr, hoff);
                 staged = (int)ch.entry;
             }
@@ -1173,7 +1175,7 @@ static void fuse_blocks(const std::vector<LGate>& prog, uint32_t nbits, int k, s
 
 // Persistent launch: as many CTAs as fit on the SMs at once (each loops
 // over its tiles with the next one in flight), never more than tiles.
-template <typename V, bool EXACT, int RB, bool TCK>
+template <typename V, bool EXACT, int RB, bool TCK, bool STG>
 static int launch_tile_k(int num_sms, unsigned threads, size_t smem, cudaStream_t s, V* st, const TileHdr& hdr,
                          const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef, const float* mmat,
                          int* err) {
@@ -1183,18 +1185,18 @@ static int launch_tile_k(int num_sms, unsigned threads, size_t smem, cudaStream_
         YAO_CUDA(cudaGetDevice(&dev));
         YAO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
         cudaFuncAttributes fa;
-        YAO_CUDA(cudaFuncGetAttributes(&fa, k_tile_pass<V, EXACT, RB, TCK>));
-        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB, TCK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        YAO_CUDA(cudaFuncGetAttributes(&fa, k_tile_pass<V, EXACT, RB, TCK, STG>));
+        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB, TCK, STG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       optin - (int)fa.sharedSizeBytes));
-        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB, TCK>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB, TCK, STG>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                       cudaSharedmemCarveoutMaxShared));
         attr = true;
     }
     int per_sm = 0;
-    YAO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_pass<V, EXACT, RB, TCK>, (int)threads, smem));
+    YAO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_pass<V, EXACT, RB, TCK, STG>, (int)threads, smem));
     if (per_sm < 1) return fail(YAO_ERR_UNSUPPORTED, "tile pass does not fit on an SM");
     const unsigned grid = (unsigned)std::min<uint64_t>(hdr.ntiles, (uint64_t)per_sm * (uint64_t)num_sms);
-    k_tile_pass<V, EXACT, RB, TCK><<<grid, threads, smem, s>>>(st, hdr, ops, segs, coef, mmat, err);
+    k_tile_pass<V, EXACT, RB, TCK, STG><<<grid, threads, smem, s>>>(st, hdr, ops, segs, coef, mmat, err);
     return YAO_OK;
 }
 
@@ -1203,9 +1205,14 @@ static int launch_tile_rb(int num_sms, unsigned threads, size_t smem, cudaStream
                           const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef, const float* mmat,
                           int* err) {
     if constexpr (sizeof(V) == 8 && !EXACT) {
-        if (hdr.mma) return launch_tile_k<V, EXACT, RB, true>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
+        if (hdr.mma)
+            return hdr.staged
+                       ? launch_tile_k<V, EXACT, RB, true, true>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err)
+                       : launch_tile_k<V, EXACT, RB, true, false>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
     }
-    return launch_tile_k<V, EXACT, RB, false>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
+    return hdr.staged
+               ? launch_tile_k<V, EXACT, RB, false, true>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err)
+               : launch_tile_k<V, EXACT, RB, false, false>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
 }
 
 template <typename V, bool EXACT>
@@ -1258,7 +1265,12 @@ static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
     if (hdr.tbits - hdr.m > kMaxScatterBits) return fail(YAO_ERR_UNSUPPORTED, "tile has too many scattered bits");
     const size_t tile_bytes = ((size_t)1 << hdr.tbits) * sizeof(V);
     const size_t stg = staged_bytes(hdr.nops, hdr.nsegs, hdr.ncoef, sizeof(C));
-    hdr.staged = stg <= kMaxStagedBytes ? 1 : 0;
+    // staged when it fits next to the tiles (and the tensor-core operands),
+    // with 16 KiB left for the kernel's static shared memory
+    static int optin = 0;
+    if (!optin) YAO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    const size_t used = 2 * tile_bytes + (hdr.mma ? 1024 + kTcSmemBytes : 0) + 16 * 1024;
+    hdr.staged = used + stg <= (size_t)optin ? 1 : 0;
     size_t smem = 2 * tile_bytes + (hdr.staged ? stg : 0);
     if (hdr.mma) smem = ((smem + 1023) & ~(size_t)1023) + kTcSmemBytes;
     const unsigned threads = (unsigned)(((uint32_t)1 << pp.hdr.tbits) >> pp.rb);
