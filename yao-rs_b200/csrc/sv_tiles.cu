@@ -45,7 +45,7 @@ struct TileHdr {
     int32_t ncoef;
     int32_t staged;  // op table, segments and coefficients are copied to shared memory
     int32_t mma;     // some wide op of the pass runs on the tensor cores
-    int32_t pad;
+    int32_t dmma;    // complex128 FUSED: some dense 3..5-qubit block runs on the FP64 tensor cores
 };
 
 struct TOp {
@@ -427,9 +427,91 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
     }
 }
 
+// ------------------------------------------------- FP64 tensor-core ops
+//
+// A dense K-qubit block (K = 3..5) of a complex128 FUSED pass as one real
+// FP64 GEMM on the tensor cores (`mma.sync` m8n8k4 f64; tcgen05 has no FP64
+// kind): Y = A X, where column g of X holds the 2^K amplitudes of group g as
+// 2^(K+1) reals (re, im of local index 0, 1, ...) and A is the block's real
+// form (row 2r + o, column 2c + i: Re U[r][c] where o = i, -Im U[r][c] for
+// o = 0, i = 1, Im U[r][c] for o = 1, i = 0), read straight from the complex
+// coefficients, stored by the host with a row stride of 2^K + 2.  Warp w owns the 8-group column blocks w NB .. w NB + NB - 1
+// and every row block, so it reads and writes only its own groups'
+// amplitudes: 2^(RB+1) FP64 accumulators per thread.  Fragments (m8n8k4,
+// lane l): A (8 x 4) element (l / 4, l % 4); B (4 x 8) element (l % 4, l / 4);
+// D (8 x 8) elements (l / 4, 2 (l % 4) + j), j = 0, 1.  `wsw[c]`: swizzled
+// tile offset of local index c.
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+        : "+d"(d0), "+d"(d1)
+        : "d"(a), "d"(b));
+}
+
+template <int K, int RB>
+__device__ __forceinline__ void wide_dmma(const TOp& op, const double2* __restrict__ m, double2* s,
+                                          const uint32_t* wsw) {
+    constexpr int NL = 1 << K, KS = NL / 2, MB = NL / 4;  // k-steps of 4 reals, 8-row blocks
+    constexpr int NB = (1 << (RB + 2)) >> K;                // 8-group column blocks per warp
+    static_assert(NB >= 1, "a warp needs at least one column block");
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t ri = lane & 1, ro = (lane >> 2) & 1, cb = (lane & 3) >> 1;
+    double* sd = (double*)s;
+    double2* tag = nullptr;
+    uint32_t sb[NB];  // swizzled base of the input group of B column l / 4
+#pragma unroll
+    for (int j = 0; j < NB; j++) {
+        uint32_t b = (warp * NB + j) * 8 + (lane >> 2);
+#pragma unroll
+        for (int q = 0; q < K; q++) b = ins0(b, op.ts[q]);
+        sb[j] = swz(b, tag);
+    }
+    double acc[NB][MB][2];
+#pragma unroll
+    for (int j = 0; j < NB; j++)
+#pragma unroll
+        for (int mb = 0; mb < MB; mb++) acc[j][mb][0] = acc[j][mb][1] = 0.0;
+    constexpr int RS = NL + 2;  // padded row stride: the A fragment's 8 coefficients sit in 8 bank groups
+    const double2* mr = m + (size_t)(lane >> 3) * RS + cb;  // row r = 4 mb + l / 8
+#pragma unroll
+    for (int ks = 0; ks < KS; ks++) {
+        const uint32_t wc = wsw[2 * ks + cb];
+        double bf[NB];
+#pragma unroll
+        for (int j = 0; j < NB; j++) bf[j] = sd[2 * (sb[j] ^ wc) + ri];
+#pragma unroll
+        for (int mb = 0; mb < MB; mb++) {
+            const double2 u = mr[(size_t)mb * 4 * RS + 2 * ks];
+            const double a = ro == ri ? u.x : (ro ? u.y : -u.y);
+#pragma unroll
+            for (int j = 0; j < NB; j++) dmma884(acc[j][mb][0], acc[j][mb][1], a, bf[j]);
+        }
+    }
+    __syncwarp();
+    // output group 8 (w NB + j) + 2 (l % 4) + i, row r = 4 mb + l / 8,
+    // component o; groups outside the in-tile controls keep their amplitudes
+#pragma unroll
+    for (int j = 0; j < NB; j++)
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            uint32_t b = (warp * NB + j) * 8 + 2 * (lane & 3) + i;
+#pragma unroll
+            for (int q = 0; q < K; q++) b = ins0(b, op.ts[q]);
+            if ((b & op.lcmask) != op.lcval) continue;
+            const uint32_t so = swz(b, tag);
+#pragma unroll
+            for (int mb = 0; mb < MB; mb++) sd[2 * (so ^ wsw[4 * mb + (lane >> 3)]) + ro] = acc[j][mb][i];
+        }
+}
+
+// Whether a wide op runs on the FP64 tensor cores: dense 3..RB+2 qubits (at
+// most 5), every thread of the tile present (T = threads << RB) in whole warps.
+__host__ __device__ inline bool dmma_op(int k, int rb, uint32_t tbits, uint32_t threads) {
+    return k >= 3 && k <= rb + 2 && k <= 5 && rb >= 2 && ((1u << tbits) >> rb) == threads && threads >= 32;
+}
+
 // The segments of one pass on one tile held in shared memory `s` (the tile
 // at `base`).  Ends with the tile updated in `s` and a __syncthreads().
-template <typename V, bool EXACT, int RB, bool TC = false>
+template <typename V, bool EXACT, int RB, bool TC = false, bool DM = false>
 __device__ __forceinline__ void tile_compute(const TileHdr& hdr, uint64_t base, const TOp* __restrict__ ops,
                                              const TSeg* __restrict__ segs,
                                              const typename CoefT<V>::C* __restrict__ coef, V* s,
@@ -499,6 +581,28 @@ __device__ __forceinline__ void tile_compute(const TileHdr& hdr, uint64_t base, 
             if constexpr (TC) {
                 if (op.mma >= 0) {  // no controls, 5 targets, 2^12 tile (host-checked)
                     wide_tc<V>(op, s, *tcx);
+                    __syncthreads();
+                    continue;
+                }
+            }
+            if constexpr (DM && sizeof(V) == 16 && !EXACT && RB >= 2) {
+                if (dmma_op(op.k, RB, hdr.tbits, nt)) {
+                    __shared__ uint32_t wsw[32];
+                    if (threadIdx.x < (1u << op.k)) {
+                        uint32_t co = 0;
+                        for (int q = 0; q < op.k; q++) co |= (uint32_t)((threadIdx.x >> q) & 1) << op.tl[q];
+                        wsw[threadIdx.x] = swz(co, tag);
+                    }
+                    __syncthreads();
+                    if (on) {
+                        const double2* md = (const double2*)(coef + op.moff);
+                        if (op.k == 3)
+                            wide_dmma<3, RB>(op, md, (double2*)s, wsw);
+                        else if (op.k == 4)
+                            wide_dmma<4, RB>(op, md, (double2*)s, wsw);
+                        else if constexpr (RB >= 3)
+                            wide_dmma<5, RB>(op, md, (double2*)s, wsw);
+                    }
                     __syncthreads();
                     continue;
                 }
@@ -653,10 +757,12 @@ __device__ __forceinline__ void stage_pass(const TileHdr& hdr, unsigned char* sm
 // HBM traffic overlaps the arithmetic even with one CTA per SM.
 // TCK: the pass holds tensor-core ops (complex64 FUSED only); a separate
 // instantiation, so passes without them carry none of its state.
+// DM: the pass holds dense blocks for the FP64 tensor cores (complex128
+// FUSED only); a separate instantiation like TCK.
 // STG: the pass description is copied to shared memory, unconditionally, so
 // every read of it compiles to a shared-memory load (a pointer chosen at run
 // time between global and shared memory would make them generic loads).
-template <typename V, bool EXACT, int RB, bool TCK, bool STG>
+template <typename V, bool EXACT, int RB, bool TCK, bool STG, bool DM = false>
 __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
     k_tile_pass(V* __restrict__ st, const TileHdr phdr, const TOp* __restrict__ gops, const TSeg* __restrict__ gsegs,
                 const typename CoefT<V>::C* __restrict__ gcoef, const float* __restrict__ mmat, int* __restrict__ err) {
@@ -723,7 +829,7 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         if constexpr (use_tc)
             tile_compute<V, EXACT, RB, true>(hdr, base, ops, segs, coef, cur, &tcx);
         else
-            tile_compute<V, EXACT, RB, false>(hdr, base, ops, segs, coef, cur);
+            tile_compute<V, EXACT, RB, false, DM>(hdr, base, ops, segs, coef, cur);
         tile_store<V>(st, hdr, hoff, base, cur);
         __syncthreads();  // `cur` is read out before it receives tile t + 2 * gridDim.x
         V* tmp = cur;
@@ -1175,7 +1281,7 @@ static void fuse_blocks(const std::vector<LGate>& prog, uint32_t nbits, int k, s
 
 // Persistent launch: as many CTAs as fit on the SMs at once (each loops
 // over its tiles with the next one in flight), never more than tiles.
-template <typename V, bool EXACT, int RB, bool TCK, bool STG>
+template <typename V, bool EXACT, int RB, bool TCK, bool STG, bool DM = false>
 static int launch_tile_k(int num_sms, unsigned threads, size_t smem, cudaStream_t s, V* st, const TileHdr& hdr,
                          const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef, const float* mmat,
                          int* err) {
@@ -1185,18 +1291,18 @@ static int launch_tile_k(int num_sms, unsigned threads, size_t smem, cudaStream_
         YAO_CUDA(cudaGetDevice(&dev));
         YAO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
         cudaFuncAttributes fa;
-        YAO_CUDA(cudaFuncGetAttributes(&fa, k_tile_pass<V, EXACT, RB, TCK, STG>));
-        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB, TCK, STG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        YAO_CUDA(cudaFuncGetAttributes(&fa, k_tile_pass<V, EXACT, RB, TCK, STG, DM>));
+        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB, TCK, STG, DM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       optin - (int)fa.sharedSizeBytes));
-        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB, TCK, STG>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        YAO_CUDA(cudaFuncSetAttribute(k_tile_pass<V, EXACT, RB, TCK, STG, DM>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                       cudaSharedmemCarveoutMaxShared));
         attr = true;
     }
     int per_sm = 0;
-    YAO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_pass<V, EXACT, RB, TCK, STG>, (int)threads, smem));
+    YAO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_pass<V, EXACT, RB, TCK, STG, DM>, (int)threads, smem));
     if (per_sm < 1) return fail(YAO_ERR_UNSUPPORTED, "tile pass does not fit on an SM");
     const unsigned grid = (unsigned)std::min<uint64_t>(hdr.ntiles, (uint64_t)per_sm * (uint64_t)num_sms);
-    k_tile_pass<V, EXACT, RB, TCK, STG><<<grid, threads, smem, s>>>(st, hdr, ops, segs, coef, mmat, err);
+    k_tile_pass<V, EXACT, RB, TCK, STG, DM><<<grid, threads, smem, s>>>(st, hdr, ops, segs, coef, mmat, err);
     return YAO_OK;
 }
 
@@ -1209,6 +1315,14 @@ static int launch_tile_rb(int num_sms, unsigned threads, size_t smem, cudaStream
             return hdr.staged
                        ? launch_tile_k<V, EXACT, RB, true, true>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err)
                        : launch_tile_k<V, EXACT, RB, true, false>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
+    }
+    if constexpr (sizeof(V) == 16 && !EXACT && RB >= 2) {
+        if (hdr.dmma)
+            return hdr.staged
+                       ? launch_tile_k<V, EXACT, RB, false, true, true>(num_sms, threads, smem, s, st, hdr, ops, segs, coef,
+                                                                        mmat, err)
+                       : launch_tile_k<V, EXACT, RB, false, false, true>(num_sms, threads, smem, s, st, hdr, ops, segs,
+                                                                         coef, mmat, err);
     }
     return hdr.staged
                ? launch_tile_k<V, EXACT, RB, false, true>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err)
@@ -1232,31 +1346,56 @@ static int launch_tile(int rb, int num_sms, unsigned threads, size_t smem, cudaS
     return fail(YAO_ERR_INVALID_ARGUMENT, "unsupported register-bit count");
 }
 
+// Dense complex128 FUSED blocks on the FP64 tensor cores (YAO_DMMA=0 keeps
+// them on the CUDA cores).
+static bool dmma_enabled() {
+    const char* e = getenv("YAO_DMMA");
+    return !(e && e[0] == '0');
+}
+
 template <typename V, bool EXACT>
 static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
     typedef typename CoefT<V>::C C;
-    std::vector<C> hc(pp.coef.size());
-    for (size_t i = 0; i < pp.coef.size(); i++) {
+    // blocks for the FP64 tensor cores get a copy of their matrix with a
+    // row stride of 2^k + 2 (appended; the op points at it)
+    std::vector<TOp> ops = pp.ops;
+    std::vector<Cx> cx = pp.coef;
+    const unsigned threads = (unsigned)(((uint32_t)1 << pp.hdr.tbits) >> pp.rb);
+    bool dm = false;
+    if (sizeof(V) == 16 && !EXACT && dmma_enabled())
+        for (TOp& op : ops)
+            if (op.cls == GC_DENSE && op.mma < 0 && dmma_op(op.k, pp.rb, (uint32_t)pp.hdr.tbits, threads)) {
+                const size_t nl = (size_t)1 << op.k, m0 = (size_t)op.moff;
+                op.moff = (int32_t)cx.size();
+                for (size_t r = 0; r < nl; r++) {
+                    for (size_t c = 0; c < nl; c++) cx.push_back(pp.coef[m0 + r * nl + c]);
+                    cx.push_back(Cx{0.0, 0.0});
+                    cx.push_back(Cx{0.0, 0.0});
+                }
+                dm = true;
+            }
+    std::vector<C> hc(cx.size());
+    for (size_t i = 0; i < cx.size(); i++) {
         if (sizeof(V) == 16) {
             double2* p = (double2*)&hc[i];
-            *p = make_double2(pp.coef[i].re, pp.coef[i].im);
+            *p = make_double2(cx[i].re, cx[i].im);
         } else {
             float4* p = (float4*)&hc[i];
-            float hr = (float)pp.coef[i].re, hi = (float)pp.coef[i].im;
-            *p = make_float4(hr, hi, (float)(pp.coef[i].re - (double)hr), (float)(pp.coef[i].im - (double)hi));
+            float hr = (float)cx[i].re, hi = (float)cx[i].im;
+            *p = make_float4(hr, hi, (float)(cx[i].re - (double)hr), (float)(cx[i].im - (double)hi));
         }
     }
     // one device buffer: ops | segments | coefficients | tensor-core operands
     // (256-byte aligned parts)
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-    size_t ob = pp.ops.size() * sizeof(TOp), sb = pp.segs.size() * sizeof(TSeg), cb = hc.size() * sizeof(C),
+    size_t ob = ops.size() * sizeof(TOp), sb = pp.segs.size() * sizeof(TSeg), cb = hc.size() * sizeof(C),
            mb = pp.mmat.size() * sizeof(float);
     size_t sb_off = al(ob);
     size_t cb_off = sb_off + al(sb);
     size_t mb_off = cb_off + al(cb);
     void* dbuf = nullptr;
     YAO_CUDA(cudaMallocAsync(&dbuf, mb_off + mb, ctx->stream));
-    YAO_CUDA(cudaMemcpyAsync(dbuf, pp.ops.data(), ob, cudaMemcpyHostToDevice, ctx->stream));
+    YAO_CUDA(cudaMemcpyAsync(dbuf, ops.data(), ob, cudaMemcpyHostToDevice, ctx->stream));
     YAO_CUDA(cudaMemcpyAsync((char*)dbuf + sb_off, pp.segs.data(), sb, cudaMemcpyHostToDevice, ctx->stream));
     YAO_CUDA(cudaMemcpyAsync((char*)dbuf + cb_off, hc.data(), cb, cudaMemcpyHostToDevice, ctx->stream));
     if (mb) YAO_CUDA(cudaMemcpyAsync((char*)dbuf + mb_off, pp.mmat.data(), mb, cudaMemcpyHostToDevice, ctx->stream));
@@ -1271,9 +1410,9 @@ static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
     if (!optin) YAO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
     const size_t used = 2 * tile_bytes + (hdr.mma ? 1024 + kTcSmemBytes : 0) + 16 * 1024;
     hdr.staged = used + stg <= (size_t)optin ? 1 : 0;
+    hdr.dmma = dm ? 1 : 0;
     size_t smem = 2 * tile_bytes + (hdr.staged ? stg : 0);
     if (hdr.mma) smem = ((smem + 1023) & ~(size_t)1023) + kTcSmemBytes;
-    const unsigned threads = (unsigned)(((uint32_t)1 << pp.hdr.tbits) >> pp.rb);
     const TOp* dops = (const TOp*)dbuf;
     const TSeg* dsegs = (const TSeg*)((char*)dbuf + sb_off);
     const C* dcoef = (const C*)((char*)dbuf + cb_off);
