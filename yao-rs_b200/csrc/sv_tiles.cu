@@ -341,27 +341,45 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
             co[tid] = o;
         }
         __syncthreads();
-        // 1. X: row g = tid % 128 (one group per thread), 16-byte chunks jp
-        {
-            const uint32_t g = tid & (kTcRows - 1);
-            uint32_t b = g;
+        // 1. X: row g = tid % 128 (one group per thread), 16-byte chunks jp,
+        // in two halves of K: the MMAs on columns 0..31 run while the
+        // threads build columns 32..63
+        const uint32_t g = tid & (kTcRows - 1);
+        uint32_t gb = g;
 #pragma unroll
-            for (int q = 0; q < kTcK; q++) b = ins0(b, op.ts[q]);
-            for (uint32_t jp = tid >> 7; jp < 16; jp += nt >> 7) {
-                const float2 v0 = t[swz(b | co[2 * jp], (float2*)nullptr)];
-                const float2 v1 = t[swz(b | co[2 * jp + 1], (float2*)nullptr)];
+        for (int q = 0; q < kTcK; q++) gb = ins0(gb, op.ts[q]);
+        auto build_x = [&](uint32_t jp0) {
+            for (uint32_t jp = jp0 + (tid >> 7); jp < jp0 + 8; jp += nt >> 7) {
+                const float2 v0 = t[swz(gb | co[2 * jp], (float2*)nullptr)];
+                const float2 v1 = t[swz(gb | co[2 * jp + 1], (float2*)nullptr)];
                 const float4 h = make_float4(tc::to_tf32(v0.x), tc::to_tf32(v0.y), tc::to_tf32(v1.x), tc::to_tf32(v1.y));
                 const float4 l = make_float4(v0.x - h.x, v0.y - h.y, v1.x - h.z, v1.y - h.w);
                 const uint32_t off = tc_off(g, 4 * jp);
                 *(float4*)((char*)tc.xh + off) = h;
                 *(float4*)((char*)tc.xl + off) = l;
             }
-        }
-        tc::fence_proxy_async();
-        tc::fence_before_sync();
-        __syncthreads();
-        // 2. one thread issues the MMAs: 8 K-steps x 3 products
+            tc::fence_proxy_async();
+            tc::fence_before_sync();
+            __syncthreads();
+        };
+        // 2. one thread issues the MMAs: 8 K-steps x 3 products, 4 K-steps
+        // per half; the B operands are waited for before the first
         bool b_ok = true;
+        constexpr uint32_t idesc = tc::idesc_tf32(kTcRows, kTcN);
+        const uint32_t xh = tc::smem_u32(tc.xh), xl = tc::smem_u32(tc.xl);
+        const uint32_t bh = tc::smem_u32(tc.bh), bl = tc::smem_u32(tc.bl);
+        auto issue = [&](int k0) {
+            tc::fence_after_sync();
+#pragma unroll
+            for (int k8 = k0; k8 < k0 + kTcKr / 16; k8++) {
+                const uint32_t o = (uint32_t)k8 * 256;
+                tc::mma_tf32(tc.tmem, tc::smem_desc(xh + o, 128, kTcSbo), tc::smem_desc(bh + o, 128, kTcSbo), idesc,
+                             k8 > 0);
+                tc::mma_tf32(tc.tmem, tc::smem_desc(xh + o, 128, kTcSbo), tc::smem_desc(bl + o, 128, kTcSbo), idesc, 1);
+                tc::mma_tf32(tc.tmem, tc::smem_desc(xl + o, 128, kTcSbo), tc::smem_desc(bh + o, 128, kTcSbo), idesc, 1);
+            }
+        };
+        build_x(0);
         if (need_b) {
             tc.loaded = op.mma;
             if (tid == 0) {
@@ -371,23 +389,14 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
             }
             tc.bphase ^= 1u;
         }
+        if (tid == 0 && b_ok) issue(0);
+        build_x(8);
         if (tid == 0 && !b_ok) {
             tc.failed = 1;
             atomicExch(tc.err, 1);
             tc::commit(tc.bar);  // no MMA: the barrier completes right away
         } else if (tid == 0) {
-            tc::fence_after_sync();
-            constexpr uint32_t idesc = tc::idesc_tf32(kTcRows, kTcN);
-            const uint32_t xh = tc::smem_u32(tc.xh), xl = tc::smem_u32(tc.xl);
-            const uint32_t bh = tc::smem_u32(tc.bh), bl = tc::smem_u32(tc.bl);
-#pragma unroll
-            for (int k8 = 0; k8 < kTcKr / 8; k8++) {
-                const uint32_t o = (uint32_t)k8 * 256;
-                tc::mma_tf32(tc.tmem, tc::smem_desc(xh + o, 128, kTcSbo), tc::smem_desc(bh + o, 128, kTcSbo), idesc,
-                             k8 > 0);
-                tc::mma_tf32(tc.tmem, tc::smem_desc(xh + o, 128, kTcSbo), tc::smem_desc(bl + o, 128, kTcSbo), idesc, 1);
-                tc::mma_tf32(tc.tmem, tc::smem_desc(xl + o, 128, kTcSbo), tc::smem_desc(bh + o, 128, kTcSbo), idesc, 1);
-            }
+            issue(kTcKr / 16);
             tc::commit(tc.bar);
         }
         // 3. every thread waits for completion (bounded)
