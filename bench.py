@@ -254,8 +254,9 @@ def main():
     ap.add_argument("--qubits", type=int, default=NQ)
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
-    ap.add_argument("--profile-case", default=None, choices=["plain", "tiled", "fused64", "fused32", "fused32_tc", "pass1q",
-                                                             "vqe", "dm", "batch", "vqe_batch"],
+    ap.add_argument("--profile-case", default=None,
+                    choices=["plain", "tiled", "fused64", "fused32", "fused32_tc", "pass1q", "fused64_dmma",
+                             "fused64_cuda", "vqe", "dm", "batch", "vqe_batch"],
                     help="run one small case of a kernel family (for ncu captures) and exit")
     args = ap.parse_args()
     if args.profile_case:
@@ -423,6 +424,15 @@ def profile_case(args):
         c = Y.Circuit.qubits(n, [el for l in range(8) for el in layer_elements(Y, n, l)])
         r = Y.ArrayReg.zero_state(n, Y.C64)
         Y.apply_inplace(c, r, Y.MODE_FUSED, 5)
+    elif args.profile_case in ("fused64_dmma", "fused64_cuda"):
+        # 8 layers as one circuit, complex128 FUSED k = 4 on 2^11 tiles:
+        # dense 3..4-qubit blocks on the FP64 tensor cores, or (cuda) on the
+        # CUDA cores
+        os.environ.update(YAO_TILE_BITS="11", YAO_REG_BITS="3", YAO_AUTOTUNE="0",
+                          YAO_DMMA="1" if args.profile_case == "fused64_dmma" else "0")
+        c = Y.Circuit.qubits(n, [el for l in range(8) for el in layer_elements(Y, n, l)])
+        r = Y.ArrayReg.zero_state(n, Y.C128)
+        Y.apply_inplace(c, r, Y.MODE_FUSED, 4)
     elif args.profile_case == "dm":
         nd = 12
         els = []
