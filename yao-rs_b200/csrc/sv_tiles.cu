@@ -736,16 +736,26 @@ __host__ __device__ inline size_t staged_bytes(int nops, int nsegs, int ncoef, s
 // shared memory when the host marked it `staged`; returns the pointers the
 // tile body reads.
 template <typename V>
-__device__ __forceinline__ void stage_pass(const TileHdr& hdr, unsigned char* smem, int nbuf, const TOp*& ops,
-                                           const TSeg*& segs, const typename CoefT<V>::C*& coef) {
+__device__ __forceinline__ void staged_ptrs(const TileHdr& hdr, unsigned char* smem, int nbuf, TOp*& so, TSeg*& ss,
+                                            typename CoefT<V>::C*& sc) {
     typedef typename CoefT<V>::C C;
     auto a16 = [](size_t x) { return (x + 15) / 16 * 16; };
     unsigned char* p = smem + (size_t)nbuf * ((size_t)1 << hdr.tbits) * sizeof(V);
-    TOp* so = (TOp*)p;
+    so = (TOp*)p;
     p += a16((size_t)hdr.nops * sizeof(TOp));
-    TSeg* ss = (TSeg*)p;
+    ss = (TSeg*)p;
     p += a16((size_t)hdr.nsegs * sizeof(TSeg));
-    C* sc = (C*)p;
+    sc = (C*)p;
+}
+
+template <typename V>
+__device__ __forceinline__ void stage_pass(const TileHdr& hdr, unsigned char* smem, int nbuf, const TOp*& ops,
+                                           const TSeg*& segs, const typename CoefT<V>::C*& coef) {
+    typedef typename CoefT<V>::C C;
+    TOp* so;
+    TSeg* ss;
+    C* sc;
+    staged_ptrs<V>(hdr, smem, nbuf, so, ss, sc);
     {
         const int* src = (const int*)ops;
         int* dst = (int*)so;
@@ -896,7 +906,10 @@ __device__ __forceinline__ uint64_t global_ns() {
 
 constexpr uint64_t kBatchWaitNs = 2000000000ull;  // 2 s
 
-template <typename V, bool EXACT, int RB>
+// STG: every entry's pass description is staged (shared-memory loads only);
+// DM: entries may hold dense blocks for the FP64 tensor cores (complex128
+// FUSED), as in k_tile_pass.
+template <typename V, bool EXACT, int RB, bool STG = false, bool DM = false>
 __global__ void __launch_bounds__(kTileThreads, 1)
     k_batch_tiles(const BatchEntry* __restrict__ entries, const BatchChunk* __restrict__ chunks, uint64_t nchunks,
                   unsigned long long* __restrict__ next, unsigned int* __restrict__ done, int* __restrict__ err,
@@ -944,10 +957,23 @@ __global__ void __launch_bounds__(kTileThreads, 1)
                 tile_offsets(e.hdr, hoff);
                 staged = (int)ch.entry;
             }
+            const TOp* po = o;
+            const TSeg* ps = sgs;
+            const typename CoefT<V>::C* pc = cf;
+            if constexpr (STG) {
+                // the staged copy, addressed from the shared-memory base
+                TOp* so;
+                TSeg* ss;
+                typename CoefT<V>::C* sc;
+                staged_ptrs<V>(e.hdr, smem_raw, 1, so, ss, sc);
+                po = so;
+                ps = ss;
+                pc = sc;
+            }
             for (uint32_t t = ch.tile0; t < ch.tile0 + ch.ntile; t++) {
                 const uint64_t base = insert_zeros(t, e.hdr.tb, e.hdr.tbits);
                 tile_load<V, true>((V*)e.state, e.hdr, hoff, base, (V*)smem_raw);
-                tile_compute<V, EXACT, RB>(e.hdr, base, o, sgs, cf, (V*)smem_raw);
+                tile_compute<V, EXACT, RB, false, DM>(e.hdr, base, po, ps, pc, (V*)smem_raw);
                 tile_store<V>((V*)e.state, e.hdr, hoff, base, (V*)smem_raw);
                 __syncthreads();
             }
@@ -1362,27 +1388,46 @@ static bool dmma_enabled() {
     return !(e && e[0] == '0');
 }
 
+// The coefficients of a pass with every block for the FP64 tensor cores
+// stored with a row stride of 2^k + 2 (in place of its plain copy; each op
+// owns the range from its offset to the next op's); rewrites the ops'
+// offsets.  Returns whether some op was rewritten.
+static bool pad_dmma(std::vector<TOp>& ops, const std::vector<Cx>& in, std::vector<Cx>& out, int rb, uint32_t tbits,
+                     unsigned threads) {
+    out.clear();
+    bool any = false;
+    const size_t first = ops.empty() ? in.size() : (size_t)ops[0].moff;
+    out.insert(out.end(), in.begin(), in.begin() + first);
+    for (size_t i = 0; i < ops.size(); i++) {
+        TOp& op = ops[i];
+        const size_t m0 = (size_t)op.moff, m1 = i + 1 < ops.size() ? (size_t)ops[i + 1].moff : in.size();
+        op.moff = (int32_t)out.size();
+        if (op.cls == GC_DENSE && op.mma < 0 && dmma_op(op.k, rb, tbits, threads)) {
+            const size_t nl = (size_t)1 << op.k;
+            for (size_t r = 0; r < nl; r++) {
+                out.insert(out.end(), in.begin() + m0 + r * nl, in.begin() + m0 + (r + 1) * nl);
+                out.push_back(Cx{0.0, 0.0});
+                out.push_back(Cx{0.0, 0.0});
+            }
+            any = true;
+        } else {
+            out.insert(out.end(), in.begin() + m0, in.begin() + m1);
+        }
+    }
+    return any;
+}
+
 template <typename V, bool EXACT>
 static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
     typedef typename CoefT<V>::C C;
     // blocks for the FP64 tensor cores get a copy of their matrix with a
     // row stride of 2^k + 2 (appended; the op points at it)
     std::vector<TOp> ops = pp.ops;
-    std::vector<Cx> cx = pp.coef;
+    std::vector<Cx> padded;
     const unsigned threads = (unsigned)(((uint32_t)1 << pp.hdr.tbits) >> pp.rb);
-    bool dm = false;
-    if (sizeof(V) == 16 && !EXACT && dmma_enabled())
-        for (TOp& op : ops)
-            if (op.cls == GC_DENSE && op.mma < 0 && dmma_op(op.k, pp.rb, (uint32_t)pp.hdr.tbits, threads)) {
-                const size_t nl = (size_t)1 << op.k, m0 = (size_t)op.moff;
-                op.moff = (int32_t)cx.size();
-                for (size_t r = 0; r < nl; r++) {
-                    for (size_t c = 0; c < nl; c++) cx.push_back(pp.coef[m0 + r * nl + c]);
-                    cx.push_back(Cx{0.0, 0.0});
-                    cx.push_back(Cx{0.0, 0.0});
-                }
-                dm = true;
-            }
+    const bool dm = sizeof(V) == 16 && !EXACT && dmma_enabled() &&
+                    pad_dmma(ops, pp.coef, padded, pp.rb, (uint32_t)pp.hdr.tbits, threads);
+    const std::vector<Cx>& cx = dm ? padded : pp.coef;
     std::vector<C> hc(cx.size());
     for (size_t i = 0; i < cx.size(); i++) {
         if (sizeof(V) == 16) {
@@ -1874,6 +1919,9 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
     std::vector<TSeg> segs;
     std::vector<C> coef;
     size_t max_stg = 0;
+    bool all_staged = true, any_dm = false;
+    std::vector<Cx> padded;
+    const bool use_dm = sizeof(V) == 16 && mode == YAO_MODE_FUSED && dmma_enabled();
     for (size_t level = 0; level < maxpasses; level++)
         for (size_t c = 0; c < progs.size(); c++) {
             if (level >= plans[c].size()) continue;
@@ -1887,9 +1935,20 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
             e.ops_off = (int32_t)ops.size();
             e.segs_off = (int32_t)segs.size();
             e.coef_off = (int32_t)coef.size();
+            const size_t op0 = ops.size();
             ops.insert(ops.end(), pp.ops.begin(), pp.ops.end());
             segs.insert(segs.end(), pp.segs.begin(), pp.segs.end());
-            for (const Cx& x : pp.coef) {
+            // blocks for the FP64 tensor cores: padded rows (see pad_dmma)
+            const std::vector<Cx>* cx = &pp.coef;
+            if (use_dm) {
+                std::vector<TOp> eops(pp.ops);
+                if (pad_dmma(eops, pp.coef, padded, rb, (uint32_t)pp.hdr.tbits, kTileThreads)) {
+                    std::copy(eops.begin(), eops.end(), ops.begin() + op0);
+                    cx = &padded;
+                    any_dm = true;
+                }
+            }
+            for (const Cx& x : *cx) {
                 C cc;
                 if (sizeof(V) == 16) {
                     *(double2*)&cc = make_double2(x.re, x.im);
@@ -1899,10 +1958,13 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
                 }
                 coef.push_back(cc);
             }
-            e.hdr.ncoef = (int32_t)pp.coef.size();
+            e.hdr.ncoef = (int32_t)(coef.size() - (size_t)e.coef_off);
             const size_t stg = staged_bytes(e.hdr.nops, e.hdr.nsegs, e.hdr.ncoef, sizeof(C));
             e.hdr.staged = stg <= kMaxStagedBytes ? 1 : 0;
-            if (e.hdr.staged) max_stg = std::max(max_stg, stg);
+            if (e.hdr.staged)
+                max_stg = std::max(max_stg, stg);
+            else
+                all_staged = false;
             // chunks of consecutive tiles: about 32 per pass of a large
             // circuit, at most 16 tiles each
             const uint32_t nt = (uint32_t)pp.hdr.ntiles;
@@ -1960,7 +2022,12 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
     YAO_CUDA(cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(C), cudaMemcpyHostToDevice, ctx->stream));
     YAO_CUDA(cudaStreamSynchronize(ctx->stream));
     const size_t smem = ((size_t)1 << tbits_cap) * sizeof(V) + max_stg;
-    auto kern = exact ? k_batch_tiles<V, true, 3> : k_batch_tiles<V, false, 3>;
+    // complex128 FUSED batches with blocks for the FP64 tensor cores: the
+    // DM instantiation, reading a staged description from shared memory only
+    // when every entry is staged (the other forms measured no faster so)
+    auto kern = exact ? k_batch_tiles<V, true, 3>
+                      : any_dm ? (all_staged ? k_batch_tiles<V, false, 3, true, true> : k_batch_tiles<V, false, 3, false, true>)
+                               : k_batch_tiles<V, false, 3>;
     YAO_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     YAO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileThreads, smem));
