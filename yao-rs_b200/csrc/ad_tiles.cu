@@ -1,0 +1,495 @@
+// ad_tiles.cu — the adjoint (reverse-sweep) gradient of expect_grad
+// (yao-rs src/ad.rs:75-156) over shared-memory tiles.
+//
+// The per-gate form reads and writes psi and lambda once per gate of the
+// reverse sweep.  Here a pass takes a run of consecutive reverse-sweep steps
+// whose targets all lie in one tile (the low 4 bits plus up to 7 scattered
+// bits), loads psi's and lambda's tile into shared memory, and for every step
+// in order
+//   - accumulates Re <lambda | G psi> over the tile's groups for each
+//     generator G of a parametric gate (only the control-matching branch,
+//     ad.rs:56-64), and
+//   - applies U^dagger to both tiles,
+// then writes both tiles back.  Consecutive steps on the same target bits
+// (a gate's generator dots and its U^dagger step, and the next gate's on the
+// same qubit) enumerate the same groups on the same threads, so no barrier
+// separates them.  Dots are reduced over the warp, added per warp in shared memory
+// (tiles of a CTA in a fixed order), summed over warps per CTA and over CTAs
+// in block order: deterministic for a given launch shape.  Arithmetic is
+// FP64 with FMA; the result is the reverse sweep of the per-gate form up to
+// rounding (~1e-15 relative).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <set>
+#include <vector>
+
+#include "device_common.cuh"
+
+namespace yao {
+
+constexpr int kAdjThreads = 256;
+constexpr int kAdjLowBits = 4;      // contiguous low bits of every tile (256-byte runs)
+constexpr int kAdjScatter = 7;      // scattered tile bits at most
+constexpr int kAdjMaxOps = 96;      // reverse-sweep ops per pass
+constexpr int kAdjMaxSlots = 64;    // generator dots per pass
+
+struct AdjTileOp {
+    int32_t gen;     // 1: accumulate Re <lambda | G psi> into `slot`; 0: U^dagger on psi and lambda
+    int32_t cls;     // GC_X / GC_SWAP / GC_DIAG / GC_DENSE (generators: GC_DENSE)
+    int32_t k;       // 1 or 2 targets
+    int32_t slot;
+    int8_t tl[2];    // local target positions; tl[0] is bit 0 of the gate-local index
+    int8_t sync;     // barrier after this op (the next op moves amplitudes along other bits)
+    int8_t pad[5];
+    uint32_t lcmask, lcval;  // in-tile controls (local positions)
+    uint64_t gcmask, gcval;  // out-of-tile controls (global bits)
+    uint64_t active;         // DIAG: entries different from 1
+    double2 m[16];           // dense 2^k x 2^k row-major, or the 2^k diagonal entries
+};
+static_assert(sizeof(AdjTileOp) % 8 == 0, "AdjTileOp is staged as 64-bit words");
+
+struct AdjTileHdr {
+    int32_t tbits, nops, nslots, nouts;
+    int8_t hb[kAdjScatter];  // global bits of local positions kAdjLowBits ..
+    int8_t pad[1];
+    int8_t outb[64];         // global bits outside the tile, ascending
+    uint64_t ntiles;
+};
+
+__device__ __forceinline__ uint32_t adj_ins0(uint32_t v, int p) {
+    return ((v >> p) << (p + 1)) | (v & ((1u << p) - 1));
+}
+// XOR swizzle of the double2 tile against bank conflicts
+__device__ __forceinline__ uint32_t adj_swz(uint32_t l) { return l ^ ((l >> 3) & 7); }
+
+__device__ __forceinline__ double2 cfma2(double2 acc, double2 a, double2 x) {
+    acc.x = fma(a.x, x.x, acc.x);
+    acc.x = fma(-a.y, x.y, acc.x);
+    acc.y = fma(a.x, x.y, acc.y);
+    acc.y = fma(a.y, x.x, acc.y);
+    return acc;
+}
+__device__ __forceinline__ double2 cmul2(double2 a, double2 x) {
+    return make_double2(fma(a.x, x.x, -a.y * x.y), fma(a.x, x.y, a.y * x.x));
+}
+// Re(conj(l) * y)
+__device__ __forceinline__ double redot(double2 l, double2 y) { return fma(l.x, y.x, l.y * y.y); }
+
+// One reverse-sweep op on the groups of the tile owned by this thread.
+// The op's fields are copied to registers first: the tile stores could
+// alias the staged op as far as the compiler knows, which would reload every
+// coefficient from shared memory for every group.
+template <int K>
+__device__ __forceinline__ void adj_op(const AdjTileOp& sop, double2* sp, double2* sl, uint32_t T, double& dot) {
+    constexpr int NL = 1 << K;
+    struct {
+        int32_t gen, cls;
+        uint32_t lcmask, lcval;
+        uint64_t active;
+        int8_t tl[2];
+        double2 m[NL * NL];
+    } op;
+    op.gen = sop.gen;
+    op.cls = sop.cls;
+    op.lcmask = sop.lcmask;
+    op.lcval = sop.lcval;
+    op.active = sop.active;
+    op.tl[0] = sop.tl[0];
+    op.tl[1] = sop.tl[1];
+#pragma unroll
+    for (int i = 0; i < NL * NL; i++) op.m[i] = sop.m[i];
+    const uint32_t ngroups = T >> K;
+    const int p0 = op.tl[0], p1 = K == 2 ? op.tl[1] : 0;
+    const int lo = K == 2 ? min(p0, p1) : p0, hi = K == 2 ? max(p0, p1) : p0;
+    constexpr int UNR = K == 1 ? 4 : 1;
+#pragma unroll UNR
+    for (uint32_t g = threadIdx.x; g < ngroups; g += blockDim.x) {
+        uint32_t b = adj_ins0(g, lo);
+        if (K == 2) b = adj_ins0(b, hi);
+        if ((b & op.lcmask) != op.lcval) continue;
+        uint32_t idx[NL];
+#pragma unroll
+        for (int q = 0; q < NL; q++) {
+            uint32_t l = b;
+            if (q & 1) l |= 1u << p0;
+            if (K == 2 && (q & 2)) l |= 1u << p1;
+            idx[q] = adj_swz(l);
+        }
+        if (op.gen) {
+            double2 x[NL];
+#pragma unroll
+            for (int q = 0; q < NL; q++) x[q] = sp[idx[q]];
+#pragma unroll
+            for (int r = 0; r < NL; r++) {
+                double2 y = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int c = 0; c < NL; c++) y = cfma2(y, op.m[r * NL + c], x[c]);
+                dot += redot(sl[idx[r]], y);
+            }
+            continue;
+        }
+        if (op.cls == GC_X) {  // K == 1
+            double2 t = sp[idx[0]];
+            sp[idx[0]] = sp[idx[1]];
+            sp[idx[1]] = t;
+            t = sl[idx[0]];
+            sl[idx[0]] = sl[idx[1]];
+            sl[idx[1]] = t;
+        } else if (op.cls == GC_SWAP) {  // K == 2: local indices 1 and 2
+            double2 t = sp[idx[1]];
+            sp[idx[1]] = sp[idx[NL / 2]];
+            sp[idx[NL / 2]] = t;
+            t = sl[idx[1]];
+            sl[idx[1]] = sl[idx[NL / 2]];
+            sl[idx[NL / 2]] = t;
+        } else if (op.cls == GC_DIAG) {
+#pragma unroll
+            for (int q = 0; q < NL; q++)
+                if ((op.active >> q) & 1) {
+                    sp[idx[q]] = cmul2(op.m[q], sp[idx[q]]);
+                    sl[idx[q]] = cmul2(op.m[q], sl[idx[q]]);
+                }
+        } else {
+            double2 x[NL], l[NL];
+#pragma unroll
+            for (int q = 0; q < NL; q++) {
+                x[q] = sp[idx[q]];
+                l[q] = sl[idx[q]];
+            }
+#pragma unroll
+            for (int r = 0; r < NL; r++) {
+                double2 a = make_double2(0.0, 0.0), c2 = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int c = 0; c < NL; c++) {
+                    a = cfma2(a, op.m[r * NL + c], x[c]);
+                    c2 = cfma2(c2, op.m[r * NL + c], l[c]);
+                }
+                sp[idx[r]] = a;
+                sl[idx[r]] = c2;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kAdjThreads, 2)
+    k_adjoint_tiles(double2* __restrict__ psi, double2* __restrict__ lam, const AdjTileHdr phdr,
+                    const AdjTileOp* __restrict__ gops, double* __restrict__ partial) {
+    extern __shared__ __align__(16) unsigned char adj_smem[];
+    __shared__ AdjTileHdr hdr;
+    __shared__ uint64_t hoff[1 << kAdjScatter];
+    if (threadIdx.x == 0) hdr = phdr;
+    __syncthreads();
+    const uint32_t T = 1u << hdr.tbits;
+    const uint32_t nw = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double2* sp = (double2*)adj_smem;
+    double2* sl = sp + T;
+    AdjTileOp* ops = (AdjTileOp*)(sl + T);
+    double* acc = (double*)(ops + hdr.nops);  // [slot][warp]
+    const int nlow = min(kAdjLowBits, hdr.tbits), nh = hdr.tbits - nlow;
+    {
+        const uint64_t* src = (const uint64_t*)gops;
+        uint64_t* dst = (uint64_t*)ops;
+        for (int i = threadIdx.x; i < hdr.nops * (int)(sizeof(AdjTileOp) / 8); i += blockDim.x) dst[i] = src[i];
+        for (int i = threadIdx.x; i < hdr.nslots * (int)nw; i += blockDim.x) acc[i] = 0.0;
+        for (uint32_t h = threadIdx.x; h < (1u << nh); h += blockDim.x) {
+            uint64_t o = 0;
+            for (int j = 0; j < nh; j++) o |= (uint64_t)((h >> j) & 1) << hdr.hb[j];
+            hoff[h] = o;
+        }
+    }
+    __syncthreads();
+    const uint32_t lmask = (1u << nlow) - 1;
+    for (uint64_t t = blockIdx.x; t < hdr.ntiles; t += gridDim.x) {
+        uint64_t base = 0;
+        for (int i = 0; i < hdr.nouts; i++) base |= ((t >> i) & 1) << hdr.outb[i];
+        for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) {
+            const uint64_t gi = base | (l & lmask) | hoff[l >> nlow];
+            const uint32_t s = adj_swz(l);
+            sp[s] = psi[gi];
+            sl[s] = lam[gi];
+        }
+        __syncthreads();
+        for (int oi = 0; oi < hdr.nops; oi++) {
+            const AdjTileOp& op = ops[oi];
+            if ((base & op.gcmask) != op.gcval) {  // uniform over the tile
+                if (op.sync) __syncthreads();
+                continue;
+            }
+            double dot = 0.0;
+            if (op.k == 1)
+                adj_op<1>(op, sp, sl, T, dot);
+            else
+                adj_op<2>(op, sp, sl, T, dot);
+            if (op.gen) {
+                dot = warp_sum(dot);
+                if (lane == 0) acc[op.slot * nw + warp] += dot;
+            }
+            if (op.sync) __syncthreads();
+        }
+        for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) {
+            const uint64_t gi = base | (l & lmask) | hoff[l >> nlow];
+            const uint32_t s = adj_swz(l);
+            psi[gi] = sp[s];
+            lam[gi] = sl[s];
+        }
+        __syncthreads();
+    }
+    // per CTA: slot sums over warps in order
+    for (int sidx = threadIdx.x; sidx < hdr.nslots; sidx += blockDim.x) {
+        double s = 0.0;
+        for (uint32_t w = 0; w < nw; w++) s += acc[sidx * nw + w];
+        partial[(size_t)blockIdx.x * hdr.nslots + sidx] = s;
+    }
+}
+
+// dots[s] = sum over blocks of partial[b][s] (one block per slot, fixed order)
+__global__ void k_adj_slot_sums(const double* __restrict__ partial, int nblocks, int nslots, double* __restrict__ dots) {
+    __shared__ double sm[kAdjThreads / 32];
+    const int s = blockIdx.x;
+    double v = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += partial[(size_t)b * nslots + s];
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sm[w];
+        dots[s] = t;
+    }
+}
+
+// ------------------------------------------------------------------ host
+
+namespace {
+
+struct HostOp {
+    AdjTileOp op;   // tl / lcmask / gcmask filled per pass
+    int tb[2];      // global target bits
+    std::vector<int> cb, cv;
+    int grad = -1;  // generator: gradient index
+};
+
+struct AdjPass {
+    AdjTileHdr hdr;
+    std::vector<AdjTileOp> ops;
+    std::vector<int> slot_grad;  // gradient index of each slot
+};
+
+bool to_host_op(const LGate& g, bool gen, int grad, HostOp& h) {
+    if (g.k < 1 || g.k > 2 || g.nc > 62) return false;
+    memset(&h.op, 0, sizeof(h.op));
+    h.op.gen = gen ? 1 : 0;
+    h.op.cls = gen ? GC_DENSE : g.cls;
+    h.op.k = g.k;
+    const size_t nl = (size_t)1 << g.k;
+    if (h.op.cls == GC_DENSE) {
+        if (g.m.size() != nl * nl) return false;
+    } else if (h.op.cls == GC_DIAG) {
+        if (g.m.size() != nl) return false;
+        for (size_t q = 0; q < nl; q++)
+            if (!(g.m[q].re == 1.0 && g.m[q].im == 0.0)) h.op.active |= (uint64_t)1 << q;
+    } else if (h.op.cls == GC_X) {
+        if (g.k != 1) return false;
+    } else if (h.op.cls == GC_SWAP) {
+        if (g.k != 2) return false;
+    } else {
+        return false;
+    }
+    for (size_t i = 0; i < g.m.size() && i < 16; i++) h.op.m[i] = make_double2(g.m[i].re, g.m[i].im);
+    h.tb[0] = g.tb[0];
+    h.tb[1] = g.k == 2 ? g.tb[1] : -1;
+    h.cb.assign(g.cb, g.cb + g.nc);
+    h.cv.assign(g.cv, g.cv + g.nc);
+    h.grad = grad;
+    return true;
+}
+
+// Greedy passes: consecutive ops while the targets above the low bits fit
+// the scattered tile bits, and the op / slot limits hold.
+void plan_adj(const std::vector<HostOp>& hops, uint32_t nbits, std::vector<AdjPass>& out) {
+    const int tbits = (int)std::min<uint32_t>(nbits, kAdjLowBits + kAdjScatter);
+    const int nlow = std::min(kAdjLowBits, tbits), S = tbits - nlow;
+    size_t i = 0;
+    while (i < hops.size()) {
+        std::set<int> H;
+        size_t j = i;
+        int nslots = 0;
+        while (j < hops.size() && (int)(j - i) < kAdjMaxOps) {
+            std::set<int> need;
+            for (int q = 0; q < hops[j].op.k; q++)
+                if (hops[j].tb[q] >= nlow && !H.count(hops[j].tb[q])) need.insert(hops[j].tb[q]);
+            if ((int)(H.size() + need.size()) > S) break;
+            if (hops[j].op.gen && nslots >= kAdjMaxSlots) break;
+            H.insert(need.begin(), need.end());
+            if (hops[j].op.gen) nslots++;
+            j++;
+        }
+        // the tile's scattered bits: the targets', then the lowest free bits
+        for (int b = nlow; (int)H.size() < S && b < (int)nbits; b++) H.insert(b);
+        AdjPass pass;
+        memset(&pass.hdr, 0, sizeof(pass.hdr));
+        pass.hdr.tbits = tbits;
+        int local[64];
+        for (int b = 0; b < 64; b++) local[b] = -1;
+        for (int b = 0; b < nlow; b++) local[b] = b;
+        int pos = nlow;
+        for (int b : H) {
+            pass.hdr.hb[pos - nlow] = (int8_t)b;
+            local[b] = pos++;
+        }
+        int no = 0;
+        for (int b = 0; b < (int)nbits; b++)
+            if (local[b] < 0) pass.hdr.outb[no++] = (int8_t)b;
+        pass.hdr.nouts = no;
+        pass.hdr.ntiles = (uint64_t)1 << (nbits - tbits);
+        for (size_t q = i; q < j; q++) {
+            AdjTileOp op = hops[q].op;
+            op.tl[0] = (int8_t)local[hops[q].tb[0]];
+            if (op.k == 2) op.tl[1] = (int8_t)local[hops[q].tb[1]];
+            for (size_t c = 0; c < hops[q].cb.size(); c++) {
+                const int b = hops[q].cb[c];
+                if (local[b] >= 0) {
+                    op.lcmask |= 1u << local[b];
+                    if (hops[q].cv[c]) op.lcval |= 1u << local[b];
+                } else {
+                    op.gcmask |= (uint64_t)1 << b;
+                    if (hops[q].cv[c]) op.gcval |= (uint64_t)1 << b;
+                }
+            }
+            if (op.gen) {
+                op.slot = (int32_t)pass.slot_grad.size();
+                pass.slot_grad.push_back(hops[q].grad);
+            }
+            pass.ops.push_back(op);
+        }
+        // a thread owns the same groups in consecutive ops on the same
+        // target positions (controls only skip groups): a barrier is needed
+        // only before an op that moves amplitudes along other bits
+        for (size_t q = 0; q < pass.ops.size(); q++) {
+            AdjTileOp& a = pass.ops[q];
+            bool same = false;
+            if (q + 1 < pass.ops.size()) {
+                const AdjTileOp& b = pass.ops[q + 1];
+                same = a.k == b.k && ((a.k == 1 && a.tl[0] == b.tl[0]) ||
+                                      (a.k == 2 && std::min(a.tl[0], a.tl[1]) == std::min(b.tl[0], b.tl[1]) &&
+                                       std::max(a.tl[0], a.tl[1]) == std::max(b.tl[0], b.tl[1])));
+            }
+            a.sync = (int8_t)(same ? 0 : 1);
+        }
+        pass.hdr.nops = (int32_t)pass.ops.size();
+        pass.hdr.nslots = (int32_t)pass.slot_grad.size();
+        out.push_back(std::move(pass));
+        i = j;
+    }
+}
+
+}  // namespace
+
+// The reverse sweep of expect_grad over tiles; psi holds the forward state
+// and lambda = H psi on entry.  Returns YAO_ERR_UNSUPPORTED, with nothing
+// launched, when some step is not a 1- or 2-qubit gate (the caller then runs
+// the per-gate form).  grad receives 2 Re <lambda | G psi> per parameter.
+int adjoint_tiles(Ctx* ctx, Reg* psi, Reg* lam, const Circuit* c, double* grad, size_t np) {
+    const uint32_t n = psi->nbits;
+    if (n < 3 || n > 62 || psi->precision != YAO_C128) return YAO_ERR_UNSUPPORTED;
+    std::vector<HostOp> hops;
+    size_t slot = np;
+    for (size_t ei = c->elems.size(); ei-- > 0;) {
+        const Element& el = c->elems[ei];
+        if (el.kind != YAO_ELEM_GATE) continue;
+        const GateElem& g = el.g;
+        std::vector<LGate> dag;
+        lower_gate(gate_dagger(g), n, 0, false, dag);
+        const int npar = gate_num_params(g.type);
+        if (npar > 0) {
+            if (slot < (size_t)npar) return YAO_ERR_UNSUPPORTED;
+            for (int i = 0; i < npar; i++) {
+                std::vector<Cx> gm;
+                uint32_t gd;
+                gate_generator(g, i, gm, gd);
+                HostOp h;
+                if (!to_host_op(lower_matrix(gm, gd, false, g.targets, g.ctrls, g.cfgs, n, 0), true,
+                                (int)(slot - npar + i), h))
+                    return YAO_ERR_UNSUPPORTED;
+                hops.push_back(h);
+            }
+            slot -= npar;
+        }
+        for (const LGate& d : dag) {
+            HostOp h;
+            if (!to_host_op(d, false, -1, h)) return YAO_ERR_UNSUPPORTED;
+            hops.push_back(h);
+        }
+    }
+    std::vector<AdjPass> passes;
+    plan_adj(hops, n, passes);
+    if (passes.empty()) return YAO_OK;
+    size_t nops = 0, ndots = 0;
+    for (const AdjPass& p : passes) {
+        nops += p.ops.size();
+        ndots += p.slot_grad.size();
+    }
+    const int tbits = passes[0].hdr.tbits;
+    const size_t tile_bytes = (size_t)2 * ((size_t)1 << tbits) * sizeof(double2);
+    // the attribute covers the largest pass (2^11-amplitude tiles, every op
+    // and slot in use)
+    const size_t smem_max = (size_t)2 * ((size_t)1 << (kAdjLowBits + kAdjScatter)) * sizeof(double2) +
+                            kAdjMaxOps * sizeof(AdjTileOp) + (size_t)kAdjMaxSlots * (kAdjThreads / 32) * 8;
+    static bool attr = false;
+    if (!attr) {
+        YAO_CUDA(cudaFuncSetAttribute(k_adjoint_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
+        attr = true;
+    }
+    int per_sm = 0;
+    YAO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint_tiles, kAdjThreads, smem_max));
+    const uint64_t ntiles = (uint64_t)1 << (n - tbits);
+    const int grid = (int)std::min<uint64_t>(ntiles, (uint64_t)std::max(1, per_sm) * (uint64_t)ctx->num_sms);
+    // device buffers: every pass's ops, the CTA partials, every pass's dots
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t b_ops = al(std::max<size_t>(1, nops) * sizeof(AdjTileOp)),
+                 b_part = al((size_t)grid * kAdjMaxSlots * sizeof(double)), b_dots = al(std::max<size_t>(1, ndots) * 8);
+    char* buf = nullptr;
+    YAO_CUDA(cudaMallocAsync((void**)&buf, b_ops + b_part + b_dots, ctx->stream));
+    AdjTileOp* d_ops = (AdjTileOp*)buf;
+    double* d_part = (double*)(buf + b_ops);
+    double* d_dots = (double*)(buf + b_ops + b_part);
+    {
+        std::vector<AdjTileOp> all;
+        all.reserve(nops);
+        for (const AdjPass& p : passes) all.insert(all.end(), p.ops.begin(), p.ops.end());
+        YAO_CUDA(cudaMemcpyAsync(d_ops, all.data(), all.size() * sizeof(AdjTileOp), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    }
+    size_t ooff = 0, doff = 0;
+    for (const AdjPass& p : passes) {
+        const size_t smem =
+            tile_bytes + p.ops.size() * sizeof(AdjTileOp) + (size_t)p.slot_grad.size() * (kAdjThreads / 32) * 8;
+        {
+            ProfScope prof(ctx, "adjoint_tiles", (double)((uint64_t)1 << n) * 4.0 * sizeof(double2));
+            k_adjoint_tiles<<<grid, kAdjThreads, smem, ctx->stream>>>((double2*)psi->d, (double2*)lam->d, p.hdr,
+                                                                       d_ops + ooff, d_part);
+        }
+        ctx->launches++;
+        YAO_CUDA(cudaGetLastError());
+        if (!p.slot_grad.empty()) {
+            k_adj_slot_sums<<<(unsigned)p.slot_grad.size(), kAdjThreads, 0, ctx->stream>>>(
+                d_part, grid, (int)p.slot_grad.size(), d_dots + doff);
+            ctx->launches++;
+            YAO_CUDA(cudaGetLastError());
+        }
+        ooff += p.ops.size();
+        doff += p.slot_grad.size();
+    }
+    std::vector<double> dots(std::max<size_t>(1, ndots));
+    if (ndots)
+        YAO_CUDA(cudaMemcpyAsync(dots.data(), d_dots, ndots * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    YAO_CUDA(cudaFreeAsync(buf, ctx->stream));
+    YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+    doff = 0;
+    for (const AdjPass& p : passes)
+        for (size_t s = 0; s < p.slot_grad.size(); s++) grad[p.slot_grad[s]] = 2.0 * dots[doff++];
+    return YAO_OK;
+}
+
+}  // namespace yao

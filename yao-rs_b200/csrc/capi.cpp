@@ -1198,7 +1198,8 @@ int yao_expect_grad(const yao_term* terms, size_t nterms, const yao_circuit* cc,
             yao_reg_free(*b);
         }
     } guard{&psi, &lam};
-    s = launch_program(ctx, psi, lowered(c), YAO_MODE_PLAIN, 0);
+    // forward pass: TILED (bit-identical to PLAIN, tiles of many gates)
+    s = launch_program(ctx, psi, lowered(c), YAO_MODE_TILED, 0);
     if (s) return s;
     std::vector<Cx> vals;
     s = expect_terms(ctx, psi, mt, vals);
@@ -1217,6 +1218,13 @@ int yao_expect_grad(const yao_term* terms, size_t nterms, const yao_circuit* cc,
     lam = static_cast<yao_reg*>(l);
     s = build_lambda(ctx, psi, mt, lam);
     if (s) return s;
+    // reverse sweep over shared-memory tiles of psi and lambda; circuits with
+    // wider gates (or YAO_ADJ_TILES=0) take the per-gate form below
+    const char* at = getenv("YAO_ADJ_TILES");
+    if (!(at && at[0] == '0')) {
+        s = adjoint_tiles(ctx, psi, lam, c, grad, np);
+        if (s != YAO_ERR_UNSUPPORTED) return s;
+    }
     size_t slot = np;
     for (size_t ei = c->elems.size(); ei-- > 0;) {
         const Element& el = c->elems[ei];

@@ -200,6 +200,7 @@ int launch_deterministic_state(Ctx* ctx, Reg* r);
 int launch_convert(Ctx* ctx, const Reg* src, Reg* dst);
 int reduce_norm_sqr(Ctx* ctx, const Reg* r, double* out);
 int launch_scale(Ctx* ctx, Reg* r, double inv_norm);
+int adjoint_tiles(Ctx* ctx, Reg* psi, Reg* lam, const Circuit* c, double* grad, size_t np);
 int launch_batch_norm_sqr(Ctx* ctx, const std::vector<Reg*>& regs, double* out);
 int launch_batch_rescale(Ctx* ctx, const std::vector<Reg*>& regs, const double* n0, const double* n1);
 int reduce_inner(Ctx* ctx, const Reg* a, const Reg* b, Cx* out);
