@@ -77,99 +77,108 @@ __device__ __forceinline__ double2 cmul2(double2 a, double2 x) {
 __device__ __forceinline__ double redot(double2 l, double2 y) { return fma(l.x, y.x, l.y * y.y); }
 
 // One reverse-sweep op on the groups of the tile owned by this thread.
-// The op's fields are copied to registers first: the tile stores could
-// alias the staged op as far as the compiler knows, which would reload every
-// coefficient from shared memory for every group.
+// A run of up to kAdjRun consecutive ops on the same target positions (in
+// the same order): each group the thread owns is loaded once, every op of
+// the run is applied (or its dot accumulated) in registers, and the group is
+// stored once.  Ops whose controls do not match a group skip it.
+constexpr int kAdjRun = 8;
+
 template <int K>
-__device__ __forceinline__ void adj_op(const AdjTileOp& sop, double2* sp, double2* sl, uint32_t T, double& dot) {
+__device__ __forceinline__ void adj_run(const AdjTileOp* rops, int nr, uint64_t base, double2* sp, double2* sl,
+                                        uint32_t T, double* acc, uint32_t nw) {
     constexpr int NL = 1 << K;
-    struct {
-        int32_t gen, cls;
-        uint32_t lcmask, lcval;
-        uint64_t active;
-        int8_t tl[2];
-        double2 m[NL * NL];
-    } op;
-    op.gen = sop.gen;
-    op.cls = sop.cls;
-    op.lcmask = sop.lcmask;
-    op.lcval = sop.lcval;
-    op.active = sop.active;
-    op.tl[0] = sop.tl[0];
-    op.tl[1] = sop.tl[1];
-#pragma unroll
-    for (int i = 0; i < NL * NL; i++) op.m[i] = sop.m[i];
     const uint32_t ngroups = T >> K;
-    const int p0 = op.tl[0], p1 = K == 2 ? op.tl[1] : 0;
+    const int p0 = rops[0].tl[0], p1 = K == 2 ? rops[0].tl[1] : 0;
     const int lo = K == 2 ? min(p0, p1) : p0, hi = K == 2 ? max(p0, p1) : p0;
-    constexpr int UNR = K == 1 ? 4 : 1;
-#pragma unroll UNR
+    bool on[kAdjRun];
+    double dot[kAdjRun];
+#pragma unroll
+    for (int j = 0; j < kAdjRun; j++) {
+        on[j] = j < nr && (base & rops[j].gcmask) == rops[j].gcval;  // uniform over the tile
+        dot[j] = 0.0;
+    }
     for (uint32_t g = threadIdx.x; g < ngroups; g += blockDim.x) {
         uint32_t b = adj_ins0(g, lo);
         if (K == 2) b = adj_ins0(b, hi);
-        if ((b & op.lcmask) != op.lcval) continue;
         uint32_t idx[NL];
+        double2 x[NL], l[NL];
 #pragma unroll
         for (int q = 0; q < NL; q++) {
-            uint32_t l = b;
-            if (q & 1) l |= 1u << p0;
-            if (K == 2 && (q & 2)) l |= 1u << p1;
-            idx[q] = adj_swz(l);
+            uint32_t li = b;
+            if (q & 1) li |= 1u << p0;
+            if (K == 2 && (q & 2)) li |= 1u << p1;
+            idx[q] = adj_swz(li);
+            x[q] = sp[idx[q]];
+            l[q] = sl[idx[q]];
         }
-        if (op.gen) {
-            double2 x[NL];
 #pragma unroll
-            for (int q = 0; q < NL; q++) x[q] = sp[idx[q]];
+        for (int j = 0; j < kAdjRun; j++) {
+            if (!on[j]) continue;
+            const AdjTileOp& op = rops[j];
+            if ((b & op.lcmask) != op.lcval) continue;
+            if (op.gen) {
 #pragma unroll
-            for (int r = 0; r < NL; r++) {
-                double2 y = make_double2(0.0, 0.0);
+                for (int r = 0; r < NL; r++) {
+                    double2 y = make_double2(0.0, 0.0);
 #pragma unroll
-                for (int c = 0; c < NL; c++) y = cfma2(y, op.m[r * NL + c], x[c]);
-                dot += redot(sl[idx[r]], y);
+                    for (int c = 0; c < NL; c++) y = cfma2(y, op.m[r * NL + c], x[c]);
+                    dot[j] += redot(l[r], y);
+                }
+            } else if (op.cls == GC_X) {
+                double2 t = x[0];
+                x[0] = x[1];
+                x[1] = t;
+                t = l[0];
+                l[0] = l[1];
+                l[1] = t;
+            } else if (op.cls == GC_SWAP) {
+                double2 t = x[1];
+                x[1] = x[NL / 2];
+                x[NL / 2] = t;
+                t = l[1];
+                l[1] = l[NL / 2];
+                l[NL / 2] = t;
+            } else if (op.cls == GC_DIAG) {
+#pragma unroll
+                for (int q = 0; q < NL; q++)
+                    if ((op.active >> q) & 1) {
+                        x[q] = cmul2(op.m[q], x[q]);
+                        l[q] = cmul2(op.m[q], l[q]);
+                    }
+            } else {
+                double2 nx[NL], nl[NL];
+#pragma unroll
+                for (int r = 0; r < NL; r++) {
+                    double2 a = make_double2(0.0, 0.0), c2 = make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int c = 0; c < NL; c++) {
+                        const double2 mm = op.m[r * NL + c];
+                        a = cfma2(a, mm, x[c]);
+                        c2 = cfma2(c2, mm, l[c]);
+                    }
+                    nx[r] = a;
+                    nl[r] = c2;
+                }
+#pragma unroll
+                for (int q = 0; q < NL; q++) {
+                    x[q] = nx[q];
+                    l[q] = nl[q];
+                }
             }
-            continue;
         }
-        if (op.cls == GC_X) {  // K == 1
-            double2 t = sp[idx[0]];
-            sp[idx[0]] = sp[idx[1]];
-            sp[idx[1]] = t;
-            t = sl[idx[0]];
-            sl[idx[0]] = sl[idx[1]];
-            sl[idx[1]] = t;
-        } else if (op.cls == GC_SWAP) {  // K == 2: local indices 1 and 2
-            double2 t = sp[idx[1]];
-            sp[idx[1]] = sp[idx[NL / 2]];
-            sp[idx[NL / 2]] = t;
-            t = sl[idx[1]];
-            sl[idx[1]] = sl[idx[NL / 2]];
-            sl[idx[NL / 2]] = t;
-        } else if (op.cls == GC_DIAG) {
 #pragma unroll
-            for (int q = 0; q < NL; q++)
-                if ((op.active >> q) & 1) {
-                    sp[idx[q]] = cmul2(op.m[q], sp[idx[q]]);
-                    sl[idx[q]] = cmul2(op.m[q], sl[idx[q]]);
-                }
-        } else {
-            double2 x[NL], l[NL];
-#pragma unroll
-            for (int q = 0; q < NL; q++) {
-                x[q] = sp[idx[q]];
-                l[q] = sl[idx[q]];
-            }
-#pragma unroll
-            for (int r = 0; r < NL; r++) {
-                double2 a = make_double2(0.0, 0.0), c2 = make_double2(0.0, 0.0);
-#pragma unroll
-                for (int c = 0; c < NL; c++) {
-                    a = cfma2(a, op.m[r * NL + c], x[c]);
-                    c2 = cfma2(c2, op.m[r * NL + c], l[c]);
-                }
-                sp[idx[r]] = a;
-                sl[idx[r]] = c2;
-            }
+        for (int q = 0; q < NL; q++) {
+            sp[idx[q]] = x[q];
+            sl[idx[q]] = l[q];
         }
     }
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < kAdjRun; j++)
+        if (on[j] && rops[j].gen) {
+            const double d = warp_sum(dot[j]);
+            if (lane == 0) acc[rops[j].slot * nw + warp] += d;
+        }
 }
 
 __global__ void __launch_bounds__(kAdjThreads, 2)
@@ -181,7 +190,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2)
     if (threadIdx.x == 0) hdr = phdr;
     __syncthreads();
     const uint32_t T = 1u << hdr.tbits;
-    const uint32_t nw = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t nw = blockDim.x >> 5;
     double2* sp = (double2*)adj_smem;
     double2* sl = sp + T;
     AdjTileOp* ops = (AdjTileOp*)(sl + T);
@@ -203,29 +212,29 @@ __global__ void __launch_bounds__(kAdjThreads, 2)
     for (uint64_t t = blockIdx.x; t < hdr.ntiles; t += gridDim.x) {
         uint64_t base = 0;
         for (int i = 0; i < hdr.nouts; i++) base |= ((t >> i) & 1) << hdr.outb[i];
+        // the tile's copies are issued back to back (cp.async), then waited for
         for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) {
             const uint64_t gi = base | (l & lmask) | hoff[l >> nlow];
             const uint32_t s = adj_swz(l);
-            sp[s] = psi[gi];
-            sl[s] = lam[gi];
+            const uint32_t dp = (uint32_t)__cvta_generic_to_shared(&sp[s]);
+            const uint32_t dl = (uint32_t)__cvta_generic_to_shared(&sl[s]);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dp), "l"(&psi[gi]) : "memory");
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dl), "l"(&lam[gi]) : "memory");
         }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         __syncthreads();
-        for (int oi = 0; oi < hdr.nops; oi++) {
-            const AdjTileOp& op = ops[oi];
-            if ((base & op.gcmask) != op.gcval) {  // uniform over the tile
-                if (op.sync) __syncthreads();
-                continue;
-            }
-            double dot = 0.0;
-            if (op.k == 1)
-                adj_op<1>(op, sp, sl, T, dot);
+        for (int oi = 0; oi < hdr.nops;) {
+            // the run ends at the first op followed by a barrier
+            int e = oi;
+            while (!ops[e].sync) e++;
+            e++;
+            if (ops[oi].k == 1)
+                adj_run<1>(ops + oi, e - oi, base, sp, sl, T, acc, nw);
             else
-                adj_op<2>(op, sp, sl, T, dot);
-            if (op.gen) {
-                dot = warp_sum(dot);
-                if (lane == 0) acc[op.slot * nw + warp] += dot;
-            }
-            if (op.sync) __syncthreads();
+                adj_run<2>(ops + oi, e - oi, base, sp, sl, T, acc, nw);
+            __syncthreads();
+            oi = e;
         }
         for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) {
             const uint64_t gi = base | (l & lmask) | hoff[l >> nlow];
@@ -366,16 +375,18 @@ void plan_adj(const std::vector<HostOp>& hops, uint32_t nbits, std::vector<AdjPa
         // a thread owns the same groups in consecutive ops on the same
         // target positions (controls only skip groups): a barrier is needed
         // only before an op that moves amplitudes along other bits
+        int run = 0;
         for (size_t q = 0; q < pass.ops.size(); q++) {
             AdjTileOp& a = pass.ops[q];
             bool same = false;
             if (q + 1 < pass.ops.size()) {
                 const AdjTileOp& b = pass.ops[q + 1];
-                same = a.k == b.k && ((a.k == 1 && a.tl[0] == b.tl[0]) ||
-                                      (a.k == 2 && std::min(a.tl[0], a.tl[1]) == std::min(b.tl[0], b.tl[1]) &&
-                                       std::max(a.tl[0], a.tl[1]) == std::max(b.tl[0], b.tl[1])));
+                same = a.k == b.k && a.tl[0] == b.tl[0] && (a.k == 1 || a.tl[1] == b.tl[1]);
             }
+            run++;
+            if (run >= kAdjRun) same = false;
             a.sync = (int8_t)(same ? 0 : 1);
+            if (a.sync) run = 0;
         }
         pass.hdr.nops = (int32_t)pass.ops.size();
         pass.hdr.nslots = (int32_t)pass.slot_grad.size();
