@@ -581,10 +581,10 @@ def batch_extra(Y, A, torch, stream, dev, timed):
     forms = {}
     for name, mode, prec, k in (("tiled_c128", Y.MODE_TILED, Y.C128, 0), ("fused_c128_auto", Y.MODE_FUSED, Y.C128, 0),
                                 ("fused_c64_auto", Y.MODE_FUSED, Y.C64, 0), ("fused_c64_k2", Y.MODE_FUSED, Y.C64, 2)):
-        # warm-up on 64 of the circuits (the batch autotuner runs here)
-        wi = [max(range(len(draws)), key=lambda i: draws[i][0])] + list(range(63))
-        warm = [Y.ArrayReg.zero_state(draws[i][0], prec, device=dev) for i in wi]
-        Y.batch_apply([circuits[i] for i in wi], warm, mode, k)
+        # warm-up: the whole batch once (the batch autotuner runs here, and
+        # the kept table buffers reach their size)
+        warm = [Y.ArrayReg.zero_state(n, prec, device=dev) for n, _ in draws]
+        Y.batch_apply(circuits, warm, mode, k)
         del warm
         regs = [Y.ArrayReg.zero_state(n, prec, device=dev) for n, _ in draws]
         t0 = time.perf_counter()

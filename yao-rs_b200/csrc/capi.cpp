@@ -353,6 +353,8 @@ int yao_ctx_destroy(yao_ctx* c) {
     if (c->scratch) cudaFree(c->scratch);
     if (c->d_err) cudaFree(c->d_err);
     if (c->host_pinned) cudaFreeHost(c->host_pinned);
+    if (c->batch_dev) cudaFree(c->batch_dev);
+    if (c->batch_host) cudaFreeHost(c->batch_host);
     cudaStreamDestroy(c->stream);
     delete c;
     return YAO_OK;

@@ -28,6 +28,7 @@
 #include <string>
 #include <thread>
 #include <atomic>
+#include <chrono>
 #include <vector>
 
 #include "device_common.cuh"
@@ -1417,6 +1418,53 @@ static bool pad_dmma(std::vector<TOp>& ops, const std::vector<Cx>& in, std::vect
     return any;
 }
 
+// Coefficient count of a pass after pad_dmma (without building it).
+static size_t padded_count(const std::vector<TOp>& ops, size_t ncoef, int rb, uint32_t tbits, unsigned threads) {
+    size_t n = ops.empty() ? ncoef : (size_t)ops[0].moff;
+    for (size_t i = 0; i < ops.size(); i++) {
+        const TOp& op = ops[i];
+        const size_t m0 = (size_t)op.moff, m1 = i + 1 < ops.size() ? (size_t)ops[i + 1].moff : ncoef;
+        if (op.cls == GC_DENSE && op.mma < 0 && dmma_op(op.k, rb, tbits, threads)) {
+            const size_t nl = (size_t)1 << op.k;
+            n += nl * (nl + 2);
+        } else {
+            n += m1 - m0;
+        }
+    }
+    return n;
+}
+
+// Grow a kept device / pinned host buffer to at least `bytes` (by 1.25x).
+static int grow_dev(void** p, size_t* have, size_t bytes, cudaStream_t s) {
+    if (bytes <= *have) return YAO_OK;
+    const size_t nb = std::max(bytes, *have + *have / 4);
+    if (*p) {
+        YAO_CUDA(cudaStreamSynchronize(s));
+        YAO_CUDA(cudaFree(*p));
+        *p = nullptr;
+        *have = 0;
+    }
+    if (cudaMalloc(p, nb) != cudaSuccess) {
+        *p = nullptr;
+        return fail(YAO_ERR_OUT_OF_MEMORY, "cannot allocate the batch tables");
+    }
+    *have = nb;
+    return YAO_OK;
+}
+static int grow_host(void** p, size_t* have, size_t bytes) {
+    if (bytes <= *have) return YAO_OK;
+    const size_t nb = std::max(bytes, *have + *have / 4);
+    if (*p) cudaFreeHost(*p);
+    *p = nullptr;
+    *have = 0;
+    if (cudaMallocHost(p, nb) != cudaSuccess) {
+        *p = nullptr;
+        return fail(YAO_ERR_OUT_OF_MEMORY, "cannot allocate pinned memory for the batch tables");
+    }
+    *have = nb;
+    return YAO_OK;
+}
+
 template <typename V, bool EXACT>
 static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
     typedef typename CoefT<V>::C C;
@@ -1869,10 +1917,24 @@ int autotune_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t m
 
 // ------------------------------------------------------------ batch host
 
+// YAO_BATCH_TIMING=1: host phase times of a batched launch on stderr.
+struct PhaseTimer {
+    bool on;
+    std::chrono::steady_clock::time_point t0;
+    PhaseTimer() : on(getenv("YAO_BATCH_TIMING") != nullptr), t0(std::chrono::steady_clock::now()) {}
+    void mark(const char* what) {
+        if (!on) return;
+        const auto t = std::chrono::steady_clock::now();
+        fprintf(stderr, "batch %s: %.1f ms\n", what, std::chrono::duration<double, std::milli>(t - t0).count());
+        t0 = t;
+    }
+};
+
 template <typename V>
 static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs, const std::vector<Reg*>& regs,
                    int32_t mode, const TileConfig& cfg) {
     typedef typename CoefT<V>::C C;
+    PhaseTimer ptimer;
     const int tbits_cap = std::min(cfg.tbits, 12), rb = 3;
     const int k = cfg.k;
     const bool exact = mode == YAO_MODE_TILED && sizeof(V) == 16;
@@ -1912,42 +1974,90 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
         if (bad[c] == 2) return fail(YAO_ERR_UNSUPPORTED, "tile has too many scattered bits");
         maxpasses = std::max(maxpasses, plans[c].size());
     }
-    // entries level-major, ops / segments / coefficients concatenated
-    std::vector<BatchEntry> entries;
-    std::vector<BatchChunk> chunks;
-    std::vector<TOp> ops;
-    std::vector<TSeg> segs;
-    std::vector<C> coef;
-    size_t max_stg = 0;
-    bool all_staged = true, any_dm = false;
-    std::vector<Cx> padded;
+    ptimer.mark("plan");
+    // entries level-major, ops / segments / coefficients concatenated, in
+    // one table laid out as on the device: sizes and offsets first, then
+    // every entry filled in parallel into pinned memory, one copy up
     const bool use_dm = sizeof(V) == 16 && mode == YAO_MODE_FUSED && dmma_enabled();
+    struct Slot {
+        uint32_t c, level;
+        size_t ops, segs, coef, chunk;  // offsets
+        uint32_t nchunk, per;
+    };
+    std::vector<Slot> slots;
+    size_t nops = 0, nsegs = 0, ncoef = 0, nchunks = 0;
     for (size_t level = 0; level < maxpasses; level++)
         for (size_t c = 0; c < progs.size(); c++) {
             if (level >= plans[c].size()) continue;
             const PassPlan& pp = plans[c][level];
-            BatchEntry e;
-            memset(&e, 0, sizeof(e));
-            e.hdr = pp.hdr;
-            e.state = (uint64_t)(uintptr_t)regs[c]->d;
-            e.circuit = (uint32_t)c;
-            e.pass = (uint32_t)level;
-            e.ops_off = (int32_t)ops.size();
-            e.segs_off = (int32_t)segs.size();
-            e.coef_off = (int32_t)coef.size();
-            const size_t op0 = ops.size();
-            ops.insert(ops.end(), pp.ops.begin(), pp.ops.end());
-            segs.insert(segs.end(), pp.segs.begin(), pp.segs.end());
+            Slot sl;
+            sl.c = (uint32_t)c;
+            sl.level = (uint32_t)level;
+            sl.ops = nops;
+            sl.segs = nsegs;
+            sl.coef = ncoef;
+            sl.chunk = nchunks;
+            // chunks of consecutive tiles: about 32 per pass of a large
+            // circuit, at most 16 tiles each
+            const uint32_t nt = (uint32_t)pp.hdr.ntiles;
+            sl.per = std::max<uint32_t>(1, std::min<uint32_t>(16, nt / 32));
+            sl.nchunk = (nt + sl.per - 1) / sl.per;
+            nops += pp.ops.size();
+            nsegs += pp.segs.size();
+            ncoef += use_dm ? padded_count(pp.ops, pp.coef.size(), rb, (uint32_t)pp.hdr.tbits, kTileThreads)
+                            : pp.coef.size();
+            nchunks += sl.nchunk;
+            slots.push_back(sl);
+        }
+    if (nchunks == 0) return YAO_OK;
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t b_ent = al(slots.size() * sizeof(BatchEntry)), b_chk = al(nchunks * sizeof(BatchChunk)),
+                 b_ops = al(std::max<size_t>(1, nops) * sizeof(TOp)), b_seg = al(std::max<size_t>(1, nsegs) * sizeof(TSeg)),
+                 b_coef = al(std::max<size_t>(1, ncoef) * sizeof(C)),
+                 b_ctr = al(sizeof(unsigned long long) + sizeof(int) + progs.size() * sizeof(unsigned int));
+    const size_t b_tab = b_ent + b_chk + b_ops + b_seg + b_coef;
+    int st;
+    if ((st = grow_host(&ctx->batch_host, &ctx->batch_host_bytes, b_tab))) return st;
+    if ((st = grow_dev(&ctx->batch_dev, &ctx->batch_dev_bytes, b_tab + b_ctr, ctx->stream))) return st;
+    char* hp = (char*)ctx->batch_host;
+    BatchEntry* h_ent = (BatchEntry*)hp;
+    BatchChunk* h_chk = (BatchChunk*)(hp + b_ent);
+    TOp* h_ops = (TOp*)(hp + b_ent + b_chk);
+    TSeg* h_seg = (TSeg*)(hp + b_ent + b_chk + b_ops);
+    C* h_coef = (C*)(hp + b_ent + b_chk + b_ops + b_seg);
+    std::atomic<size_t> next_slot(0);
+    std::atomic<int> any_dm_a(0), unstaged_a(0);
+    std::atomic<size_t> max_stg_a(0);
+    auto fill = [&]() {
+        std::vector<TOp> eops;
+        std::vector<Cx> padded;
+        size_t my_max = 0;
+        for (size_t e; (e = next_slot.fetch_add(1)) < slots.size();) {
+            const Slot& sl = slots[e];
+            const PassPlan& pp = plans[sl.c][sl.level];
+            BatchEntry be;
+            memset(&be, 0, sizeof(be));
+            be.hdr = pp.hdr;
+            be.state = (uint64_t)(uintptr_t)regs[sl.c]->d;
+            be.circuit = sl.c;
+            be.pass = sl.level;
+            be.ops_off = (int32_t)sl.ops;
+            be.segs_off = (int32_t)sl.segs;
+            be.coef_off = (int32_t)sl.coef;
             // blocks for the FP64 tensor cores: padded rows (see pad_dmma)
             const std::vector<Cx>* cx = &pp.coef;
+            const std::vector<TOp>* po = &pp.ops;
             if (use_dm) {
-                std::vector<TOp> eops(pp.ops);
+                eops = pp.ops;
                 if (pad_dmma(eops, pp.coef, padded, rb, (uint32_t)pp.hdr.tbits, kTileThreads)) {
-                    std::copy(eops.begin(), eops.end(), ops.begin() + op0);
                     cx = &padded;
-                    any_dm = true;
+                    po = &eops;
+                    any_dm_a.store(1);
                 }
             }
+            std::copy(po->begin(), po->end(), h_ops + sl.ops);
+            std::copy(pp.segs.begin(), pp.segs.end(), h_seg + sl.segs);
+            C* dst = h_coef + sl.coef;
             for (const Cx& x : *cx) {
                 C cc;
                 if (sizeof(V) == 16) {
@@ -1956,70 +2066,63 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
                     float hr = (float)x.re, hi = (float)x.im;
                     *(float4*)&cc = make_float4(hr, hi, (float)(x.re - (double)hr), (float)(x.im - (double)hi));
                 }
-                coef.push_back(cc);
+                *dst++ = cc;
             }
-            e.hdr.ncoef = (int32_t)(coef.size() - (size_t)e.coef_off);
-            const size_t stg = staged_bytes(e.hdr.nops, e.hdr.nsegs, e.hdr.ncoef, sizeof(C));
-            e.hdr.staged = stg <= kMaxStagedBytes ? 1 : 0;
-            if (e.hdr.staged)
-                max_stg = std::max(max_stg, stg);
+            be.hdr.ncoef = (int32_t)cx->size();
+            const size_t stg = staged_bytes(be.hdr.nops, be.hdr.nsegs, be.hdr.ncoef, sizeof(C));
+            be.hdr.staged = stg <= kMaxStagedBytes ? 1 : 0;
+            if (be.hdr.staged)
+                my_max = std::max(my_max, stg);
             else
-                all_staged = false;
-            // chunks of consecutive tiles: about 32 per pass of a large
-            // circuit, at most 16 tiles each
+                unstaged_a.store(1);
+            h_ent[e] = be;
             const uint32_t nt = (uint32_t)pp.hdr.ntiles;
-            const uint32_t per = std::max<uint32_t>(1, std::min<uint32_t>(16, nt / 32));
-            for (uint32_t t0 = 0; t0 < nt; t0 += per) {
+            for (uint32_t q = 0; q < sl.nchunk; q++) {
                 BatchChunk ch;
-                ch.entry = (uint32_t)entries.size();
-                ch.tile0 = t0;
-                ch.ntile = std::min(per, nt - t0);
+                ch.entry = (uint32_t)e;
+                ch.tile0 = q * sl.per;
+                ch.ntile = std::min(sl.per, nt - ch.tile0);
                 ch.pad = 0;
-                chunks.push_back(ch);
+                h_chk[sl.chunk + q] = ch;
             }
-            entries.push_back(e);
         }
-    if (chunks.empty()) return YAO_OK;
+        size_t cur = max_stg_a.load();
+        while (my_max > cur && !max_stg_a.compare_exchange_weak(cur, my_max)) {
+        }
+    };
+    {
+        const size_t nth = std::max<size_t>(1, std::min<size_t>({(size_t)std::thread::hardware_concurrency(),
+                                                                  (size_t)32, slots.size() / 64 + 1}));
+        std::vector<std::thread> pool;
+        for (size_t t = 1; t < nth; t++) pool.emplace_back(fill);
+        fill();
+        for (std::thread& th : pool) th.join();
+    }
+    const size_t max_stg = max_stg_a.load();
+    const bool all_staged = unstaged_a.load() == 0, any_dm = any_dm_a.load() != 0;
     // YAO_TEST_BATCH_STALL=1 (failure-path test): circuit 0's second pass
     // waits for a tile count that is never reached, with a 0.2 s limit, so
     // the bounded wait runs out and the call reports YAO_ERR_TIMEOUT
     uint64_t wait_ns = kBatchWaitNs;
     if (const char* e = getenv("YAO_TEST_BATCH_STALL"))
         if (e[0] == '1')
-            for (BatchEntry& be : entries)
-                if (be.circuit == 0 && be.pass == 1) {
-                    be.pass = 1u << 20;
+            for (size_t q = 0; q < slots.size(); q++)
+                if (h_ent[q].circuit == 0 && h_ent[q].pass == 1) {
+                    h_ent[q].pass = 1u << 20;
                     wait_ns = 200000000ull;
                 }
-    if (coef.empty()) coef.resize(1);
-    if (ops.empty()) ops.resize(1);
-    if (segs.empty()) segs.resize(1);
-    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-    const size_t b_ent = al(entries.size() * sizeof(BatchEntry)), b_chk = al(chunks.size() * sizeof(BatchChunk)),
-                 b_ops = al(ops.size() * sizeof(TOp)), b_seg = al(segs.size() * sizeof(TSeg)),
-                 b_coef = al(coef.size() * sizeof(C)),
-                 b_ctr = al(sizeof(unsigned long long) + sizeof(int) + progs.size() * sizeof(unsigned int));
-    char* buf = nullptr;
-    YAO_CUDA(cudaMallocAsync((void**)&buf, b_ent + b_chk + b_ops + b_seg + b_coef + b_ctr, ctx->stream));
-    char* p = buf;
-    BatchEntry* d_ent = (BatchEntry*)p;
-    p += b_ent;
-    BatchChunk* d_chk = (BatchChunk*)p;
-    p += b_chk;
-    TOp* d_ops = (TOp*)p;
-    p += b_ops;
-    TSeg* d_seg = (TSeg*)p;
-    p += b_seg;
-    C* d_coef = (C*)p;
-    p += b_coef;
+    ptimer.mark("entries");
+    char* buf = (char*)ctx->batch_dev;
+    BatchEntry* d_ent = (BatchEntry*)buf;
+    BatchChunk* d_chk = (BatchChunk*)(buf + b_ent);
+    TOp* d_ops = (TOp*)(buf + b_ent + b_chk);
+    TSeg* d_seg = (TSeg*)(buf + b_ent + b_chk + b_ops);
+    C* d_coef = (C*)(buf + b_ent + b_chk + b_ops + b_seg);
+    char* p = buf + b_tab;
     unsigned long long* d_next = (unsigned long long*)p;
     int* d_err = (int*)(p + sizeof(unsigned long long));
     unsigned int* d_done = (unsigned int*)(p + sizeof(unsigned long long) + sizeof(int));
-    YAO_CUDA(cudaMemcpyAsync(d_ent, entries.data(), entries.size() * sizeof(BatchEntry), cudaMemcpyHostToDevice, ctx->stream));
-    YAO_CUDA(cudaMemcpyAsync(d_chk, chunks.data(), chunks.size() * sizeof(BatchChunk), cudaMemcpyHostToDevice, ctx->stream));
-    YAO_CUDA(cudaMemcpyAsync(d_ops, ops.data(), ops.size() * sizeof(TOp), cudaMemcpyHostToDevice, ctx->stream));
-    YAO_CUDA(cudaMemcpyAsync(d_seg, segs.data(), segs.size() * sizeof(TSeg), cudaMemcpyHostToDevice, ctx->stream));
-    YAO_CUDA(cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(C), cudaMemcpyHostToDevice, ctx->stream));
+    YAO_CUDA(cudaMemcpyAsync(buf, hp, b_tab, cudaMemcpyHostToDevice, ctx->stream));
     YAO_CUDA(cudaStreamSynchronize(ctx->stream));
     const size_t smem = ((size_t)1 << tbits_cap) * sizeof(V) + max_stg;
     // complex128 FUSED batches with blocks for the FP64 tensor cores: the
@@ -2032,19 +2135,21 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
     int per_sm = 0;
     YAO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileThreads, smem));
     const unsigned grid = (unsigned)std::max(1, per_sm) * (unsigned)ctx->num_sms;
+    ptimer.mark("upload");
     // capture: reset the queue and counters, run the persistent kernel
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     YAO_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     cudaMemsetAsync(d_next, 0, b_ctr, ctx->stream);
-    kern<<<grid, kTileThreads, smem, ctx->stream>>>(d_ent, d_chk, (uint64_t)chunks.size(), d_next, d_done, d_err,
+    kern<<<grid, kTileThreads, smem, ctx->stream>>>(d_ent, d_chk, (uint64_t)nchunks, d_next, d_done, d_err,
                                                     d_ops, d_seg, d_coef, wait_ns);
     cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
     if (ce != cudaSuccess) return cuda_fail(ce, "capture of the batch launch");
     YAO_CUDA(cudaGraphInstantiate(&exec, graph, 0));
     {
         double bytes = 0;
-        for (const BatchEntry& e : entries) bytes += (double)e.hdr.ntiles * (double)(1u << e.hdr.tbits) * 2.0 * sizeof(V);
+        for (size_t q = 0; q < slots.size(); q++)
+            bytes += (double)h_ent[q].hdr.ntiles * (double)(1u << h_ent[q].hdr.tbits) * 2.0 * sizeof(V);
         ProfScope prof(ctx, exact ? "batch_tiles_exact" : "batch_tiles_fused", bytes);
         YAO_CUDA(cudaGraphLaunch(exec, ctx->stream));
     }
@@ -2054,7 +2159,7 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
     YAO_CUDA(cudaStreamSynchronize(ctx->stream));
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
-    YAO_CUDA(cudaFreeAsync(buf, ctx->stream));
+    ptimer.mark("launch");
     if (herr) return fail(YAO_ERR_TIMEOUT, "batched launch: a chunk waited too long for its circuit's previous pass");
     return YAO_OK;
 }

@@ -135,6 +135,12 @@ struct Ctx {
     int* d_err = nullptr;
     // the last TILED / FUSED run put some blocks on the tensor cores
     bool tc_used = false;
+    // tables of the batched launch (device and pinned host copies), kept and
+    // grown across calls; freed with the context
+    void* batch_dev = nullptr;
+    size_t batch_dev_bytes = 0;
+    void* batch_host = nullptr;
+    size_t batch_host_bytes = 0;
     int ensure_scratch(size_t bytes);
     int ensure_host_pinned(size_t bytes);
     // optional per-launch timing (CUDA events on `stream` around each launch)
