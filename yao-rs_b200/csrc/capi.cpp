@@ -487,6 +487,7 @@ int yao_circuit_dispatch(yao_circuit* c, const double* params, size_t n) {
             for (int i = 0; i < gate_num_params(el.g.type); i++) el.g.params[i] = params[k++];
     std::lock_guard<std::mutex> lk(c->mu);
     c->lowered.clear();
+    c->unitary.clear();
     c->version++;
     return YAO_OK;
 }
@@ -793,6 +794,17 @@ static bool program_is_unitary(const std::vector<LGate>& prog) {
     return true;
 }
 
+// program_is_unitary of the circuit's lowered program, cached per width.
+static bool circuit_is_unitary(Circuit* c) {
+    const std::vector<LGate>& prog = lowered(c);
+    std::lock_guard<std::mutex> lk(c->mu);
+    auto it = c->unitary.find(c->nbits);
+    if (it != c->unitary.end()) return it->second;
+    const bool u = program_is_unitary(prog);
+    c->unitary[c->nbits] = u;
+    return u;
+}
+
 int yao_apply_inplace_mode(const yao_circuit* cc, yao_reg* r, int32_t mode, int32_t k) {
     CHECK_NULL(cc);
     CHECK_NULL(r);
@@ -809,7 +821,7 @@ int yao_apply_inplace_mode(const yao_circuit* cc, yao_reg* r, int32_t mode, int3
     // input's norm, so the FP64 norm of the input is restored afterwards
     // when blocks ran on the tensor cores or the circuit has 256 gates or
     // more (shorter CUDA-core runs drift by less than an FP32 ulp).
-    const bool renorm = mode == YAO_MODE_FUSED && r->precision == YAO_C64 && program_is_unitary(prog);
+    const bool renorm = mode == YAO_MODE_FUSED && r->precision == YAO_C64 && circuit_is_unitary(c);
     double n0 = 0.0;
     if (renorm && (s = reduce_norm_sqr(r->ctx, r, &n0))) return s;
     r->ctx->tc_used = false;
@@ -1443,7 +1455,7 @@ int yao_batch_apply(const yao_circuit* const* circuits, yao_reg* const* regs, si
     bool long_prog = false;
     if (mode == YAO_MODE_FUSED && regs[0]->precision == YAO_C64)
         for (size_t i = 0; i < n; i++)
-            if (program_is_unitary(*progs[i])) {
+            if (circuit_is_unitary(const_cast<yao_circuit*>(circuits[i]))) {
                 nr.push_back(rs[i]);
                 long_prog |= progs[i]->size() >= 256;
             }

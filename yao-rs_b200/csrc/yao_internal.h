@@ -116,6 +116,7 @@ struct Circuit {
     // lowered program cache (per register width); built lazily
     std::mutex mu;
     std::map<uint32_t, std::vector<LGate>> lowered;
+    std::map<uint32_t, bool> unitary;  // every lowered gate unitary (cached beside `lowered`)
     uint64_t version = 0;  // bumped by dispatch()
 };
 
