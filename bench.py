@@ -256,7 +256,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--profile-case", default=None,
                     choices=["plain", "tiled", "fused64", "fused32", "fused32_tc", "pass1q", "fused64_dmma",
-                             "fused64_cuda", "vqe", "dm", "batch", "vqe_batch"],
+                             "fused64_cuda", "vqe", "grad24", "dm", "batch", "vqe_batch"],
                     help="run one small case of a kernel family (for ncu captures) and exit")
     args = ap.parse_args()
     if args.profile_case:
@@ -401,6 +401,13 @@ def profile_case(args):
         rng = np.random.default_rng(1)
         c = vqe_circuit(Y, nv, 2, rng.uniform(-3, 3, size=4 * nv))
         Y.expect_grad(tfim(Y, nv), c, Y.ArrayReg.zero_state(nv))
+    elif args.profile_case == "grad24":
+        # one expect_grad of the VQE ansatz (n = 24, 8 layers, 384
+        # parameters) with the TFIM Hamiltonian: FUSED forward, tiled reverse
+        # sweep
+        rng = np.random.default_rng(2024)
+        c = vqe_circuit(Y, 24, 8, rng.uniform(-math.pi, math.pi, size=2 * 24 * 8))
+        Y.expect_grad(tfim(Y, 24), c, Y.ArrayReg.zero_state(24))
     elif args.profile_case == "batch":
         draws, cs = uneven_batch(Y, count=256)
         regs = [Y.ArrayReg.zero_state(nq, Y.C64) for nq, _ in draws]
