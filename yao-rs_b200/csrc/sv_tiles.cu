@@ -1079,14 +1079,15 @@ static void plan_passes(const std::vector<LGate>& prog, uint32_t nbits, int tbit
         PassPlan pp;
         std::vector<const LGate*> run;
         size_t j = i;
-        // The tile is the moving bits plus the lowest other bits, tbits in
-        // total.  Keeping at most tbits - 4 moving bits guarantees bits 0..3
-        // are in the tile (runs of >= 16 consecutive amplitudes per load).
-        const int limit = ((int)nbits <= tbits) ? (int)nbits : tbits - 4;
+        // The tile is bits 0..3 (runs of >= 16 consecutive amplitudes per
+        // load), the moving bits and the lowest other bits, tbits in total:
+        // at most tbits - 4 moving bits outside bits 0..3.
+        const bool whole = (int)nbits <= tbits;
         for (; j < prog.size(); j++) {
             const uint64_t mb = moving_mask(prog[j]);
             const uint64_t nh = hi | mb;
-            if (__builtin_popcountll(nh) > limit || __builtin_popcountll(mb) > kMaxTargets) break;
+            const int used = whole ? __builtin_popcountll(nh) : __builtin_popcountll(nh & ~(uint64_t)0xF);
+            if (used > (whole ? (int)nbits : tbits - 4) || __builtin_popcountll(mb) > kMaxTargets) break;
             hi = nh;
             run.push_back(&prog[j]);
         }
@@ -1098,7 +1099,7 @@ static void plan_passes(const std::vector<LGate>& prog, uint32_t nbits, int tbit
             i++;
             continue;
         }
-        uint64_t tile = hi;
+        uint64_t tile = whole ? hi : (hi | (uint64_t)0xF);
         for (int b = 0; __builtin_popcountll(tile) < tbits && b < (int)nbits; b++) tile |= (uint64_t)1 << b;
         std::vector<int> TB;
         int local_tab[64];
