@@ -282,7 +282,10 @@ int yao_expect_arrayreg(const yao_reg* r, const yao_term* terms, size_t nterms, 
 int yao_expect_arrayreg_noalloc(const yao_reg* r, const yao_term* terms, size_t nterms, double out[2]);
 int yao_expect_dm(const yao_dm* d, const yao_term* terms, size_t nterms, double out[2]);
 /* expect_grad (src/ad.rs:75-156): value = Re <psi|H|psi>, grad in
- * Circuit::parameters() order; ngrad must equal num_params. */
+ * Circuit::parameters() order; ngrad must equal num_params.  The forward
+ * state is computed in FUSED form (within ~1e-15 of the PLAIN state) and the
+ * reverse sweep runs over shared-memory tiles of psi and lambda (circuits
+ * with gates on more than 2 qubits, or YAO_ADJ_TILES=0: one step per gate). */
 int yao_expect_grad(const yao_term* terms, size_t nterms, const yao_circuit* c,
                     const yao_reg* psi0, double* value, double* grad, size_t ngrad);
 
@@ -303,7 +306,9 @@ int yao_measure_with_postprocess(yao_reg* r, const uint32_t* locs, uint32_t nloc
 /* ---------------------------------------------------------------- batched */
 /* Many circuits of uneven size applied in one persistent launch.  Each
  * circuit i runs on its own register regs[i] (all C128 or all C64, one
- * context).  No yao-rs counterpart: yao-rs applies circuits one at a time
+ * context).  The context keeps the launch's tables (a device buffer and a
+ * pinned host buffer, grown as batches need) until yao_ctx_destroy.  No
+ * yao-rs counterpart: yao-rs applies circuits one at a time
  * (src/apply.rs:123). */
 int yao_batch_apply(const yao_circuit* const* circuits, yao_reg* const* regs, size_t n,
                     int32_t mode, int32_t k);
