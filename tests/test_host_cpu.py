@@ -170,3 +170,27 @@ def test_plan_info_host_only():
     assert Y.plan_info(c, Y.C64, Y.MODE_FUSED, 5, 11, 3)["tensor_core_ops"] == 0
     with pytest.raises(Y.YaoError):
         Y.plan_info(c, Y.C64, Y.MODE_PLAIN, 5, 12, 3)
+
+
+def test_planner_low_bits_and_one_qubit_runs():
+    """Planner rules on the 30-qubit, 40-layer benchmark circuit: bits 0..3
+    are always tile bits and do not count against a pass's moving bits, and
+    consecutive 1-qubit gates on one qubit are multiplied together before
+    fusion.  Each layer's Rx.Ry.Rz on a qubit is one gate, so TILED keeps
+    every gate as its own op while FUSED k = 1 needs one block per qubit and
+    layer plus the CNOTs at most."""
+    import sys
+    sys.path.insert(0, str(ROOT))
+    import bench
+    n, layers = 30, 40
+    c = Y.Circuit.qubits(n, [el for l in range(layers) for el in bench.layer_elements(Y, n, l)])
+    ngates = len(c.elements)
+    assert ngates == 4180
+    tiled = Y.plan_info(c, Y.C128, Y.MODE_TILED, 0, 12, 3)
+    assert tiled["ops"] == ngates and tiled["passes"] <= 200
+    f1 = Y.plan_info(c, Y.C128, Y.MODE_FUSED, 1, 12, 3)
+    # at most one block per merged 1-qubit run or CNOT (blocks also absorb
+    # later gates on their qubits)
+    assert f1["blocks"] <= ngates - 2 * n * layers
+    f5 = Y.plan_info(c, Y.C64, Y.MODE_FUSED, 5, 12, 3)
+    assert f5["blocks"] == 130 and f5["passes"] <= 70 and f5["tensor_core_ops"] == 109
