@@ -169,7 +169,7 @@ def cpu_baseline_sample(n, budget_s, layer=0):
         gates += 1
         if t_total > budget_s:
             break
-    return b_total / t_total / 1e9, gates, t_total
+    return b_total / t_total / 1e9, gates, t_total, st, els[:gates]
 
 
 def max_over_ranks(torch, ms, world, device):
@@ -194,6 +194,42 @@ def host_ram_gb():
     except OSError:
         pass
     return 0.0
+
+
+class Background:
+    """fn(*args) in a thread.  The oracle's calls are ctypes calls into C,
+    which release the GIL, so the CPU checks of large configurations run
+    while the GPU measurements go on."""
+
+    def __init__(self, fn, *args):
+        self.out, self.err, self.s = None, None, None
+        self.t = threading.Thread(target=self._run, args=(fn, args), daemon=True)
+        self.t.start()
+
+    def _run(self, fn, args):
+        t0 = time.perf_counter()
+        try:
+            self.out = fn(*args)
+        except Exception as e:  # reported with the result
+            self.err = repr(e)
+        self.s = time.perf_counter() - t0
+
+    def result(self):
+        self.t.join()
+        if self.err:
+            raise RuntimeError(self.err)
+        return self.out
+
+
+def sig(x, d=4):
+    """Round floats to d significant digits (compact JSON)."""
+    if isinstance(x, float):
+        return float(f"{x:.{d}g}")
+    if isinstance(x, dict):
+        return {k: sig(v, d) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [sig(v, d) for v in x]
+    return x
 
 
 # -------------------------------------------------------------- reference
@@ -333,7 +369,7 @@ def main():
                 "frac": achieved / peak, "peak_source": peak_kind,
                 "bytes_per_launch": top["bytes"] / top["launches"], "launches": top["launches"],
                 "avg_launch_ms": top["ms"] / top["launches"], "traffic": traffic,
-                "traffic_source": "ncu capture at n=27 scaled by 2^(n-27)" if traffic else None,
+                "traffic_source": "ncu at n=27 x 2^(n-27)" if traffic else None,
                 "share": top["ms"] / sum(p["ms"] for p in prof)}
     kernels = [{"kernel": p["kernel"], "launches": p["launches"], "ms": round(p["ms"], 3),
                 "GBps": round(p["bytes"] / (p["ms"] / 1e3) / 1e9, 1)} for p in prof]
@@ -355,34 +391,48 @@ def main():
     state_bytes = 16 * (1 << n)
     e2e = {"value": job_gbps(nbytes, world, e2e_ms), "unit": "GB/s",
            "h2d_bytes_per_step": state_bytes / args.steps, "d2h_bytes_per_step": state_bytes / args.steps,
-           "note": "one upload of the input state and one download of the final state per K steps"}
+           "note": "one state upload + one download per K steps"}
     del host
 
     extras = {}
     cpu = None
+    first_gates = None
+    del reg
     if rank == 0 and world == 1 and not args.no_extras:
         extras = run_extras(Y, A, torch, stream, circuits, n, dev)
     if rank == 0 and world == 1:
         nb = n if host_ram_gb() > 2.5 * 16 * (1 << n) / 1e9 else min(n, 28)
-        v, g, tt = cpu_baseline_sample(nb, args.cpu_budget)
+        v, g, tt, cpu_state, gates = cpu_baseline_sample(nb, args.cpu_budget)
         cpu = {"value": v, "unit": "GB/s", "cores": 1, "kind": "port",
-               "sample": f"first {g} gates of layer 0 at n={nb} ({tt:.1f} s), oracle = C restatement of yao-rs's "
-                         "single-threaded instruct loops"}
+               "sample": f"first {g} gates of layer 0 at n={nb} ({tt:.1f} s), oracle (C restatement of yao-rs's "
+                         "loops)"}
+        # parity at the benchmark's own size: the same gates from |0...0> on
+        # the GPU (PLAIN), compared on the device with the oracle's state
+        gr = Y.ArrayReg.zero_state(nb, device=dev)
+        Y.apply_inplace(Y.Circuit.qubits(nb, gates), gr)
+        cr = Y.ArrayReg.from_vec(nb, cpu_state, device=dev)
+        first_gates = {"qubits": nb, "gates": g, "max_abs_diff_vs_oracle": gr.max_abs_diff(cr)}
+        del gr, cr, cpu_state
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "metric": METRIC, "value": sig(value, 6), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sig(ms / args.steps, 6), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": f"layered random circuit n={n}, 40 layers (Rx,Ry,Rz per qubit + CNOT brickwork), "
-                                   "one layer per step, PLAIN gate-by-gate FP64",
+            "config": {"workload": f"layered random circuit n={n}, 40 layers (Rx,Ry,Rz + CNOT brickwork), "
+                                   "one layer per step, PLAIN FP64",
                        "qubits": n, "state_bytes": state_bytes, "l2": "state (16 GiB) larger than L2, no flush",
                        "parallelism": f"replicas x{world}"},
-            "s_per_circuit_plain": ms / args.steps * LAYERS / 1e3,
-            "roofline": roofline, "kernels": kernels, "profiled_bytes": prof_bytes, "e2e": e2e,
-            "gpu_launches": int(launches), "clocks": clk, "cpu_baseline": cpu,
+            "roofline": sig(roofline), "e2e": sig(e2e), "gpu_launches": int(launches), "clocks": clk,
+            "cpu_baseline": sig(cpu),
         }
-        line.update(extras)
-        print(json.dumps(line), flush=True)
+        plain_s = ms / args.steps * LAYERS / 1e3
+        # the full record (kernel tables, per-run lists, the DM <Z_i>) on a
+        # line of its own; the last line stays short
+        detail = {"detail": {"kernels": kernels, "profiled_bytes": prof_bytes, "first_gates_n30": first_gates,
+                             **extras}}
+        print(json.dumps(detail), flush=True)
+        line["summary"] = summary(extras, plain_s, first_gates)
+        print(json.dumps(line, separators=(",", ":")), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -468,6 +518,24 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
     """Full 40-layer circuit through the TILED and FUSED forms, 1 - F against
     the FP64 result, and the VQE gradient rate."""
     out = {}
+    # the oracle at the configurations' own sizes, in threads while the GPU
+    # works: the VQE energy and all 384 gradient entries at n = 24, and one
+    # full noisy layer of the density-matrix workload at n = 12
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    O.lib()
+    nv, lv = 24, 8
+    rng = np.random.default_rng(2024)
+    params = rng.uniform(-math.pi, math.pi, size=2 * nv * lv)
+    vc = vqe_circuit(Y, nv, lv, params)
+    op = tfim(Y, nv)
+    z24 = np.zeros(1 << nv, complex)
+    z24[0] = 1
+    bg_vqe = Background(O.expect_grad, op, vc, z24)
+    dm12 = noisy_dm_circuit(Y, 12, 1)
+    rho12 = np.zeros(1 << 24, complex)
+    rho12[0] = 1
+    bg_dm = Background(O.dm_apply_circuit, dm12, rho12)
 
     def timed(fn):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -510,11 +578,6 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
     out["autotuned"] = chosen
     del ref
     # VQE: n=24, 8 layers of Ry.Rz on every qubit + CNOT ring, TFIM
-    nv, lv = 24, 8
-    rng = np.random.default_rng(2024)
-    params = rng.uniform(-math.pi, math.pi, size=2 * nv * lv)
-    vc = vqe_circuit(Y, nv, lv, params)
-    op = tfim(Y, nv)
     z = Y.ArrayReg.zero_state(nv, device=dev)
     Y.expect_grad(op, vc, z)
     reps = 3
@@ -532,27 +595,68 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
         fm = Y.expect_arrayreg(Y.apply(vqe_circuit(Y, nv, lv, pm), z), op).real
         fd = (fp - fm) / (2 * eps)
         fd_err = max(fd_err, abs(fd - g[i]) / max(1e-12, abs(g[i])))
-    # CPU: the oracle's expect_grad (one thread) on the same ansatz at n = 18,
-    # scaled by 2^(24 - 18) to n = 24 (every pass is linear in the amplitudes)
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as O
-    nc = 18
-    cc = vqe_circuit(Y, nc, lv, rng.uniform(-math.pi, math.pi, size=2 * nc * lv))
-    zc = np.zeros(1 << nc, complex)
-    zc[0] = 1
-    t0 = time.perf_counter()
-    O.expect_grad(tfim(Y, nc), cc, zc)
-    t_cpu = time.perf_counter() - t0
+    # the oracle's expect_grad at n = 24 on the same angles (one thread,
+    # run in the background since the start of the extras)
+    vo, go = bg_vqe.result()
     out["vqe"] = {"qubits": nv, "params": len(g), "gates": len(vc.elements), "grads_per_s": 1.0 / dt,
                   "s_per_grad": dt, "energy": val, "fd_max_rel_err": fd_err,
-                  "cpu_oracle_s_per_grad_n18": t_cpu,
-                  "cpu_oracle_s_per_grad_n24_extrapolated": t_cpu * (1 << (nv - nc))}
+                  "oracle_energy_diff": abs(val - vo),
+                  "oracle_max_abs_grad_diff": float(np.max(np.abs(np.asarray(go) - np.asarray(g)))),
+                  "cpu_oracle_s_per_grad": bg_vqe.s}
     del z
     out["batched_vqe"] = vqe_batch_extra(Y, A, torch, stream, dev, timed)
     out["qft20"] = qft_extra(Y, A, torch, stream, dev, timed)
     out["noisy_dm14"] = dm_extra(Y, A, torch, stream, dev, timed)
+    # one noisy layer at n = 12 against the oracle: PLAIN bit for bit, FUSED
+    # (superoperators through the tile passes) to rounding
+    ref12 = bg_dm.result()
+    d12 = {}
+    for name, mode in (("plain", Y.MODE_PLAIN), ("fused", Y.MODE_FUSED)):
+        d = Y.DensityMatrix.zero_state(12, device=dev)
+        d.apply(dm12, mode)
+        d12[name] = float(np.max(np.abs(d.state_data() - ref12)))
+        del d
+    out["noisy_dm14"]["n12_layer_vs_oracle"] = {"max_abs_diff": d12, "cpu_oracle_s": bg_dm.s}
     out["batched_circuits"] = batch_extra(Y, A, torch, stream, dev, timed)
     return out
+
+
+def summary(x, plain_s, first_gates):
+    """The figures the benchmark's claims rest on, rounded, for the last
+    line: n = 30 forms (s/circuit, 1 - F, max |err|, autotuned choice), the
+    VQE gradient with its oracle and finite-difference checks, the batches,
+    the noisy density matrix and the parity checks at the configs' sizes."""
+    s = {"layered30": {"plain_s": plain_s, "first_gates_vs_oracle": first_gates}}
+    if not x:
+        return sig(s)
+    L = s["layered30"]
+    L["tiled_s"] = x["s_per_circuit_tiled"]
+    L["fused"] = {k: [v["s_per_circuit"], v["one_minus_fidelity"], v["max_abs_err"]] for k, v in x["fused"].items()}
+    L["autotuned"] = {k: [c["k"], c["tile_bits"], c["reg_bits"]] for k, c in x["autotuned"].items()
+                      if k in ("tiled", "fused_c64_auto", "fused_f64_auto")}
+    L["c64_auto_speedup_vs_plain"] = plain_s / x["fused"]["fused_c64_auto"]["s_per_circuit"]
+    L["c128_auto_speedup_vs_plain"] = plain_s / x["fused"]["fused_f64_auto"]["s_per_circuit"]
+    v = x["vqe"]
+    s["vqe24"] = {k: v[k] for k in ("grads_per_s", "fd_max_rel_err", "oracle_energy_diff", "oracle_max_abs_grad_diff",
+                                    "cpu_oracle_s_per_grad")}
+    b = x["batched_vqe"]
+    s["vqe16_batch"] = {k: b[k] for k in ("sets", "batched_grads_per_s", "single_grads_per_s",
+                                          "max_grad_diff_vs_oracle")}
+    c = x["batched_circuits"]
+    s["batch2048"] = {"plain_s": c["s_plain"],
+                      "forms": {k: [f["s"], f["speedup_vs_plain"], f["max_one_minus_fidelity"]]
+                                for k, f in c["forms"].items()}}
+    d = x["noisy_dm14"]
+    kern = {k["kernel"]: k["GBps"] for k in d["kernels"]}
+    s["dm14"] = {"plain_s": d["s_per_circuit"], "fused_s": d["fused_superop"]["s_per_circuit"],
+                 "purity": d["purity"], "fused_max_z_diff": d["fused_superop"]["max_z_diff"],
+                 "kernel_GBps": kern,
+                 "fused_kernel_GBps": {k["kernel"]: k["GBps"] for k in d["fused_superop"]["kernels"]},
+                 "n12_layer_vs_oracle": d["n12_layer_vs_oracle"]["max_abs_diff"]}
+    q = x["qft20"]
+    s["qft20"] = {k: q[k] for k in ("s_per_circuit_plain", "s_per_circuit_tiled", "cpu_s_per_circuit",
+                                    "max_abs_diff_vs_oracle")}
+    return sig(s, 4)
 
 
 def uneven_batch(Y, count=2048, seed=4096):

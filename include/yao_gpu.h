@@ -276,7 +276,8 @@ int yao_expect_arrayreg(const yao_reg* r, const yao_term* terms, size_t nterms, 
  * synchronises the device).  The reduction scratch is a 131,200-byte
  * file-scope device array that every GPU loading the library keeps until
  * exit; its address is looked up on the first call on each device (make
- * that first call before any stream capture).  Limits: at most 64 terms of
+ * that first call before any stream capture; a lookup that fails is tried
+ * again on the next call).  Limits: at most 64 terms of
  * at most 64 ops each, else YAO_ERR_INVALID_ARGUMENT.  All calls share the
  * array: calls that overlap on the GPU race and must be serialised. */
 int yao_expect_arrayreg_noalloc(const yao_reg* r, const yao_term* terms, size_t nterms, double out[2]);

@@ -8,6 +8,7 @@ include/yao_gpu.h, marshalled by the yao_rs binding.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import subprocess
 from pathlib import Path
 
@@ -212,6 +213,29 @@ def dm_partial_tr(rho, nbits, traced):
     lib().orc_dm_partial_tr(C.c_uint32(nbits), _p(np.ascontiguousarray(rho, np.complex128)), _p(tr),
                             C.c_uint32(len(traced)), _p(out))
     return out
+
+
+def dm_von_neumann_entropy(rho, nbits):
+    """DensityMatrix::von_neumann_entropy (src/density_matrix.rs:114-123) with
+    hermitian_eigenvalues (:227-242): eigenvalues of the self-adjoint matrix
+    read from its lower triangle, clamped at 0, those above 1e-15 summed as
+    -sum lambda ln lambda in ascending order.  yao-rs solves the eigenproblem
+    with faer (self_adjoint_eigenvalues, Side::Lower); numpy's eigvalsh with
+    UPLO='L' reads the same triangle."""
+    d = 1 << nbits
+    ev = np.linalg.eigvalsh(np.asarray(rho, np.complex128).reshape(d, d), UPLO="L")
+    acc = 0.0
+    for v in np.maximum(ev, 0.0):
+        if v > 1e-15:
+            acc += float(v) * math.log(float(v))
+    return -acc
+
+
+def density_matrix_from_reg(psi, nbits, locs):
+    """density_matrix_from_reg (src/density_matrix.rs:265-271): from_reg,
+    then partial_tr over every loc not in `locs` (ascending)."""
+    traced = [l for l in range(nbits) if l not in locs]
+    return dm_partial_tr(dm_from_reg(psi, nbits), nbits, traced)
 
 
 # ---------------------------------------------------------------- observables

@@ -1,6 +1,6 @@
 """Regenerates the golden fixtures in tests/golden/.
 
-    python tests/golden/make_golden.py [--ref PATH_TO_YAO_RS]
+    python tests/golden/make_golden.py --ref PATH_TO_YAO_RS
 
 1. Copies yao-rs's committed golden vectors (tests/data/{instruct,apply,
    measure,gates,noise}.json, generated by yao-rs from Yao.jl) as compact
@@ -83,7 +83,7 @@ def copy_cli_examples(ref: Path):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of the yao-rs checkout to read the fixtures from")
     a = ap.parse_args()
     ref = Path(a.ref)
     copy_reference_data(ref)

@@ -559,6 +559,50 @@ def test_density_matrix_purity_large():
     assert abs(mixed.purity() - 0.5) < 1e-12
 
 
+@pytest.mark.parametrize("n", [4, 6, 8])
+def test_von_neumann_entropy_of_reduced_noisy_state(n):
+    """The reduced state of a noisy circuit (partial trace of the last qubit,
+    as tests/suites/benchmark_validation.rs:256-276 of yao-rs does) and its
+    entropy, against the oracle's restatement of von_neumann_entropy (the
+    1e-15 eigenvalue filter included), to 1e-12."""
+    rng = np.random.default_rng(900 + n)
+    c = random_noisy_circuit(rng, n, 30)
+    d = Y.DensityMatrix.from_reg(Y.ArrayReg.zero_state(n))
+    d.apply(c)
+    z = np.zeros(1 << n, complex)
+    z[0] = 1
+    ref = O.dm_apply_circuit(c, O.dm_from_reg(z, n))
+    red = d.partial_tr([n - 1])
+    red_ref = O.dm_partial_tr(ref, n, [n - 1])
+    assert maxdiff(red.state_data(), red_ref) == 0.0
+    s, s_ref = red.von_neumann_entropy(), O.dm_von_neumann_entropy(red_ref, n - 1)
+    assert s > 0.0
+    assert abs(s - s_ref) < 1e-12, (s, s_ref)
+    # the full noisy state has entropy too; a pure state has none
+    assert abs(d.von_neumann_entropy() - O.dm_von_neumann_entropy(ref, n)) < 1e-12
+    assert abs(Y.DensityMatrix.zero_state(n).von_neumann_entropy()) < 1e-12
+
+
+def test_density_matrix_from_reg_and_bell_entropy():
+    """density_matrix_from_reg (src/density_matrix.rs:265-271) against the
+    oracle (bit-exact), and the entanglement entropy of a Bell pair (ln 2)
+    and of random states against the oracle."""
+    bell = Y.ArrayReg.zero_state(2)
+    Y.apply_inplace(Y.Circuit.qubits(2, [Y.put([0], Gate.H), Y.control([0], [1], Gate.X)]), bell)
+    for keep in ([0], [1]):
+        r = Y.density_matrix_from_reg(bell, keep)
+        assert r.nbits() == 1
+        assert abs(r.von_neumann_entropy() - math.log(2.0)) < 1e-12
+    rng = np.random.default_rng(77)
+    for n, keep in ((3, [1]), (5, [0, 3]), (7, [6, 2, 4]), (9, [0, 1, 2, 3])):
+        psi = random_state(rng, n)
+        r = Y.density_matrix_from_reg(Y.ArrayReg.from_vec(n, psi), keep)
+        ref = O.density_matrix_from_reg(psi, n, keep)
+        assert maxdiff(r.state_data(), ref) == 0.0, (n, keep)
+        s, s_ref = r.von_neumann_entropy(), O.dm_von_neumann_entropy(ref, len(keep))
+        assert abs(s - s_ref) < 1e-12, (n, keep, s, s_ref)
+
+
 def test_batch_bounded_wait_reports_timeout(monkeypatch):
     """The batched launch's dependency wait is bounded: with circuit 0's
     second pass made to wait for a count that never comes (test hook), the
@@ -580,6 +624,41 @@ def test_batch_bounded_wait_reports_timeout(monkeypatch):
     Y.batch_apply(circuits, regs, Y.MODE_TILED)
     for c, s, r in zip(circuits, states, regs):
         assert maxdiff(r.state_vec(), O.apply_circuit(c, s)) == 0.0
+
+
+def test_tensor_core_bounded_waits_report_timeout(monkeypatch):
+    """The tensor-core block's two mbarrier waits (operand copy, MMA
+    completion) are bounded: with the test hook set, the block issues
+    neither the copy nor the MMAs, so nothing is in flight and both waits
+    give up after 0.1 s; the call fails with YAO_ERR_TIMEOUT, the tensor
+    memory is freed, and the context keeps working."""
+    from yao_rs import _abi as A
+    n = 12
+    rng = np.random.default_rng(31)
+    # one dense 5-qubit block (no controls) in one 2^12 tile
+    els = []
+    for _ in range(12):
+        a, b = (int(x) for x in rng.choice(5, size=2, replace=False))
+        els.append(Y.put([a, b], Gate.FSim(float(rng.uniform(0, 3)), float(rng.uniform(0, 3)))))
+        els.append(Y.put([a], Gate.Rx(float(rng.uniform(0, 3)))))
+    c = Y.Circuit.qubits(n, els)
+    psi = random_state(rng, n)
+    ref = O.apply_circuit(c, psi)
+    monkeypatch.setenv("YAO_TILE_BITS", "12")
+    monkeypatch.setenv("YAO_REG_BITS", "3")
+    monkeypatch.setenv("YAO_AUTOTUNE", "0")
+    plan = Y.plan_info(c, Y.C64, Y.MODE_FUSED, 5, 12, 3)
+    assert plan["tensor_core_ops"] >= 1
+    monkeypatch.setenv("YAO_TEST_TC_STALL", "1")
+    r = Y.ArrayReg.from_vec(n, psi).to_precision(Y.C64)
+    with pytest.raises(Y.YaoError) as ei:
+        Y.apply_inplace(c, r, Y.MODE_FUSED, 5)
+    assert ei.value.status == A.YAO_ERR_TIMEOUT
+    monkeypatch.delenv("YAO_TEST_TC_STALL")
+    r = Y.ArrayReg.from_vec(n, psi).to_precision(Y.C64)
+    Y.apply_inplace(c, r, Y.MODE_FUSED, 5)
+    out = r.state_vec().astype(np.complex128)
+    assert 1 - abs(np.vdot(ref, out)) ** 2 < 1e-6
 
 
 @pytest.mark.parametrize("n,k", [(13, 5), (16, 5), (14, 4), (15, 3)])

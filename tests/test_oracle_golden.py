@@ -283,6 +283,28 @@ def test_dm_known_answers():
     assert abs(O.dm_purity(r2, 1) - 0.5) < 1e-10
 
 
+def test_dm_entropy_known_answers():
+    """von_neumann_entropy (src/density_matrix.rs:114-123) restated in the
+    oracle: 0 for a pure state, ln 2 for half of a Bell pair, n ln 2 for the
+    maximally mixed state; density_matrix_from_reg keeps locs ascending."""
+    z = np.zeros(8, complex)
+    z[5] = 1
+    assert abs(O.dm_von_neumann_entropy(O.dm_from_reg(z, 3), 3)) < 1e-14
+    bell = np.array([1, 0, 0, 1], complex) / math.sqrt(2)
+    for keep in ([0], [1]):
+        red = O.density_matrix_from_reg(bell, 2, keep)
+        assert abs(O.dm_von_neumann_entropy(red, 1) - math.log(2.0)) < 1e-14
+    mixed = (np.eye(4) / 4).astype(complex).ravel()
+    assert abs(O.dm_von_neumann_entropy(mixed, 2) - 2 * math.log(2.0)) < 1e-14
+    # |psi> = |0>|+> (loc 0 = |0>, the most significant bit).  partial_tr
+    # reads a loc as bit `loc` of the index counted from the least
+    # significant end (src/density_matrix.rs:90-101), so keeping loc 1 keeps
+    # the most significant qubit, |0><0|, and keeping loc 0 keeps |+><+|.
+    plus0 = np.array([1, 1, 0, 0], complex) / math.sqrt(2)
+    assert np.allclose(O.density_matrix_from_reg(plus0, 2, [1]), [1, 0, 0, 0])
+    assert np.allclose(O.density_matrix_from_reg(plus0, 2, [0]), np.full(4, 0.5))
+
+
 # ---------------------------------------------------------------------- AD
 def h_z(site):
     return Y.OperatorPolynomial.single(site, Y.Op.Z, 1.0)

@@ -1150,6 +1150,7 @@ int yao_expect_arrayreg(const yao_reg* r, const yao_term* terms, size_t nterms, 
 int yao_expect_arrayreg_noalloc(const yao_reg* r, const yao_term* terms, size_t nterms, double out[2]) {
     CHECK_NULL(r);
     CHECK_NULL(out);
+    clear_error();
     YAO_CUDA(cudaSetDevice(r->ctx->device));
     return expect_noalloc(r->ctx, r, terms, nterms, out);
 }

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "device_common.cuh"
@@ -922,20 +923,23 @@ constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
-// Device address of g_noalloc_scratch, looked up once per device with that
-// device current (host code cannot use the symbol itself as a pointer).
+// Device address of g_noalloc_scratch on each device (host code cannot use
+// the symbol itself as a pointer).  The caller makes `device` current before
+// the lookup.  Only a successful lookup is kept: a lookup that failed (for
+// instance because it was made inside a stream capture) is tried again on
+// the next call.
 static double* g_noalloc_ptr[kNoAllocMaxDevices];
-static cudaError_t g_noalloc_err[kNoAllocMaxDevices];
-static std::once_flag g_noalloc_once[kNoAllocMaxDevices];
+static std::mutex g_noalloc_mu;
 
 static int noalloc_scratch(int device, double** out) {
     if (device < 0 || device >= kNoAllocMaxDevices) return fail(YAO_ERR_INVALID_ARGUMENT, "device index too large");
-    std::call_once(g_noalloc_once[device], [device]() {
-        cudaError_t e = cudaSetDevice(device);
-        if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&g_noalloc_ptr[device], g_noalloc_scratch);
-        g_noalloc_err[device] = e;
-    });
-    if (g_noalloc_err[device] != cudaSuccess) return cuda_fail(g_noalloc_err[device], "cudaGetSymbolAddress");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        double* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress");
+        g_noalloc_ptr[device] = p;
+    }
     *out = g_noalloc_ptr[device];
     return YAO_OK;
 }

@@ -47,6 +47,8 @@ struct TileHdr {
     int32_t staged;  // op table, segments and coefficients are copied to shared memory
     int32_t mma;     // some wide op of the pass runs on the tensor cores
     int32_t dmma;    // complex128 FUSED: some dense 3..5-qubit block runs on the FP64 tensor cores
+    int32_t tc_test; // failure-path test: tensor-core ops issue no copy and no MMA, waits give up after 0.1 s
+    int32_t pad_;
 };
 
 struct TOp {
@@ -316,6 +318,8 @@ struct TcCtx {
     int loaded;          // op offset whose B operands are in shared memory
     int failed;          // a completion wait ran out (results of the pass are void)
     int* err;
+    uint64_t wait_ns;    // limit of every wait
+    int stall;           // failure-path test: nothing is issued, so every wait runs out
 };
 
 __device__ __forceinline__ uint32_t tc_off(uint32_t r, uint32_t k) {
@@ -331,7 +335,7 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
         // B operands of this op (Bh, Bl: 32 KiB contiguous): one bulk copy
         // started now, waited for by the MMA-issuing thread
         const bool need_b = tc.loaded != op.mma;
-        if (need_b && tid == 0) {
+        if (need_b && tid == 0 && !tc.stall) {
             tc::mbar_arrive_expect_tx(tc.bbar, (uint32_t)kTcOpFloats * 4);
             tc::bulk_g2s(tc.bh, tc.mmat + op.mma, (uint32_t)kTcOpFloats * 4, tc.bbar);
         }
@@ -386,7 +390,7 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
             if (tid == 0) {
                 const uint64_t tb = global_ns_tc();
                 while (!(b_ok = tc::mbar_try_wait(tc.bbar, tc.bphase)))
-                    if (global_ns_tc() - tb > kTcWaitNs) break;
+                    if (global_ns_tc() - tb > tc.wait_ns) break;
             }
             tc.bphase ^= 1u;
         }
@@ -395,7 +399,7 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
         if (tid == 0 && !b_ok) {
             tc.failed = 1;
             atomicExch(tc.err, 1);
-            tc::commit(tc.bar);  // no MMA: the barrier completes right away
+            if (!tc.stall) tc::commit(tc.bar);  // no MMA: the barrier completes right away
         } else if (tid == 0) {
             issue(kTcKr / 16);
             tc::commit(tc.bar);
@@ -404,7 +408,7 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
         bool done = false;
         const uint64_t t0 = global_ns_tc();
         while (!(done = tc::mbar_try_wait(tc.bar, tc.phase))) {
-            if (global_ns_tc() - t0 > kTcWaitNs) break;
+            if (global_ns_tc() - t0 > tc.wait_ns) break;
         }
         tc.phase ^= 1u;
         if (!done) {
@@ -816,6 +820,8 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         tcx.loaded = -1;
         tcx.failed = 0;
         tcx.err = err;
+        tcx.wait_ns = hdr.tc_test ? 100000000ull : kTcWaitNs;
+        tcx.stall = hdr.tc_test;
         tcx.phase = 0;
         tcx.bar = &tc_bar;
         tcx.bphase = 0;
@@ -862,10 +868,10 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         // again (bounded) before the accumulator is freed
         if (tcx.failed) {
             const uint64_t t0 = global_ns_tc();
-            while (!tc::mbar_try_wait(tcx.bar, tcx.phase ^ 1u) && global_ns_tc() - t0 < kTcWaitNs) {
+            while (!tc::mbar_try_wait(tcx.bar, tcx.phase ^ 1u) && global_ns_tc() - t0 < tcx.wait_ns) {
             }
             while (tcx.loaded >= 0 && !tc::mbar_try_wait(tcx.bbar, tcx.bphase ^ 1u) &&
-                   global_ns_tc() - t0 < 2 * kTcWaitNs) {
+                   global_ns_tc() - t0 < 2 * tcx.wait_ns) {
             }
         }
         tc::fence_before_sync();
@@ -1563,6 +1569,11 @@ static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
     const size_t used = 2 * tile_bytes + (hdr.mma ? 1024 + kTcSmemBytes : 0) + 16 * 1024;
     hdr.staged = used + stg <= (size_t)optin ? 1 : 0;
     hdr.dmma = dm ? 1 : 0;
+    // YAO_TEST_TC_STALL=1 (failure-path test): the tensor-core ops issue
+    // neither their operand copy nor their MMAs, so both bounded waits of
+    // each op run out (0.1 s each) and the call reports YAO_ERR_TIMEOUT
+    if (hdr.mma)
+        if (const char* e = getenv("YAO_TEST_TC_STALL")) hdr.tc_test = e[0] == '1';
     size_t smem = 2 * tile_bytes + (hdr.staged ? stg : 0);
     if (hdr.mma) smem = ((smem + 1023) & ~(size_t)1023) + kTcSmemBytes;
     const TOp* dops = (const TOp*)dbuf;
