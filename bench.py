@@ -292,7 +292,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--profile-case", default=None,
                     choices=["plain", "tiled", "fused64", "fused32", "fused32_tc", "pass1q", "fused64_dmma",
-                             "fused64_cuda", "vqe", "grad24", "dm", "batch", "vqe_batch"],
+                             "fused64_cuda", "vqe", "grad24", "dm", "batch", "vqe_batch", "tc_drift"],
                     help="run one small case of a kernel family (for ncu captures) and exit")
     args = ap.parse_args()
     if args.profile_case:
@@ -446,6 +446,8 @@ def profile_case(args):
     from yao_rs import _abi as A
 
     n = args.qubits
+    if args.profile_case == "tc_drift":
+        return tc_drift(Y, A, min(n, 24))
     if args.profile_case == "vqe":
         nv = 20
         rng = np.random.default_rng(1)
@@ -512,6 +514,40 @@ def profile_case(args):
         Y.apply_inplace(c, r, mode, k)
     A.synchronize()
     print(f"profile case {args.profile_case} done: {Y.launch_count()} launches")
+
+
+def tc_drift(Y, A, n):
+    """Complex64 FUSED k = 5 on the layered circuit (40 layers) without the
+    FP64 norm restore: the norm drift per tensor-core block, 1 - F and max
+    |error| against the FP64 PLAIN result, for every tensor-core variant
+    (YAO_TC_VARIANT bits: 1 X low part rounded, 2 separate correction
+    accumulator, 4 three-part B) and for the CUDA-core split form; one JSON
+    line per form."""
+    import torch
+    os.environ.update(YAO_TILE_BITS="12", YAO_REG_BITS="3", YAO_AUTOTUNE="0", YAO_NORM_RESTORE="0")
+    c = Y.Circuit.qubits(n, [el for l in range(LAYERS) for el in layer_elements(Y, n, l)])
+    ref = Y.ArrayReg.zero_state(n)
+    Y.apply_inplace(c, ref)
+    info = Y.plan_info(c, Y.C64, Y.MODE_FUSED, 5, 12, 3)
+    stream = torch.cuda.ExternalStream(A.stream_ptr(0), device=torch.device("cuda", 0))
+    forms = [("tc_v%d" % v, "1", str(v)) for v in range(8)] + [("cuda_core", "0", "0")]
+    for name, tc, var in forms:
+        os.environ.update(YAO_TC=tc, YAO_TC_VARIANT=var)
+        r = Y.ArrayReg.zero_state(n, Y.C64)
+        Y.apply_inplace(c, r, Y.MODE_FUSED, 5)  # warm-up
+        r = Y.ArrayReg.zero_state(n, Y.C64)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        A.synchronize()
+        e0.record(stream)
+        Y.apply_inplace(c, r, Y.MODE_FUSED, 5)
+        e1.record(stream)
+        e1.synchronize()
+        nrm2 = r.norm() ** 2
+        blocks = info["tensor_core_ops"] if tc == "1" else info["blocks"]
+        print(json.dumps({"form": name, "qubits": n, "tc_blocks": info["tensor_core_ops"], "blocks": info["blocks"],
+                          "norm2_minus_1": nrm2 - 1.0, "norm2_drift_per_tc_block": (nrm2 - 1.0) / max(1, blocks),
+                          "one_minus_fidelity": 1.0 - ref.fidelity(r), "max_abs_err": ref.max_abs_diff(r),
+                          "ms": e0.elapsed_time(e1)}), flush=True)
 
 
 def run_extras(Y, A, torch, stream, circuits, n, dev):

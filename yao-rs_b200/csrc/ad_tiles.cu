@@ -25,23 +25,38 @@
 #include <vector>
 
 #include "device_common.cuh"
+#include "tc_sm100.cuh"
+#include "tma_sm100.cuh"
 
 namespace yao {
 
-constexpr int kAdjThreads = 256;
+constexpr int kAdjThreads = 512;
 constexpr int kAdjLowBits = 4;      // contiguous low bits of every tile (256-byte runs)
 constexpr int kAdjScatter = 7;      // scattered tile bits at most
 constexpr int kAdjMaxOps = 96;      // reverse-sweep ops per pass
 constexpr int kAdjMaxSlots = 64;    // generator dots per pass
 
+// A run of uncontrolled 1-qubit reverse-sweep steps on one target bit,
+// folded on the host into one op (cls kAdjFused): with A the product of the
+// run's U^dagger matrices so far, the dot of a generator G taken after them
+// is Re <A lambda | G A psi> = Re <lambda | (A^dagger G A) psi>, so every dot
+// of the run is taken against the run's input amplitudes with G' = A^dagger
+// G A, and the run's U^dagger steps are one 2 x 2 product A at the end.
+// m[0..3] = A, m[4 + 4 j ..] = G'_j, gslot[j] its dot slot (ngen <= 3).
+constexpr int32_t kAdjFused = 16;
+constexpr int kAdjFusedGens = 3;
+
 struct AdjTileOp {
     int32_t gen;     // 1: accumulate Re <lambda | G psi> into `slot`; 0: U^dagger on psi and lambda
-    int32_t cls;     // GC_X / GC_SWAP / GC_DIAG / GC_DENSE (generators: GC_DENSE)
+    int32_t cls;     // GC_X / GC_SWAP / GC_DIAG / GC_DENSE (generators: GC_DENSE), or kAdjFused
     int32_t k;       // 1 or 2 targets
     int32_t slot;
     int8_t tl[2];    // local target positions; tl[0] is bit 0 of the gate-local index
     int8_t sync;     // barrier after this op (the next op moves amplitudes along other bits)
-    int8_t pad[5];
+    int8_t ngen;     // kAdjFused: generator dots of the run
+    int8_t pad[4];
+    int32_t gslot[kAdjFusedGens];
+    int32_t a_id;    // kAdjFused: A is the identity (no U^dagger in the run)
     uint32_t lcmask, lcval;  // in-tile controls (local positions)
     uint64_t gcmask, gcval;  // out-of-tile controls (global bits)
     uint64_t active;         // DIAG: entries different from 1
@@ -55,6 +70,9 @@ struct AdjTileHdr {
     int8_t pad[1];
     int8_t outb[64];         // global bits outside the tile, ascending
     uint64_t ntiles;
+    int32_t use_tma;         // psi's and lambda's tiles move by TMA (maps of the same plan)
+    int32_t nstage;          // tile buffers (psi + lambda each) in flight
+    TmaPlan tma;
 };
 
 __device__ __forceinline__ uint32_t adj_ins0(uint32_t v, int p) {
@@ -181,19 +199,93 @@ __device__ __forceinline__ void adj_run(const AdjTileOp* rops, int nr, uint64_t 
         }
 }
 
-__global__ void __launch_bounds__(kAdjThreads, 2)
+// A fused run (kAdjFused) on the groups of the tile owned by this thread:
+// coefficients in registers, every group read once, P = conj(lambda_r) psi_c
+// formed once for all the run's dots, A applied once.
+__device__ __forceinline__ void adj_fused1(const AdjTileOp& op, double2* sp, double2* sl, uint32_t T, double* acc,
+                                           uint32_t nw) {
+    const uint32_t ngroups = T >> 1;
+    const int p = op.tl[0];
+    const int ng = op.ngen;
+    const bool apply = !op.a_id;
+    const double2 a0 = op.m[0], a1 = op.m[1], a2 = op.m[2], a3 = op.m[3];
+    double2 G[kAdjFusedGens][4];
+    double dot[kAdjFusedGens];
+#pragma unroll
+    for (int j = 0; j < kAdjFusedGens; j++) {
+        dot[j] = 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) G[j][q] = j < ng ? op.m[4 + 4 * j + q] : make_double2(0.0, 0.0);
+    }
+    for (uint32_t g = threadIdx.x; g < ngroups; g += blockDim.x) {
+        const uint32_t b = adj_ins0(g, p);
+        const uint32_t i0 = adj_swz(b), i1 = adj_swz(b | (1u << p));
+        const double2 x0 = sp[i0], x1 = sp[i1], l0 = sl[i0], l1 = sl[i1];
+        // P[r][c] = conj(l_r) * x_c
+        const double2 p00 = make_double2(fma(l0.x, x0.x, l0.y * x0.y), fma(l0.x, x0.y, -l0.y * x0.x));
+        const double2 p01 = make_double2(fma(l0.x, x1.x, l0.y * x1.y), fma(l0.x, x1.y, -l0.y * x1.x));
+        const double2 p10 = make_double2(fma(l1.x, x0.x, l1.y * x0.y), fma(l1.x, x0.y, -l1.y * x0.x));
+        const double2 p11 = make_double2(fma(l1.x, x1.x, l1.y * x1.y), fma(l1.x, x1.y, -l1.y * x1.x));
+#pragma unroll
+        for (int j = 0; j < kAdjFusedGens; j++) {
+            if (j < ng) {
+                // Re sum_rc G'[r][c] P[r][c]
+                double d = fma(G[j][0].x, p00.x, -G[j][0].y * p00.y);
+                d = fma(G[j][1].x, p01.x, fma(-G[j][1].y, p01.y, d));
+                d = fma(G[j][2].x, p10.x, fma(-G[j][2].y, p10.y, d));
+                d = fma(G[j][3].x, p11.x, fma(-G[j][3].y, p11.y, d));
+                dot[j] += d;
+            }
+        }
+        if (apply) {
+            sp[i0] = cfma2(cmul2(a0, x0), a1, x1);
+            sp[i1] = cfma2(cmul2(a2, x0), a3, x1);
+            sl[i0] = cfma2(cmul2(a0, l0), a1, l1);
+            sl[i1] = cfma2(cmul2(a2, l0), a3, l1);
+        }
+    }
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < kAdjFusedGens; j++)
+        if (j < ng) {
+            const double d = warp_sum(dot[j]);
+            if (lane == 0) acc[op.gslot[j] * nw + warp] += d;
+        }
+}
+
+constexpr uint64_t kAdjWaitNs = 1000000000ull;  // 1 s
+constexpr int kAdjMaxStages = 2;
+
+__device__ __forceinline__ uint64_t adj_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// One pass of the reverse sweep over every tile of psi and lambda.
+// TMA form (hdr.use_tma): `nstage` buffers, each psi's and lambda's tile;
+// one thread issues the next tile's box copies (tensor maps mpsi, mlam)
+// while the current tile is computed, every thread waits for its tile on
+// the buffer's mbarrier (bounded: 1 s, then `*err` is set and the pass's
+// results are void), and the same thread stores both tiles back with bulk
+// tensor stores.  Plain form (tiny states): cp.async in, plain stores out.
+__global__ void __launch_bounds__(kAdjThreads, 1)
     k_adjoint_tiles(double2* __restrict__ psi, double2* __restrict__ lam, const AdjTileHdr phdr,
-                    const AdjTileOp* __restrict__ gops, double* __restrict__ partial) {
-    extern __shared__ __align__(16) unsigned char adj_smem[];
+                    const AdjTileOp* __restrict__ gops, double* __restrict__ partial, int* __restrict__ err,
+                    const __grid_constant__ CUtensorMap mpsi, const __grid_constant__ CUtensorMap mlam) {
+    extern __shared__ __align__(1024) unsigned char adj_smem[];
     __shared__ AdjTileHdr hdr;
     __shared__ uint64_t hoff[1 << kAdjScatter];
+    __shared__ uint64_t full_bar[kAdjMaxStages];
     if (threadIdx.x == 0) hdr = phdr;
     __syncthreads();
     const uint32_t T = 1u << hdr.tbits;
     const uint32_t nw = blockDim.x >> 5;
-    double2* sp = (double2*)adj_smem;
-    double2* sl = sp + T;
-    AdjTileOp* ops = (AdjTileOp*)(sl + T);
+    const bool use_tma = hdr.use_tma != 0;
+    const int nbuf = use_tma ? hdr.nstage : 1;
+    unsigned char* smem = adj_smem + ((1024u - (tc::smem_u32(adj_smem) & 1023u)) & 1023u);
+    const uint32_t tile_bytes = T * (uint32_t)sizeof(double2);  // one array's tile
+    AdjTileOp* ops = (AdjTileOp*)(smem + (size_t)nbuf * 2 * tile_bytes);
     double* acc = (double*)(ops + hdr.nops);  // [slot][warp]
     const int nlow = min(kAdjLowBits, hdr.tbits), nh = hdr.tbits - nlow;
     {
@@ -207,43 +299,119 @@ __global__ void __launch_bounds__(kAdjThreads, 2)
             hoff[h] = o;
         }
     }
-    __syncthreads();
-    const uint32_t lmask = (1u << nlow) - 1;
-    for (uint64_t t = blockIdx.x; t < hdr.ntiles; t += gridDim.x) {
+    auto tile_base = [&](uint64_t t) {
         uint64_t base = 0;
         for (int i = 0; i < hdr.nouts; i++) base |= ((t >> i) & 1) << hdr.outb[i];
-        // the tile's copies are issued back to back (cp.async), then waited for
-        for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) {
-            const uint64_t gi = base | (l & lmask) | hoff[l >> nlow];
-            const uint32_t s = adj_swz(l);
-            const uint32_t dp = (uint32_t)__cvta_generic_to_shared(&sp[s]);
-            const uint32_t dl = (uint32_t)__cvta_generic_to_shared(&sl[s]);
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dp), "l"(&psi[gi]) : "memory");
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dl), "l"(&lam[gi]) : "memory");
+        return base;
+    };
+    const uint32_t sbase = tc::smem_u32(smem);
+    auto issue = [&](uint64_t t, int b) {  // thread 0: both tiles of tile t into buffer b
+        tc::mbar_arrive_expect_tx(&full_bar[b], 2 * tile_bytes);
+        const uint64_t base = tile_base(t);
+        const uint32_t dst = sbase + (uint32_t)b * 2 * tile_bytes;
+        tma::load_boxes(&mpsi, hdr.tma, base, dst, tc::smem_u32(&full_bar[b]));
+        tma::load_boxes(&mlam, hdr.tma, base, dst + tile_bytes, tc::smem_u32(&full_bar[b]));
+    };
+    uint32_t pending = 0;
+    if (use_tma && threadIdx.x == 0) {
+        tma::prefetch_map(&mpsi);
+        tma::prefetch_map(&mlam);
+        for (int q = 0; q < nbuf; q++) tc::mbar_init(&full_bar[q], 1);
+        if (blockIdx.x < hdr.ntiles) {
+            issue(blockIdx.x, 0);
+            pending |= 1u;
         }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        __syncthreads();
+    }
+    __syncthreads();
+    const uint32_t lmask = (1u << nlow) - 1;
+    bool dead = false;
+    uint32_t it = 0;
+    for (uint64_t t = blockIdx.x; t < hdr.ntiles; t += gridDim.x, it++) {
+        const uint64_t base = tile_base(t);
+        const int b = use_tma ? (int)(it % (uint32_t)nbuf) : 0;
+        double2* sp = (double2*)(smem + (size_t)b * 2 * tile_bytes);
+        double2* sl = sp + T;
+        if (use_tma) {
+            if (threadIdx.x == 0 && nbuf > 1 && t + gridDim.x < hdr.ntiles) {
+                const int bn = (int)((it + 1) % (uint32_t)nbuf);
+                tma::wait_group_read<0>();  // the previous tile's stores have read buffer bn
+                issue(t + gridDim.x, bn);
+                pending |= 1u << bn;
+            }
+            if (!dead) {
+                const uint32_t parity = (it / (uint32_t)nbuf) & 1u;
+                const uint64_t t0 = adj_ns();
+                while (!tc::mbar_try_wait(&full_bar[b], parity)) {
+                    if (adj_ns() - t0 > kAdjWaitNs) {
+                        dead = true;
+                        atomicExch(err, 1);
+                        break;
+                    }
+                }
+                if (!dead && threadIdx.x == 0) pending &= ~(1u << b);
+            }
+        } else {
+            // the tile's copies are issued back to back (cp.async), then waited for
+            for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) {
+                const uint64_t gi = base | (l & lmask) | hoff[l >> nlow];
+                const uint32_t s = adj_swz(l);
+                const uint32_t dp = (uint32_t)__cvta_generic_to_shared(&sp[s]);
+                const uint32_t dl = (uint32_t)__cvta_generic_to_shared(&sl[s]);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dp), "l"(&psi[gi]) : "memory");
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dl), "l"(&lam[gi]) : "memory");
+            }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+            __syncthreads();
+        }
         for (int oi = 0; oi < hdr.nops;) {
             // the run ends at the first op followed by a barrier
             int e = oi;
             while (!ops[e].sync) e++;
             e++;
-            if (ops[oi].k == 1)
+            if (ops[oi].cls == kAdjFused)
+                adj_fused1(ops[oi], sp, sl, T, acc, nw);
+            else if (ops[oi].k == 1)
                 adj_run<1>(ops + oi, e - oi, base, sp, sl, T, acc, nw);
             else
                 adj_run<2>(ops + oi, e - oi, base, sp, sl, T, acc, nw);
             __syncthreads();
             oi = e;
         }
-        for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) {
-            const uint64_t gi = base | (l & lmask) | hoff[l >> nlow];
-            const uint32_t s = adj_swz(l);
-            psi[gi] = sp[s];
-            lam[gi] = sl[s];
+        if (use_tma) {
+            tc::fence_proxy_async();  // the tiles' writes are visible to the bulk stores
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                const uint32_t src = sbase + (uint32_t)b * 2 * tile_bytes;
+                tma::store_boxes(&mpsi, hdr.tma, base, src);
+                tma::store_boxes(&mlam, hdr.tma, base, src + tile_bytes);
+                tma::commit_group();
+                if (nbuf == 1 && t + gridDim.x < hdr.ntiles) {
+                    tma::wait_group_read<0>();
+                    issue(t + gridDim.x, 0);
+                    pending |= 1u;
+                }
+            }
+        } else {
+            for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) {
+                const uint64_t gi = base | (l & lmask) | hoff[l >> nlow];
+                const uint32_t s = adj_swz(l);
+                psi[gi] = sp[s];
+                lam[gi] = sl[s];
+            }
+            __syncthreads();
         }
-        __syncthreads();
     }
+    if (use_tma && threadIdx.x == 0) {
+        tma::wait_group<0>();  // stores complete before the shared memory goes away
+        const uint64_t t0 = adj_ns();
+        for (int q = 0; q < nbuf; q++)
+            if (pending & (1u << q))
+                for (uint32_t ph = 0; ph < 2; ph++)
+                    while (!tc::mbar_try_wait(&full_bar[q], ph) && adj_ns() - t0 < kAdjWaitNs) {
+                    }
+    }
+    __syncthreads();
     // per CTA: slot sums over warps in order
     for (int sidx = threadIdx.x; sidx < hdr.nslots; sidx += blockDim.x) {
         double s = 0.0;
@@ -314,6 +482,91 @@ bool to_host_op(const LGate& g, bool gen, int grad, HostOp& h) {
     return true;
 }
 
+// 2 x 2 complex helpers (host, FP64)
+struct M2 {
+    double2 e[4];
+};
+static M2 m2_mul(const M2& a, const M2& b) {
+    M2 r;
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) {
+            double re = 0, im = 0;
+            for (int k = 0; k < 2; k++) {
+                const double2 x = a.e[i * 2 + k], y = b.e[k * 2 + j];
+                re += x.x * y.x - x.y * y.y;
+                im += x.x * y.y + x.y * y.x;
+            }
+            r.e[i * 2 + j] = make_double2(re, im);
+        }
+    return r;
+}
+static M2 m2_adj(const M2& a) {
+    M2 r;
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) r.e[i * 2 + j] = make_double2(a.e[j * 2 + i].x, -a.e[j * 2 + i].y);
+    return r;
+}
+static bool m2_of(const AdjTileOp& op, M2& m) {
+    const double2 z = make_double2(0, 0), one = make_double2(1, 0);
+    if (op.cls == GC_DENSE)
+        for (int q = 0; q < 4; q++) m.e[q] = op.m[q];
+    else if (op.cls == GC_DIAG)
+        m = M2{{op.m[0], z, z, op.m[1]}};
+    else if (op.cls == GC_X)
+        m = M2{{z, one, one, z}};
+    else
+        return false;
+    return true;
+}
+
+// Fold runs of uncontrolled 1-qubit steps on one target into kAdjFused ops
+// (at most kAdjFusedGens generator dots each).
+static void fuse_runs(std::vector<AdjTileOp>& ops) {
+    const char* env = getenv("YAO_ADJ_FUSE");
+    if (env && env[0] == '0') return;  // YAO_ADJ_FUSE=0: every step its own op
+    auto plain = [](const AdjTileOp& o) { return o.k == 1 && o.lcmask == 0 && o.gcmask == 0; };
+    std::vector<AdjTileOp> out;
+    size_t i = 0;
+    while (i < ops.size()) {
+        if (!plain(ops[i])) {
+            out.push_back(ops[i++]);
+            continue;
+        }
+        AdjTileOp f;
+        memset(&f, 0, sizeof(f));
+        f.cls = kAdjFused;
+        f.k = 1;
+        f.tl[0] = ops[i].tl[0];
+        f.slot = -1;
+        M2 A{{make_double2(1, 0), make_double2(0, 0), make_double2(0, 0), make_double2(1, 0)}};
+        bool any_u = false;
+        size_t j = i;
+        for (; j < ops.size() && plain(ops[j]) && ops[j].tl[0] == f.tl[0]; j++) {
+            const AdjTileOp& o = ops[j];
+            M2 m;
+            if (!m2_of(o, m)) break;
+            if (o.gen) {
+                if (f.ngen == kAdjFusedGens) break;
+                const M2 g = m2_mul(m2_adj(A), m2_mul(m, A));
+                for (int q = 0; q < 4; q++) f.m[4 + 4 * f.ngen + q] = g.e[q];
+                f.gslot[f.ngen++] = o.slot;
+            } else {
+                A = m2_mul(m, A);
+                any_u = true;
+            }
+        }
+        if (j == i) {  // not foldable after all
+            out.push_back(ops[i++]);
+            continue;
+        }
+        for (int q = 0; q < 4; q++) f.m[q] = A.e[q];
+        f.a_id = any_u ? 0 : 1;
+        out.push_back(f);
+        i = j;
+    }
+    ops.swap(out);
+}
+
 // Greedy passes: consecutive ops while the targets above the low bits fit
 // the scattered tile bits, and the op / slot limits hold.
 void plan_adj(const std::vector<HostOp>& hops, uint32_t nbits, std::vector<AdjPass>& out) {
@@ -372,6 +625,7 @@ void plan_adj(const std::vector<HostOp>& hops, uint32_t nbits, std::vector<AdjPa
             }
             pass.ops.push_back(op);
         }
+        fuse_runs(pass.ops);
         // a thread owns the same groups in consecutive ops on the same
         // target positions (controls only skip groups): a barrier is needed
         // only before an op that moves amplitudes along other bits
@@ -384,7 +638,8 @@ void plan_adj(const std::vector<HostOp>& hops, uint32_t nbits, std::vector<AdjPa
                 same = a.k == b.k && a.tl[0] == b.tl[0] && (a.k == 1 || a.tl[1] == b.tl[1]);
             }
             run++;
-            if (run >= kAdjRun) same = false;
+            if (run >= kAdjRun || a.cls == kAdjFused || (q + 1 < pass.ops.size() && pass.ops[q + 1].cls == kAdjFused))
+                same = false;
             a.sync = (int8_t)(same ? 0 : 1);
             if (a.sync) run = 0;
         }
@@ -442,14 +697,18 @@ int adjoint_tiles(Ctx* ctx, Reg* psi, Reg* lam, const Circuit* c, double* grad, 
         ndots += p.slot_grad.size();
     }
     const int tbits = passes[0].hdr.tbits;
-    const size_t tile_bytes = (size_t)2 * ((size_t)1 << tbits) * sizeof(double2);
-    // the attribute covers the largest pass (2^11-amplitude tiles, every op
-    // and slot in use)
-    const size_t smem_max = (size_t)2 * ((size_t)1 << (kAdjLowBits + kAdjScatter)) * sizeof(double2) +
-                            kAdjMaxOps * sizeof(AdjTileOp) + (size_t)kAdjMaxSlots * (kAdjThreads / 32) * 8;
+    const size_t tile_bytes = (size_t)2 * ((size_t)1 << tbits) * sizeof(double2);  // psi's and lambda's tile
+    // shared memory: the tile buffers (two when they fit), every op and slot
+    // of the largest pass, 1 KiB for aligning the tiles
+    static int optin = 0;
+    if (!optin) YAO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    const size_t rest = kAdjMaxOps * sizeof(AdjTileOp) + (size_t)kAdjMaxSlots * (kAdjThreads / 32) * 8 + 1024;
+    const size_t budget = (size_t)optin - 4096;  // static shared memory of the kernel
+    const int nstage = 2 * tile_bytes + rest <= budget ? 2 : 1;
+    const size_t smem_max = (size_t)nstage * tile_bytes + rest;
     static bool attr = false;
     if (!attr) {
-        YAO_CUDA(cudaFuncSetAttribute(k_adjoint_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
+        YAO_CUDA(cudaFuncSetAttribute(k_adjoint_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget));
         attr = true;
     }
     int per_sm = 0;
@@ -472,14 +731,30 @@ int adjoint_tiles(Ctx* ctx, Reg* psi, Reg* lam, const Circuit* c, double* grad, 
         YAO_CUDA(cudaMemcpyAsync(d_ops, all.data(), all.size() * sizeof(AdjTileOp), cudaMemcpyHostToDevice,
                                  ctx->stream));
     }
+    if (!ctx->d_err) {
+        YAO_CUDA(cudaMalloc((void**)&ctx->d_err, sizeof(int)));
+        YAO_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    }
     size_t ooff = 0, doff = 0;
     for (const AdjPass& p : passes) {
-        const size_t smem =
-            tile_bytes + p.ops.size() * sizeof(AdjTileOp) + (size_t)p.slot_grad.size() * (kAdjThreads / 32) * 8;
+        AdjTileHdr hdr = p.hdr;
+        CUtensorMap mpsi, mlam;
+        memset(&mpsi, 0, sizeof(mpsi));
+        memset(&mlam, 0, sizeof(mlam));
+        int8_t tb[kAdjLowBits + kAdjScatter];
+        const int nlow = std::min(kAdjLowBits, hdr.tbits);
+        for (int q = 0; q < hdr.tbits; q++) tb[q] = (int8_t)(q < nlow ? q : hdr.hb[q - nlow]);
+        hdr.use_tma = tma_enabled() && tma_make_plan(tb, hdr.tbits, n, sizeof(double2), psi->d, hdr.tma, &mpsi) &&
+                              tma_make_plan(tb, hdr.tbits, n, sizeof(double2), lam->d, hdr.tma, &mlam)
+                          ? 1
+                          : 0;
+        hdr.nstage = hdr.use_tma ? nstage : 1;
+        const size_t smem = 1024 + (size_t)(hdr.use_tma ? nstage : 1) * tile_bytes + p.ops.size() * sizeof(AdjTileOp) +
+                            (size_t)p.slot_grad.size() * (kAdjThreads / 32) * 8;
         {
             ProfScope prof(ctx, "adjoint_tiles", (double)((uint64_t)1 << n) * 4.0 * sizeof(double2));
-            k_adjoint_tiles<<<grid, kAdjThreads, smem, ctx->stream>>>((double2*)psi->d, (double2*)lam->d, p.hdr,
-                                                                       d_ops + ooff, d_part);
+            k_adjoint_tiles<<<grid, kAdjThreads, smem, ctx->stream>>>((double2*)psi->d, (double2*)lam->d, hdr,
+                                                                       d_ops + ooff, d_part, ctx->d_err, mpsi, mlam);
         }
         ctx->launches++;
         YAO_CUDA(cudaGetLastError());
@@ -496,7 +771,13 @@ int adjoint_tiles(Ctx* ctx, Reg* psi, Reg* lam, const Circuit* c, double* grad, 
     if (ndots)
         YAO_CUDA(cudaMemcpyAsync(dots.data(), d_dots, ndots * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     YAO_CUDA(cudaFreeAsync(buf, ctx->stream));
+    int herr = 0;
+    YAO_CUDA(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (herr) {
+        YAO_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+        return fail(YAO_ERR_TIMEOUT, "adjoint sweep: a tile copy wait gave up");
+    }
     doff = 0;
     for (const AdjPass& p : passes)
         for (size_t s = 0; s < p.slot_grad.size(); s++) grad[p.slot_grad[s]] = 2.0 * dots[doff++];

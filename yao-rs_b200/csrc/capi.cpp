@@ -821,7 +821,11 @@ int yao_apply_inplace_mode(const yao_circuit* cc, yao_reg* r, int32_t mode, int3
     // input's norm, so the FP64 norm of the input is restored afterwards
     // when blocks ran on the tensor cores or the circuit has 256 gates or
     // more (shorter CUDA-core runs drift by less than an FP32 ulp).
-    const bool renorm = mode == YAO_MODE_FUSED && r->precision == YAO_C64 && circuit_is_unitary(c);
+    // YAO_NORM_RESTORE=0 leaves the norm as the arithmetic produced it (for
+    // measuring the drift)
+    const char* nr_env = getenv("YAO_NORM_RESTORE");
+    const bool renorm = mode == YAO_MODE_FUSED && r->precision == YAO_C64 && circuit_is_unitary(c) &&
+                        !(nr_env && nr_env[0] == '0');
     double n0 = 0.0;
     if (renorm && (s = reduce_norm_sqr(r->ctx, r, &n0))) return s;
     r->ctx->tc_used = false;

@@ -211,31 +211,67 @@ int launch_dm_gate(Ctx* ctx, DM* d, const LGate& row, const LGate& col) {
 
 constexpr int kMaxKraus = 16;
 constexpr int kDCT = 128;  // channel kernel block size
+// A channel pass's description travels in the kernel parameters (about
+// 8.7 KB: no allocation and no copy per launch).  `mono[q]`: Kraus operator q
+// and its conjugate have at most one non-zero entry per row (Pauli products,
+// amplitude-damping jumps); perm[q][axis][i] is that entry's column (-1: the
+// row is zero).
 struct DMChan {
     int32_t k, nk, nlocked, pad;
     int8_t locked[32];
     uint64_t roff[4], coff[4];
     int32_t cls[kMaxKraus];       // GC_DIAG or GC_DENSE per Kraus operator
     uint32_t active[kMaxKraus];
+    int32_t mono[kMaxKraus];
+    int8_t perm[kMaxKraus][2][4];
+    double2 kr[kMaxKraus * 16], kc[kMaxKraus * 16];  // row / column matrices, 2^k x 2^k each
 };
 
+// c * x with the operation structure of num_complex, for a coefficient that
+// is real (c.y == 0) or imaginary (c.x == 0) by two products: the omitted
+// terms are products with an exact zero, so the result is the same number
+// (at most the sign of a zero differs).
+__device__ __forceinline__ double2 cmul_sparse(double2 c, double2 x) {
+    if (c.y == 0.0) return make_double2(__dmul_rn(c.x, x.x), __dmul_rn(c.x, x.y));
+    if (c.x == 0.0) return make_double2(-__dmul_rn(c.y, x.y), __dmul_rn(c.y, x.x));
+    return cmul_x(c, x);
+}
+// x *= c (MulAssign) for a diagonal entry, same shortcut
+__device__ __forceinline__ double2 cmulassign_sparse(double2 x, double2 c) {
+    if (c.y == 0.0) return make_double2(__dmul_rn(x.x, c.x), __dmul_rn(x.y, c.x));
+    return cmulassign_x(x, c);
+}
+
 // The untouched original group is kept in shared memory (one column per
-// thread), the branch and the accumulator in registers.
-template <int K>
-__global__ void __launch_bounds__(kDCT) k_dm_channel(double2* __restrict__ rho, uint64_t ngroups, const DMChan op,
-                                                    const double2* __restrict__ kr, const double2* __restrict__ kc) {
+// thread) and the accumulator in registers.  For each Kraus operator in
+// order: branch = original, K on the row bits, conj(K) on the column bits,
+// acc += branch (src/density_matrix.rs:181-224, per entry).  For a diagonal
+// or monomial operator, branch entry (a, b) depends on one original entry:
+// (K conj(K) applied per axis) it is
+//     cmul(kc[b], cmul(kr[a], orig[pr[a]][pc[b]]))
+// (monomial: kr[a] = K[a][pr[a]], kc[b] = conj(K)[b][pc[b]]; a zero row
+// contributes exact zeros, which leave the accumulator as it is) or
+//     (orig[a][b] *= kr[a]) *= kc[b]
+// (diagonal), the same operations on the same values as the row pass
+// followed by the column pass.  DENSE instantiation: channels with some
+// operator that is neither (the whole branch block in registers).
+template <int K, bool DENSE>
+__global__ void __launch_bounds__(kDCT, DENSE ? 1 : 4) k_dm_channel(double2* __restrict__ rho, uint64_t ngroups,
+                                                    const __grid_constant__ DMChan op) {
     constexpr int NL = 1 << K, MS = NL * NL;
     __shared__ double2 smr[kMaxKraus * MS], smc[kMaxKraus * MS];
     __shared__ double2 sorig[MS * kDCT];
+    __shared__ int8_t sperm[kMaxKraus][2][4];
     for (int i = threadIdx.x; i < op.nk * MS; i += blockDim.x) {
-        smr[i] = kr[i];
-        smc[i] = kc[i];
+        smr[i] = op.kr[i];
+        smc[i] = op.kc[i];
     }
+    for (int i = threadIdx.x; i < op.nk * 8; i += blockDim.x) (&sperm[0][0][0])[i] = (&op.perm[0][0][0])[i];
     __syncthreads();
     double2* orig = sorig + threadIdx.x;  // orig[(a*NL+b) * kDCT]
     GRID_STRIDE(g, ngroups) {
         uint64_t base = insert_zeros(g, op.locked, op.nlocked);
-        double2 acc[NL][NL], br[NL][NL];
+        double2 acc[NL][NL];
 #pragma unroll
         for (int a = 0; a < NL; a++)
 #pragma unroll
@@ -244,27 +280,69 @@ __global__ void __launch_bounds__(kDCT) k_dm_channel(double2* __restrict__ rho, 
                 acc[a][b] = make_double2(0.0, 0.0);
             }
         for (int q = 0; q < op.nk; q++) {
-#pragma unroll
-            for (int a = 0; a < NL; a++)
-#pragma unroll
-                for (int b = 0; b < NL; b++) br[a][b] = orig[(a * NL + b) * kDCT];
+            const double2* mr = smr + q * MS;
+            const double2* mc = smc + q * MS;
             if (op.cls[q] == GC_DIAG) {
-                axis_apply<GC_DIAG, K>(br, smr + q * MS, op.active[q], true);
-                axis_apply<GC_DIAG, K>(br, smc + q * MS, op.active[q], false);
-            } else {
-                axis_apply<GC_DENSE, K>(br, smr + q * MS, 0, true);
-                axis_apply<GC_DENSE, K>(br, smc + q * MS, 0, false);
+#pragma unroll
+                for (int a = 0; a < NL; a++) {
+                    const double2 dr = mr[a * (NL + 1)];
+#pragma unroll
+                    for (int b = 0; b < NL; b++) {
+                        const double2 y = cmulassign_sparse(cmulassign_sparse(orig[(a * NL + b) * kDCT], dr),
+                                                            mc[b * (NL + 1)]);
+                        acc[a][b] = cadd_x(acc[a][b], y);
+                    }
+                }
+            } else if (!DENSE || op.mono[q]) {
+                const int8_t* pr = sperm[q][0];
+                const int8_t* pc = sperm[q][1];
+#pragma unroll
+                for (int a = 0; a < NL; a++) {
+                    const int ra = pr[a];
+                    if (ra < 0) continue;
+                    const double2 cr = mr[a * NL + ra];
+#pragma unroll
+                    for (int b = 0; b < NL; b++) {
+                        const int cb = pc[b];
+                        if (cb < 0) continue;
+                        const double2 y = cmul_sparse(mc[b * NL + cb], cmul_sparse(cr, orig[(ra * NL + cb) * kDCT]));
+                        acc[a][b] = cadd_x(acc[a][b], y);
+                    }
+                }
+            } else if constexpr (DENSE) {
+                double2 br[NL][NL];
+#pragma unroll
+                for (int a = 0; a < NL; a++)
+#pragma unroll
+                    for (int b = 0; b < NL; b++) br[a][b] = orig[(a * NL + b) * kDCT];
+                axis_apply<GC_DENSE, K>(br, mr, 0, true);
+                axis_apply<GC_DENSE, K>(br, mc, 0, false);
+#pragma unroll
+                for (int a = 0; a < NL; a++)
+#pragma unroll
+                    for (int b = 0; b < NL; b++) acc[a][b] = cadd_x(acc[a][b], br[a][b]);
             }
-#pragma unroll
-            for (int a = 0; a < NL; a++)
-#pragma unroll
-                for (int b = 0; b < NL; b++) acc[a][b] = cadd_x(acc[a][b], br[a][b]);
         }
 #pragma unroll
         for (int a = 0; a < NL; a++)
 #pragma unroll
             for (int b = 0; b < NL; b++) rho[base + op.roff[a] + op.coff[b]] = acc[a][b];
     }
+}
+
+// Column of the single non-zero entry of each row of a d x d matrix (-1 for
+// a zero row); false when some row has two or more.
+static bool monomial_rows(const std::vector<Cx>& m, int d, int8_t* perm) {
+    for (int i = 0; i < d; i++) {
+        perm[i] = -1;
+        for (int j = 0; j < d; j++) {
+            const Cx c = m[(size_t)i * d + j];
+            if (c.re == 0.0 && c.im == 0.0) continue;
+            if (perm[i] >= 0) return false;
+            perm[i] = (int8_t)j;
+        }
+    }
+    return true;
 }
 
 int launch_dm_channel(Ctx* ctx, DM* d, const std::vector<LGate>& rows, const std::vector<LGate>& cols,
@@ -285,32 +363,38 @@ int launch_dm_channel(Ctx* ctx, DM* d, const std::vector<LGate>& rows, const std
     offsets(rows[0], op.roff);
     offsets(cols[0], op.coff);
     const int NL = 1 << k, MS = NL * NL;
-    std::vector<double2> hr((size_t)nk * MS), hc((size_t)nk * MS);
     for (int q = 0; q < nk; q++) {
         // the 2q lowering sorts each Kraus operator's bits identically
         op.cls[q] = rows[q].cls;
         op.active[q] = active_mask(rows[q]) | active_mask(cols[q]);
-        for (size_t i = 0; i < rows[q].m.size(); i++) hr[(size_t)q * MS + i] = make_double2(rows[q].m[i].re, rows[q].m[i].im);
-        for (size_t i = 0; i < cols[q].m.size(); i++) hc[(size_t)q * MS + i] = make_double2(cols[q].m[i].re, cols[q].m[i].im);
-        if (rows[q].cls == GC_DIAG) op.active[q] = (1u << NL) - 1;  // multiply every entry, as the CPU path does
+        if (rows[q].cls == GC_DIAG) {
+            // a diagonal operator's entries, on the diagonal of the block
+            for (int i = 0; i < NL; i++) {
+                op.kr[q * MS + i * (NL + 1)] = make_double2(rows[q].m[i].re, rows[q].m[i].im);
+                op.kc[q * MS + i * (NL + 1)] = make_double2(cols[q].m[i].re, cols[q].m[i].im);
+            }
+            op.active[q] = (1u << NL) - 1;  // multiply every entry, as the CPU path does
+            continue;
+        }
+        for (int i = 0; i < MS; i++) {
+            op.kr[q * MS + i] = make_double2(rows[q].m[i].re, rows[q].m[i].im);
+            op.kc[q * MS + i] = make_double2(cols[q].m[i].re, cols[q].m[i].im);
+        }
+        op.mono[q] = monomial_rows(rows[q].m, NL, op.perm[q][0]) && monomial_rows(cols[q].m, NL, op.perm[q][1]);
     }
-    void* buf = nullptr;
-    size_t bytes = sizeof(double2) * (size_t)nk * MS;
-    YAO_CUDA(cudaMallocAsync(&buf, 2 * bytes, ctx->stream));
-    YAO_CUDA(cudaMemcpyAsync(buf, hr.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
-    YAO_CUDA(cudaMemcpyAsync((char*)buf + bytes, hc.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
     uint64_t ngroups = (uint64_t)1 << (2 * d->nbits - op.nlocked);
     unsigned grid = grid_for(ngroups, kDT, ctx->num_sms);
     ProfScope prof(ctx, "dm_channel", (double)ngroups * (double)(1 << (2 * k)) * 32.0);
+    bool dense = false;
+    for (int q = 0; q < nk; q++) dense |= op.cls[q] != GC_DIAG && !op.mono[q];
     if (k == 1)
-        k_dm_channel<1><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op, (const double2*)buf,
-                                                        (const double2*)((char*)buf + bytes));
+        dense ? k_dm_channel<1, true><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op)
+              : k_dm_channel<1, false><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);
     else
-        k_dm_channel<2><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op, (const double2*)buf,
-                                                        (const double2*)((char*)buf + bytes));
+        dense ? k_dm_channel<2, true><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op)
+              : k_dm_channel<2, false><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);
     ctx->launches++;
     YAO_CUDA(cudaGetLastError());
-    YAO_CUDA(cudaFreeAsync(buf, ctx->stream));
     (void)row_bits;
     (void)col_bits;
     return YAO_OK;

@@ -31,8 +31,11 @@
 #include <chrono>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "device_common.cuh"
 #include "tc_sm100.cuh"
+#include "tma_sm100.cuh"
 
 namespace yao {
 
@@ -48,7 +51,10 @@ struct TileHdr {
     int32_t mma;     // some wide op of the pass runs on the tensor cores
     int32_t dmma;    // complex128 FUSED: some dense 3..5-qubit block runs on the FP64 tensor cores
     int32_t tc_test; // failure-path test: tensor-core ops issue no copy and no MMA, waits give up after 0.1 s
-    int32_t pad_;
+    int32_t use_tma; // tiles move by TMA (tma, nstage); else by cp.async
+    int32_t nstage;  // TMA tile buffers in flight (2..3)
+    int32_t tc_variant;  // tensor-core block variant bits (kTcVar*)
+    TmaPlan tma;
 };
 
 struct TOp {
@@ -147,8 +153,14 @@ struct TSeg {
 
 // XOR swizzle of the shared-memory tile against bank conflicts when the
 // lanes of a warp step through higher tile bits.
+// It is the 128-byte swizzle of the TMA unit: in every 1024-byte block,
+// 16-byte chunk q of 128-byte row r sits at chunk q ^ (r % 8), i.e. bits
+// 4..6 of the byte offset are XORed with bits 7..9.  In amplitude units:
+// complex128 (16 B) XORs position bits 0..2 with bits 3..5, complex64 (8 B)
+// bits 1..3 with bits 4..6 (bit 0 stays: the two halves of a 16-byte chunk
+// stay together, and swz(l | 1) = swz(l) | 1).
 __device__ __forceinline__ uint32_t swz(uint32_t l, double2*) { return l ^ ((l >> 3) & 7); }
-__device__ __forceinline__ uint32_t swz(uint32_t l, float2*) { return l ^ ((l >> 4) & 15); }
+__device__ __forceinline__ uint32_t swz(uint32_t l, float2*) { return l ^ (((l >> 4) & 7) << 1); }
 
 // Global index of tile position l: the low m positions are the low bits
 // themselves; the rest scatter to the tile's higher bits through a table of
@@ -293,9 +305,16 @@ constexpr int kTcTileBits = 12;         // tile of a tensor-core pass (2^12 comp
 constexpr int kTcRows = 128;            // groups per tile = MMA M
 constexpr int kTcN = 64;                // real outputs = MMA N
 constexpr int kTcKr = 64;               // real inputs = reduction length
-constexpr int kTcOpFloats = 2 * kTcN * kTcKr;  // Bh then Bl
+constexpr int kTcOpFloats = 3 * kTcN * kTcKr;  // Bh, Bl, then Bll (B - Bh - Bl rounded to TF32)
 constexpr uint32_t kTcSbo = (kTcKr / 4) * 128;  // bytes between 8-row groups
-constexpr size_t kTcSmemBytes = 2 * (size_t)kTcRows * kTcKr * 4 + 2 * (size_t)kTcN * kTcKr * 4;  // Xh, Xl, Bh, Bl
+constexpr size_t kTcSmemBytes = 2 * (size_t)kTcRows * kTcKr * 4 + 3 * (size_t)kTcN * kTcKr * 4;  // Xh, Xl, Bh, Bl, Bll
+constexpr int kTcCols = 128;  // tensor-memory columns: the main accumulator, then the correction accumulator
+// Variants of the tensor-core block (hdr.tc_variant bits, from YAO_TC_VARIANT):
+//   1: X's low part rounded to TF32 (round to nearest) before the MMAs read it
+//   2: the correction products (Xh Bl + Xl Bh [+ Xh Bll]) accumulate apart from
+//      Xh Bh, and the two are added in FP32 (round to nearest) on read-back
+//   4: B in three TF32 parts, a fourth product Xh Bll
+constexpr int kTcVarXlRound = 1, kTcVarSplitAcc = 2, kTcVarB3 = 4;
 constexpr uint64_t kTcWaitNs = 1000000000ull;  // 1 s
 
 __device__ __forceinline__ uint64_t global_ns_tc() {
@@ -314,7 +333,9 @@ struct TcCtx {
     float* xl;
     float* bh;
     float* bl;
-    const float* mmat;   // every tensor-core op's Bh, Bl of the pass (global)
+    float* bll;
+    int variant;         // kTcVar* bits
+    const float* mmat;   // every tensor-core op's Bh, Bl, Bll of the pass (global)
     int loaded;          // op offset whose B operands are in shared memory
     int failed;          // a completion wait ran out (results of the pass are void)
     int* err;
@@ -332,12 +353,14 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
         float2* t = (float2*)s;
         const uint32_t nt = blockDim.x, tid = threadIdx.x;
         __shared__ uint32_t co[1 << kTcK];  // tile offset of local index c
-        // B operands of this op (Bh, Bl: 32 KiB contiguous): one bulk copy
-        // started now, waited for by the MMA-issuing thread
+        // B operands of this op (Bh, Bl[, Bll]: 32 or 48 KiB contiguous): one
+        // bulk copy started now, waited for by the MMA-issuing thread
+        const bool split = tc.variant & kTcVarSplitAcc, b3 = tc.variant & kTcVarB3;
+        const uint32_t bbytes = (b3 ? 3u : 2u) * kTcN * kTcKr * 4;
         const bool need_b = tc.loaded != op.mma;
         if (need_b && tid == 0 && !tc.stall) {
-            tc::mbar_arrive_expect_tx(tc.bbar, (uint32_t)kTcOpFloats * 4);
-            tc::bulk_g2s(tc.bh, tc.mmat + op.mma, (uint32_t)kTcOpFloats * 4, tc.bbar);
+            tc::mbar_arrive_expect_tx(tc.bbar, bbytes);
+            tc::bulk_g2s(tc.bh, tc.mmat + op.mma, bbytes, tc.bbar);
         }
         if (tid < (1u << kTcK)) {
             uint32_t o = 0;
@@ -358,7 +381,9 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
                 const float2 v0 = t[swz(gb | co[2 * jp], (float2*)nullptr)];
                 const float2 v1 = t[swz(gb | co[2 * jp + 1], (float2*)nullptr)];
                 const float4 h = make_float4(tc::to_tf32(v0.x), tc::to_tf32(v0.y), tc::to_tf32(v1.x), tc::to_tf32(v1.y));
-                const float4 l = make_float4(v0.x - h.x, v0.y - h.y, v1.x - h.z, v1.y - h.w);
+                float4 l = make_float4(v0.x - h.x, v0.y - h.y, v1.x - h.z, v1.y - h.w);
+                if (tc.variant & kTcVarXlRound)
+                    l = make_float4(tc::to_tf32(l.x), tc::to_tf32(l.y), tc::to_tf32(l.z), tc::to_tf32(l.w));
                 const uint32_t off = tc_off(g, 4 * jp);
                 *(float4*)((char*)tc.xh + off) = h;
                 *(float4*)((char*)tc.xl + off) = l;
@@ -372,7 +397,8 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
         bool b_ok = true;
         constexpr uint32_t idesc = tc::idesc_tf32(kTcRows, kTcN);
         const uint32_t xh = tc::smem_u32(tc.xh), xl = tc::smem_u32(tc.xl);
-        const uint32_t bh = tc::smem_u32(tc.bh), bl = tc::smem_u32(tc.bl);
+        const uint32_t bh = tc::smem_u32(tc.bh), bl = tc::smem_u32(tc.bl), bll = tc::smem_u32(tc.bll);
+        const uint32_t acc_c = tc.tmem + (split ? (uint32_t)kTcN : 0u);  // correction accumulator
         auto issue = [&](int k0) {
             tc::fence_after_sync();
 #pragma unroll
@@ -380,8 +406,12 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
                 const uint32_t o = (uint32_t)k8 * 256;
                 tc::mma_tf32(tc.tmem, tc::smem_desc(xh + o, 128, kTcSbo), tc::smem_desc(bh + o, 128, kTcSbo), idesc,
                              k8 > 0);
-                tc::mma_tf32(tc.tmem, tc::smem_desc(xh + o, 128, kTcSbo), tc::smem_desc(bl + o, 128, kTcSbo), idesc, 1);
-                tc::mma_tf32(tc.tmem, tc::smem_desc(xl + o, 128, kTcSbo), tc::smem_desc(bh + o, 128, kTcSbo), idesc, 1);
+                tc::mma_tf32(acc_c, tc::smem_desc(xh + o, 128, kTcSbo), tc::smem_desc(bl + o, 128, kTcSbo), idesc,
+                             split ? k8 > 0 : 1);
+                tc::mma_tf32(acc_c, tc::smem_desc(xl + o, 128, kTcSbo), tc::smem_desc(bh + o, 128, kTcSbo), idesc, 1);
+                if (b3)
+                    tc::mma_tf32(acc_c, tc::smem_desc(xh + o, 128, kTcSbo), tc::smem_desc(bll + o, 128, kTcSbo), idesc,
+                                 1);
             }
         };
         build_x(0);
@@ -428,9 +458,13 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
             for (int q = 0; q < kTcK; q++) b = ins0(b, op.ts[q]);
             const uint32_t c0 = (warp >> 2) * cpw;
             for (uint32_t c = c0; c < c0 + cpw; c += 16) {
-                uint32_t r[16];
+                uint32_t r[16], rc[16];
                 tc::tmem_ld16(tc.tmem + (((warp & 3) << 5) << 16) + c, r);
+                if (split) tc::tmem_ld16(tc.tmem + (((warp & 3) << 5) << 16) + kTcN + c, rc);
                 tc::tmem_wait_ld();
+                if (split)
+#pragma unroll
+                    for (int i = 0; i < 16; i++) r[i] = __float_as_uint(__uint_as_float(r[i]) + __uint_as_float(rc[i]));
 #pragma unroll
                 for (int i = 0; i < 8; i++)
                     t[swz(b | co[(c >> 1) + i], (float2*)nullptr)] =
@@ -550,7 +584,23 @@ __device__ __forceinline__ void tile_compute(const TileHdr& hdr, uint64_t base, 
 #pragma unroll
                     for (int i = 0; i < RB; i++) o |= (uint32_t)((j >> i) & 1) << sg.rbs[i];
                     roff[j] = o;
-                    v[j] = s[swz(lbase | o, tag)];
+                }
+                // complex64 with tile bit 0 among the register bits: the
+                // pairs (l, l | 1) are one 16-byte chunk each
+                const bool pair = sizeof(V) == 8 && sg.rbs[0] == 0;
+                if constexpr (sizeof(V) == 8) {
+                    if (pair) {
+#pragma unroll
+                        for (int j = 0; j < NA; j += 2) {
+                            const float4 q = *(const float4*)&s[swz(lbase | roff[j], tag)];
+                            v[j] = make_float2(q.x, q.y);
+                            v[j + 1] = make_float2(q.z, q.w);
+                        }
+                    }
+                }
+                if (!pair) {
+#pragma unroll
+                    for (int j = 0; j < NA; j++) v[j] = s[swz(lbase | roff[j], tag)];
                 }
                 for (int oi = sg.op_begin; oi < sg.op_end; oi++) {
                     const TOp& op = ops[oi];
@@ -578,8 +628,19 @@ __device__ __forceinline__ void tile_compute(const TileHdr& hdr, uint64_t base, 
                         reg2_at<V, EXACT, RB, 0, 1>(op.rp[0], op.rp[1], v, lbase, roff, op, m);
                     }
                 }
+                if constexpr (sizeof(V) == 8) {
+                    if (pair) {
 #pragma unroll
-                for (int j = 0; j < NA; j++) s[swz(lbase | roff[j], tag)] = v[j];
+                        for (int j = 0; j < NA; j += 2) {
+                            const float2 a = v[j], b = v[j + 1];
+                            *(float4*)&s[swz(lbase | roff[j], tag)] = make_float4(a.x, a.y, b.x, b.y);
+                        }
+                    }
+                }
+                if (!pair) {
+#pragma unroll
+                    for (int j = 0; j < NA; j++) s[swz(lbase | roff[j], tag)] = v[j];
+                }
             }
         } else {
             // one dense op on k >= 3 targets (a 2^k x 2^k matrix times the
@@ -706,31 +767,6 @@ __device__ __forceinline__ void tile_store(V* __restrict__ st, const TileHdr& hd
     for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) st[tile_global(base, l, m, hoff)] = s[swz(l, (V*)tag)];
 }
 
-// Asynchronous tile load (cp.async, no register staging): the copies of one
-// call form one commit group.
-__device__ __forceinline__ void cp_async_amp(double2* dst, const double2* src) {
-    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_amp(float2* dst, const float2* src) {
-    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-template <typename V>
-__device__ __forceinline__ void tile_load_async(const V* __restrict__ st, const TileHdr& hdr, const uint64_t* hoff,
-                                                uint64_t base, V* s) {
-    V* tag = nullptr;
-    const uint32_t T = 1u << hdr.tbits;
-    const int m = hdr.m;
-    for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) cp_async_amp(&s[swz(l, tag)], &st[tile_global(base, l, m, hoff)]);
-}
-
 // Bytes of shared memory that hold a staged pass description.
 __host__ __device__ inline size_t staged_bytes(int nops, int nsegs, int ncoef, size_t coef_size) {
     auto a16 = [](size_t x) { return (x + 15) / 16 * 16; };
@@ -776,9 +812,35 @@ __device__ __forceinline__ void stage_pass(const TileHdr& hdr, unsigned char* sm
     coef = sc;
 }
 
-// One pass over every tile.  Two tile buffers: while a CTA works on one
-// tile, the next tile it owns streams into the other buffer (cp.async), so
-// HBM traffic overlaps the arithmetic even with one CTA per SM.
+// One thread: every box of the tile at `base` into shared memory at `dst`,
+// all counted on `bar` (armed here with the tile's bytes).
+__device__ __forceinline__ void tma_load_tile(const CUtensorMap* map, const TileHdr& hdr, uint64_t base,
+                                              uint32_t dst, uint64_t* bar, uint32_t tile_bytes) {
+    tc::mbar_arrive_expect_tx(bar, tile_bytes);
+    tma::load_boxes(map, hdr.tma, base, dst, tc::smem_u32(bar));
+}
+
+// One thread: every box of the tile at `base` from shared memory at `src`
+// back to the state, as one bulk async-group.
+__device__ __forceinline__ void tma_store_tile(const CUtensorMap* map, const TileHdr& hdr, uint64_t base,
+                                               uint32_t src) {
+    tma::store_boxes(map, hdr.tma, base, src);
+    tma::commit_group();
+}
+
+constexpr uint64_t kTileWaitNs = 1000000000ull;  // 1 s
+constexpr int kMaxStages = 3;
+
+// One pass over every tile.  Persistent: each CTA loops over the tiles t =
+// blockIdx.x, blockIdx.x + gridDim.x, ...
+//  - TMA form (hdr.use_tma): `nstage` tile buffers; one thread issues the
+//    tile's box copies (tensor map `tmap`) nstage - 1 tiles ahead, every
+//    thread waits for its tile on the buffer's mbarrier (bounded: 1 s, then
+//    the error word is set and the pass's results are void), the tile is
+//    computed, and the same thread stores it back with bulk tensor stores
+//    while the next tiles compute.  No thread computes an address.
+//  - plain form (tiles of less than 2 KiB, and passes without a TMA
+//    plan): each tile is loaded, computed and stored in turn.
 // TCK: the pass holds tensor-core ops (complex64 FUSED only); a separate
 // instantiation, so passes without them carry none of its state.
 // DM: the pass holds dense blocks for the FP64 tensor cores (complex128
@@ -789,33 +851,43 @@ __device__ __forceinline__ void stage_pass(const TileHdr& hdr, unsigned char* sm
 template <typename V, bool EXACT, int RB, bool TCK, bool STG, bool DM = false>
 __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
     k_tile_pass(V* __restrict__ st, const TileHdr phdr, const TOp* __restrict__ gops, const TSeg* __restrict__ gsegs,
-                const typename CoefT<V>::C* __restrict__ gcoef, const float* __restrict__ mmat, int* __restrict__ err) {
+                const typename CoefT<V>::C* __restrict__ gcoef, const float* __restrict__ mmat, int* __restrict__ err,
+                const __grid_constant__ CUtensorMap tmap) {
     constexpr bool TC = TCK && sizeof(V) == 8 && !EXACT;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ TileHdr hdr;  // indexed with run-time subscripts: keep it out of the parameter space
     __shared__ uint64_t hoff[1 << kMaxScatterBits];
     __shared__ uint64_t tc_bar, tc_bbar;
+    __shared__ uint64_t full_bar[kMaxStages];
     __shared__ uint32_t tc_tmem;
     __shared__ uint64_t bt[4 * 256];  // tile base tables
     if (threadIdx.x == 0) hdr = phdr;
     __syncthreads();
+    // tile buffers from the first 1024-byte boundary (the TMA swizzle
+    // pattern is a function of the shared-memory address)
+    unsigned char* smem =
+        smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
+    const bool use_tma = hdr.use_tma != 0;
+    const int nbuf = use_tma ? hdr.nstage : 1;
     const TOp* ops = gops;
     const TSeg* segs = gsegs;
     const typename CoefT<V>::C* coef = gcoef;
-    if constexpr (STG) stage_pass<V>(hdr, smem_raw, 2, ops, segs, coef);
-    tile_offsets(hdr, hoff);
+    if constexpr (STG) stage_pass<V>(hdr, smem, nbuf, ops, segs, coef);
+    if (!use_tma) tile_offsets(hdr, hoff);
     tile_base_tables(hdr, bt);
     TcCtx tcx;
     constexpr bool use_tc = TC;
     if constexpr (use_tc) {
-        // operands after the two tiles and the staged pass description (1 KiB aligned)
-        size_t off = 2 * ((size_t)1 << hdr.tbits) * sizeof(V);
+        // operands after the tiles and the staged pass description (1 KiB aligned)
+        size_t off = (size_t)nbuf * ((size_t)1 << hdr.tbits) * sizeof(V);
         if (STG) off += staged_bytes(hdr.nops, hdr.nsegs, hdr.ncoef, sizeof(typename CoefT<V>::C));
         off = (off + 1023) & ~(size_t)1023;
-        tcx.xh = (float*)(smem_raw + off);
+        tcx.xh = (float*)(smem + off);
         tcx.xl = tcx.xh + kTcRows * kTcKr;
         tcx.bh = tcx.xl + kTcRows * kTcKr;
         tcx.bl = tcx.bh + kTcN * kTcKr;
+        tcx.bll = tcx.bl + kTcN * kTcKr;
+        tcx.variant = hdr.tc_variant;
         tcx.mmat = mmat;
         tcx.loaded = -1;
         tcx.failed = 0;
@@ -831,7 +903,7 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
             tc::mbar_init(&tc_bbar, 1);
         }
         if (threadIdx.x < 32) {
-            tc::tmem_alloc(&tc_tmem, kTcN);
+            tc::tmem_alloc(&tc_tmem, kTcCols);
             tc::tmem_relinquish();
         }
         tc::fence_before_sync();
@@ -840,29 +912,79 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         tcx.tmem = tc_tmem;
     }
     const uint32_t T = 1u << hdr.tbits;
-    V* cur = (V*)smem_raw;
-    V* nxt = cur + T;
+    const uint32_t tile_bytes = T * (uint32_t)sizeof(V);
+    const uint32_t sbase = tc::smem_u32(smem);
+    const uint64_t grid = gridDim.x;
     uint64_t t = blockIdx.x;
-    if (t < hdr.ntiles) tile_load_async<V>(st, hdr, hoff, tile_base(t, bt), cur);
-    cp_async_commit();
-    for (; t < hdr.ntiles; t += gridDim.x) {
-        const uint64_t tn = t + gridDim.x;
-        if (tn < hdr.ntiles) tile_load_async<V>(st, hdr, hoff, tile_base(tn, bt), nxt);
-        cp_async_commit();
-        cp_async_wait<1>();  // this thread's copies into `cur` have landed
-        __syncthreads();     // ... and every other thread's
+    // loads in flight per buffer (thread 0's view): a wait that gave up
+    // leaves one, waited for again before the CTA exits
+    uint32_t pending = 0;
+    if (use_tma) {
+        if (threadIdx.x == 0) {
+            tma::prefetch_map(&tmap);
+            for (int q = 0; q < nbuf; q++) tc::mbar_init(&full_bar[q], 1);
+            for (int q = 0; q < nbuf - 1; q++) {
+                const uint64_t tq = t + (uint64_t)q * grid;
+                if (tq < hdr.ntiles) {
+                    tma_load_tile(&tmap, hdr, tile_base(tq, bt), sbase + q * tile_bytes, &full_bar[q], tile_bytes);
+                    pending |= 1u << q;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    bool dead = false;  // a wait gave up: skip the remaining waits
+    for (uint32_t it = 0; t < hdr.ntiles; t += grid, it++) {
+        const uint32_t b = use_tma ? it % (uint32_t)nbuf : 0;
+        V* cur = (V*)(smem + (size_t)b * tile_bytes);
         const uint64_t base = tile_base(t, bt);
+        if (use_tma) {
+            if (threadIdx.x == 0) {
+                const uint64_t tn = t + (uint64_t)(nbuf - 1) * grid;
+                if (tn < hdr.ntiles) {
+                    const uint32_t bn = (it + (uint32_t)nbuf - 1) % (uint32_t)nbuf;
+                    tma::wait_group_read<0>();  // the previous tile's store has read buffer bn
+                    tma_load_tile(&tmap, hdr, tile_base(tn, bt), sbase + bn * tile_bytes, &full_bar[bn], tile_bytes);
+                    pending |= 1u << bn;
+                }
+            }
+            if (!dead) {
+                const uint32_t parity = (it / (uint32_t)nbuf) & 1u;
+                const uint64_t t0 = global_ns_tc();
+                while (!tc::mbar_try_wait(&full_bar[b], parity)) {
+                    if (global_ns_tc() - t0 > kTileWaitNs) {
+                        dead = true;
+                        atomicExch(err, 1);
+                        break;
+                    }
+                }
+                if (!dead && threadIdx.x == 0) pending &= ~(1u << b);
+            }
+        } else {
+            tile_load<V, false>(st, hdr, hoff, base, cur);  // ends with __syncthreads
+        }
         if constexpr (use_tc)
             tile_compute<V, EXACT, RB, true>(hdr, base, ops, segs, coef, cur, &tcx);
         else
             tile_compute<V, EXACT, RB, false, DM>(hdr, base, ops, segs, coef, cur);
-        tile_store<V>(st, hdr, hoff, base, cur);
-        __syncthreads();  // `cur` is read out before it receives tile t + 2 * gridDim.x
-        V* tmp = cur;
-        cur = nxt;
-        nxt = tmp;
+        if (use_tma) {
+            tc::fence_proxy_async();  // this thread's tile writes are visible to the bulk store
+            __syncthreads();
+            if (threadIdx.x == 0) tma_store_tile(&tmap, hdr, base, sbase + b * tile_bytes);
+        } else {
+            tile_store<V>(st, hdr, hoff, base, cur);
+            __syncthreads();  // `cur` is read out before it receives the next tile
+        }
     }
-    cp_async_wait<0>();
+    if (use_tma && threadIdx.x == 0) {
+        tma::wait_group<0>();  // stores complete before the shared memory goes away
+        const uint64_t t0 = global_ns_tc();
+        for (int q = 0; q < nbuf; q++)
+            if (pending & (1u << q))
+                for (uint32_t ph = 0; ph < 2; ph++)
+                    while (!tc::mbar_try_wait(&full_bar[q], ph) && global_ns_tc() - t0 < kTileWaitNs) {
+                    }
+    }
     if constexpr (use_tc) {
         // an MMA still in flight after a wait that gave up: wait for it
         // again (bounded) before the accumulator is freed
@@ -878,7 +1000,7 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         __syncthreads();
         if (threadIdx.x < 32) {
             tc::fence_after_sync();
-            tc::tmem_dealloc(tcx.tmem, kTcN);
+            tc::tmem_dealloc(tcx.tmem, kTcCols);
         }
     }
 }
@@ -1018,7 +1140,9 @@ constexpr int max_reg_bits() {
 // Cut a pass's ops into segments (see TSeg): consecutive ops whose moving
 // tile bits fit in rb register bits share a register segment; a dense op on
 // three or more targets is a wide segment of its own.
-static void plan_segments(PassPlan& pp, int rb) {
+// pair0 (complex64 tiles): tile bit 0 is the first padding bit of a
+// register segment, so each thread's amplitudes come in 16-byte pairs.
+static void plan_segments(PassPlan& pp, int rb, bool pair0 = false) {
     // every non-wide op must fit one register segment
     for (const TOp& op : pp.ops)
         if (op.cls != GC_DIAG && !(op.cls == GC_DENSE && op.k >= 3)) rb = std::max(rb, (int)op.k);
@@ -1051,6 +1175,7 @@ static void plan_segments(PassPlan& pp, int rb) {
         }
         // pad with the highest unused tile bits: lanes of a warp then step
         // through the low bits, which are contiguous in shared memory
+        if (pair0 && (int)bits.size() < rb) bits.insert(0);
         for (int b = tbits - 1; (int)bits.size() < rb && b >= 0; b--) bits.insert(b);
         std::vector<int> rbs(bits.begin(), bits.end());
         for (int q = 0; q < rb; q++) sg.rbs[q] = (int8_t)rbs[q];
@@ -1376,7 +1501,7 @@ static void fuse_blocks(const std::vector<LGate>& prog_in, uint32_t nbits, int k
 template <typename V, bool EXACT, int RB, bool TCK, bool STG, bool DM = false>
 static int launch_tile_k(int num_sms, unsigned threads, size_t smem, cudaStream_t s, V* st, const TileHdr& hdr,
                          const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef, const float* mmat,
-                         int* err) {
+                         int* err, const CUtensorMap& tmap) {
     static bool attr = false;
     if (!attr) {
         int dev = 0, optin = 0;
@@ -1394,44 +1519,44 @@ static int launch_tile_k(int num_sms, unsigned threads, size_t smem, cudaStream_
     YAO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_pass<V, EXACT, RB, TCK, STG, DM>, (int)threads, smem));
     if (per_sm < 1) return fail(YAO_ERR_UNSUPPORTED, "tile pass does not fit on an SM");
     const unsigned grid = (unsigned)std::min<uint64_t>(hdr.ntiles, (uint64_t)per_sm * (uint64_t)num_sms);
-    k_tile_pass<V, EXACT, RB, TCK, STG, DM><<<grid, threads, smem, s>>>(st, hdr, ops, segs, coef, mmat, err);
+    k_tile_pass<V, EXACT, RB, TCK, STG, DM><<<grid, threads, smem, s>>>(st, hdr, ops, segs, coef, mmat, err, tmap);
     return YAO_OK;
 }
 
 template <typename V, bool EXACT, int RB>
 static int launch_tile_rb(int num_sms, unsigned threads, size_t smem, cudaStream_t s, V* st, const TileHdr& hdr,
                           const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef, const float* mmat,
-                          int* err) {
+                          int* err, const CUtensorMap& tmap) {
     if constexpr (sizeof(V) == 8 && !EXACT) {
         if (hdr.mma)
             return hdr.staged
-                       ? launch_tile_k<V, EXACT, RB, true, true>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err)
-                       : launch_tile_k<V, EXACT, RB, true, false>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
+                       ? launch_tile_k<V, EXACT, RB, true, true>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err, tmap)
+                       : launch_tile_k<V, EXACT, RB, true, false>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err, tmap);
     }
     if constexpr (sizeof(V) == 16 && !EXACT && RB >= 2) {
         if (hdr.dmma)
             return hdr.staged
                        ? launch_tile_k<V, EXACT, RB, false, true, true>(num_sms, threads, smem, s, st, hdr, ops, segs, coef,
-                                                                        mmat, err)
+                                                                        mmat, err, tmap)
                        : launch_tile_k<V, EXACT, RB, false, false, true>(num_sms, threads, smem, s, st, hdr, ops, segs,
-                                                                         coef, mmat, err);
+                                                                         coef, mmat, err, tmap);
     }
     return hdr.staged
-               ? launch_tile_k<V, EXACT, RB, false, true>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err)
-               : launch_tile_k<V, EXACT, RB, false, false>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
+               ? launch_tile_k<V, EXACT, RB, false, true>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err, tmap)
+               : launch_tile_k<V, EXACT, RB, false, false>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err, tmap);
 }
 
 template <typename V, bool EXACT>
 static int launch_tile(int rb, int num_sms, unsigned threads, size_t smem, cudaStream_t s, V* st,
                        const TileHdr& hdr, const TOp* ops, const TSeg* segs, const typename CoefT<V>::C* coef,
-                       const float* mmat, int* err) {
+                       const float* mmat, int* err, const CUtensorMap& tmap) {
     switch (rb) {
-    case 1: return launch_tile_rb<V, EXACT, 1>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
-    case 2: return launch_tile_rb<V, EXACT, 2>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
-    case 3: return launch_tile_rb<V, EXACT, 3>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
+    case 1: return launch_tile_rb<V, EXACT, 1>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err, tmap);
+    case 2: return launch_tile_rb<V, EXACT, 2>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err, tmap);
+    case 3: return launch_tile_rb<V, EXACT, 3>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err, tmap);
     case 4:
         if constexpr (sizeof(V) == 8)
-            return launch_tile_rb<V, EXACT, 4>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err);
+            return launch_tile_rb<V, EXACT, 4>(num_sms, threads, smem, s, st, hdr, ops, segs, coef, mmat, err, tmap);
         break;
     default: break;
     }
@@ -1521,6 +1646,89 @@ static int grow_host(void** p, size_t* have, size_t bytes) {
     return YAO_OK;
 }
 
+// Tensor-core block variant (kTcVar* bits; YAO_TC_VARIANT overrides).
+static int tc_variant() {
+    const char* e = getenv("YAO_TC_VARIANT");
+    return e ? (atoi(e) & 7) : 0;
+}
+
+// ------------------------------------------------------------- TMA maps
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (the library does not link libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
+bool tma_enabled() {
+    const char* e = getenv("YAO_TMA");
+    return !(e && e[0] == '0');
+}
+
+// The TMA plan of a tile (see TmaPlan) whose positions are the global bits
+// tb[0] < tb[1] < ... < tb[tbits - 1], and its tensor map over the state
+// `st` of 2^nbits amplitudes of `amp` bytes.  Dimension 0 is the lowest c
+// bits (128 bytes: c = 4 for complex64, 3 for complex128); then each run of
+// consecutive global bits among the next tile positions (at most 8 bits a
+// run: a box edge is at most 256) is one dimension, up to 4 of them; tile
+// positions beyond those are enumerated (at least 1024 bytes a box, so
+// every box lands on a swizzle-atom boundary).  Returns false when the tile
+// cannot move by TMA (tiny tiles, low bits 0..c-1 not all in the tile,
+// coordinates beyond 31 bits); the caller then moves it with plain copies.
+bool tma_make_plan(const int8_t* tb, int tbits, uint32_t nbits, size_t amp, void* st, TmaPlan& p, CUtensorMap* map) {
+    const int c = amp == 8 ? 4 : 3;
+    int m = 0;
+    while (m < tbits && tb[m] == m) m++;
+    if (m < c || ((size_t)1 << tbits) * amp < 2048 || nbits > 33) return false;
+    struct Run {
+        int g0, len;
+    };
+    std::vector<Run> runs;
+    int pos = c, J = c;
+    while (pos < tbits && (int)runs.size() < 4) {
+        Run r{tb[pos], 1};
+        while (pos + r.len < tbits && r.len < 8 && tb[pos + r.len] == r.g0 + r.len) r.len++;
+        runs.push_back(r);
+        pos += r.len;
+        J = pos;
+    }
+    if (((size_t)1 << J) * amp < 1024 || tbits - J > 6) return false;
+    memset(&p, 0, sizeof(p));
+    p.nebits = tbits - J;
+    for (int q = 0; q < p.nebits; q++) p.ebits[q] = tb[J + q];
+    p.copy_bytes = (int32_t)(((size_t)1 << J) * amp);
+    cuuint64_t dim[5], stride[4];
+    cuuint32_t box[5], estr[5] = {1, 1, 1, 1, 1};
+    const int nd = 1 + (int)runs.size();
+    for (int r = 0; r < 5; r++) {
+        const int sh = r == 0 ? 0 : (r < nd ? runs[r - 1].g0 : (int)nbits);
+        const int next = r + 1 < nd ? runs[r].g0 : (int)nbits;
+        p.shift[r] = (int8_t)sh;
+        p.width[r] = (int8_t)(r < nd ? next - sh : 0);
+        dim[r] = (cuuint64_t)1 << p.width[r];
+        box[r] = r == 0 ? 1u << c : (r < nd ? 1u << runs[r - 1].len : 1u);
+        if (r > 0) stride[r - 1] = ((cuuint64_t)1 << sh) * amp;
+    }
+    if (p.width[0] > 29) return false;  // c0 = 2 x (bits below the first run) stays a positive int32
+    dim[0] *= 2;  // two real elements per amplitude
+    box[0] *= 2;
+    auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const CUresult e = enc(map, amp == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, st,
+                           dim, stride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return e == CUDA_SUCCESS;
+}
+
 template <typename V, bool EXACT>
 static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
     typedef typename CoefT<V>::C C;
@@ -1562,25 +1770,36 @@ static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
     if (hdr.tbits - hdr.m > kMaxScatterBits) return fail(YAO_ERR_UNSUPPORTED, "tile has too many scattered bits");
     const size_t tile_bytes = ((size_t)1 << hdr.tbits) * sizeof(V);
     const size_t stg = staged_bytes(hdr.nops, hdr.nsegs, hdr.ncoef, sizeof(C));
-    // staged when it fits next to the tiles (and the tensor-core operands),
-    // with 16 KiB left for the kernel's static shared memory
+    // tiles by TMA when the pass has a plan; the pass description is staged
+    // when it fits next to two tiles (and the tensor-core operands), and a
+    // TMA pass gets a third tile buffer when that fits too; 16 KiB are left
+    // for the kernel's static shared memory, 1 KiB for aligning the tiles
+    CUtensorMap tmap;
+    memset(&tmap, 0, sizeof(tmap));
+    hdr.use_tma = tma_enabled() && tma_make_plan(hdr.tb, hdr.tbits, nbits, sizeof(V), st, hdr.tma, &tmap) ? 1 : 0;
     static int optin = 0;
     if (!optin) YAO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-    const size_t used = 2 * tile_bytes + (hdr.mma ? 1024 + kTcSmemBytes : 0) + 16 * 1024;
-    hdr.staged = used + stg <= (size_t)optin ? 1 : 0;
+    const size_t budget = (size_t)optin - 16 * 1024 - 1024;
+    const size_t tcb = hdr.mma ? 1024 + kTcSmemBytes : 0;
+    hdr.staged = 2 * tile_bytes + tcb + stg <= budget ? 1 : 0;
+    hdr.nstage = 2;
+    if (hdr.use_tma && 3 * tile_bytes + tcb + (hdr.staged ? stg : 0) <= budget) hdr.nstage = 3;
     hdr.dmma = dm ? 1 : 0;
     // YAO_TEST_TC_STALL=1 (failure-path test): the tensor-core ops issue
     // neither their operand copy nor their MMAs, so both bounded waits of
     // each op run out (0.1 s each) and the call reports YAO_ERR_TIMEOUT
-    if (hdr.mma)
+    if (hdr.mma) {
         if (const char* e = getenv("YAO_TEST_TC_STALL")) hdr.tc_test = e[0] == '1';
-    size_t smem = 2 * tile_bytes + (hdr.staged ? stg : 0);
+        hdr.tc_variant = tc_variant();
+    }
+    size_t smem = (size_t)(hdr.use_tma ? hdr.nstage : 1) * tile_bytes + (hdr.staged ? stg : 0);
     if (hdr.mma) smem = ((smem + 1023) & ~(size_t)1023) + kTcSmemBytes;
+    smem += 1024;
     const TOp* dops = (const TOp*)dbuf;
     const TSeg* dsegs = (const TSeg*)((char*)dbuf + sb_off);
     const C* dcoef = (const C*)((char*)dbuf + cb_off);
     const float* dmmat = (const float*)((char*)dbuf + mb_off);
-    if (hdr.mma && !ctx->d_err) {
+    if (!ctx->d_err) {
         YAO_CUDA(cudaMalloc((void**)&ctx->d_err, sizeof(int)));
         YAO_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
     }
@@ -1588,7 +1807,7 @@ static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
         ProfScope prof(ctx, hdr.mma ? "tile_pass_tc" : (EXACT ? "tile_pass_exact" : "tile_pass_fused"),
                        (double)pp.hdr.ntiles * (double)((uint64_t)1 << pp.hdr.tbits) * 2.0 * sizeof(V));
         int s = launch_tile<V, EXACT>(pp.rb, ctx->num_sms, threads, smem, ctx->stream, st, hdr, dops, dsegs, dcoef,
-                                      dmmat, ctx->d_err);
+                                      dmmat, ctx->d_err, tmap);
         if (s) return s;
     }
     ctx->launches++;
@@ -1641,6 +1860,7 @@ static void tc_prepare(PassPlan& pp) {
         pp.mmat.resize(pp.mmat.size() + kTcOpFloats, 0.f);
         float* bh = pp.mmat.data() + op.mma;
         float* bl = bh + kTcN * kTcKr;
+        float* bll = bl + kTcN * kTcKr;
         const int nl = 1 << kTcK;
         for (int i = 0; i < nl; i++)
             for (int j = 0; j < nl; j++) {
@@ -1653,8 +1873,10 @@ static void tc_prepare(PassPlan& pp) {
                         const uint32_t o = 2 * i + q, kk = 2 * j + p2;
                         const size_t at = ((o >> 3) * kTcSbo + (kk >> 2) * 128 + (o & 7) * 16 + (kk & 3) * 4) / 4;
                         const float h = host_tf32((float)v[q][p2]);
+                        const float l = host_tf32((float)(v[q][p2] - (double)h));
                         bh[at] = h;
-                        bl[at] = host_tf32((float)(v[q][p2] - (double)h));
+                        bl[at] = l;
+                        bll[at] = host_tf32((float)(v[q][p2] - (double)h - (double)l));
                     }
             }
         pp.hdr.mma = 1;
@@ -1677,7 +1899,7 @@ static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, c
             // at most kTileThreads threads per tile
             const int tb = (int)pp.hdr.tbits;
             const int rb = std::max(tb - 9, std::min(cfg.rb, tb));
-            plan_segments(pp, std::min(rb, max_reg_bits<V>()));
+            plan_segments(pp, std::min(rb, max_reg_bits<V>()), sizeof(V) == 8);
         }
     // dense 5-qubit blocks of complex64 FUSED runs go to the tensor cores
     // (YAO_TC=0 keeps them on the CUDA cores)
@@ -1702,13 +1924,15 @@ static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, c
         if (s) return s;
     }
     ctx->tc_used = any_tc;
-    if (any_tc) {
+    // a bounded wait of some pass (a tile's TMA copies, a tensor-core
+    // operand copy or MMA completion) gave up: the run's result is void
+    if (ctx->d_err) {
         int herr = 0;
         YAO_CUDA(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         YAO_CUDA(cudaStreamSynchronize(ctx->stream));
         if (herr) {
             YAO_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
-            return fail(YAO_ERR_TIMEOUT, "tensor-core pass: an MMA completion wait gave up");
+            return fail(YAO_ERR_TIMEOUT, "tile pass: a bounded wait (tile copy, tensor-core operand or MMA) gave up");
         }
     }
     return YAO_OK;
@@ -1826,42 +2050,46 @@ static int tune_program(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog, 
         YAO_CUDA(cudaEventElapsedTime(ms, a, b));
         return YAO_OK;
     };
-    // the better of two timed runs: one disturbed sample (power cap, other
-    // work on the host) does not pick a slower candidate
-    auto timed2 = [&](const TileConfig& c, float* ms) -> int {
-        float m1 = 0.f, m2 = 0.f;
-        int s = timed(c, &m1);
-        if (!s) s = timed(c, &m2);
-        *ms = std::min(m1, m2);
-        return s;
+    // Candidates are timed in interleaved rounds (every candidate once per
+    // round, after a warm-up round: first launches of each kernel variant
+    // carry one-time costs), keeping each one's best run.  Under the power
+    // cap the SM clock drifts over seconds; interleaving gives every
+    // candidate the same clocks, so a drift does not pick a slower one.
+    constexpr int kRounds = 3;
+    auto best_of = [&](const std::vector<TileConfig>& cand, size_t* pick, float* pick_ms) -> int {
+        std::vector<float> bestv(cand.size(), 0.f);
+        float ms = 0.f;
+        for (int round = 0; round <= kRounds; round++)
+            for (size_t i = 0; i < cand.size(); i++) {
+                int s = timed(cand[i], &ms);
+                if (s) return s;
+                if (round == 1 || (round > 1 && ms < bestv[i])) bestv[i] = ms;
+            }
+        *pick = 0;
+        for (size_t i = 1; i < cand.size(); i++)
+            if (bestv[i] < bestv[*pick]) *pick = i;
+        *pick_ms = bestv[*pick];
+        return YAO_OK;
     };
     std::vector<TileConfig> shapes;
     tile_candidates<V>(n, shapes);
-    TileConfig cur = *best;
-    float ms = 0.f, bms = 0.f;
-    // warm-up (first launches of each kernel variant carry one-time costs)
+    std::vector<TileConfig> cand;
     for (const TileConfig& sc : shapes) {
-        TileConfig c = cur;
+        TileConfig c = *best;
         c.tbits = sc.tbits;
         c.rb = sc.rb;
-        if ((st = timed(c, &ms))) break;
+        cand.push_back(c);
     }
-    bool have = false;
-    for (size_t i = 0; !st && i < shapes.size(); i++) {
-        TileConfig c = cur;
-        c.tbits = shapes[i].tbits;
-        c.rb = shapes[i].rb;
-        if ((st = timed2(c, &ms))) break;
-        if (!have || ms < bms) {
-            bms = ms;
-            *best = c;
-            have = true;
-        }
-    }
+    size_t pick = 0;
+    float bms = 0.f;
+    st = best_of(cand, &pick, &bms);
+    if (!st) *best = cand[pick];
     if (!st && mode == YAO_MODE_FUSED && kreq <= 0) {
-        // widths: each timed after a warm-up run (first-use costs), tensor-core
-        // widths with the 2^12 tile they need
+        // widths 2..6 with the chosen shape (tensor-core widths with the 2^12
+        // tile they need), the chosen configuration among them
         const TileConfig shape = *best;
+        cand.clear();
+        cand.push_back(shape);
         for (int k = 2; k <= kMaxTargets; k++) {
             if (k == shape.k) continue;
             TileConfig c = shape;
@@ -1870,13 +2098,10 @@ static int tune_program(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog, 
                 c.tbits = kTcTileBits;
                 c.rb = 3;
             }
-            if ((st = timed(c, &ms))) break;
-            if ((st = timed2(c, &ms))) break;
-            if (ms < bms) {
-                bms = ms;
-                *best = c;
-            }
+            cand.push_back(c);
         }
+        st = best_of(cand, &pick, &bms);
+        if (!st) *best = cand[pick];
     }
     ctx->prof = prof;
     cudaEventDestroy(a);
@@ -1960,7 +2185,7 @@ int plan_info(const std::vector<LGate>& prog, uint32_t nbits, int32_t precision,
             continue;
         }
         const int tb = (int)pp.hdr.tbits;
-        plan_segments(pp, std::min(std::max(tb - 9, std::min<int>(rb, tb)), maxrb));
+        plan_segments(pp, std::min(std::max(tb - 9, std::min<int>(rb, tb)), maxrb), precision == YAO_C64);
         if (precision == YAO_C64 && mode == YAO_MODE_FUSED) tc_prepare(pp);
         info[2] += (int64_t)pp.ops.size();
         for (const TOp& op : pp.ops) {
@@ -2021,7 +2246,7 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
         for (PassPlan& pp : plans[c]) {
             if (pp.single) bad[c] = 1;
             else if (pp.hdr.tbits - pp.hdr.m > kMaxScatterBits) bad[c] = 2;
-            else plan_segments(pp, rb);
+            else plan_segments(pp, rb, sizeof(V) == 8);
         }
     };
     {
