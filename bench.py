@@ -594,8 +594,9 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
     t_tiled = timed(lambda: Y.apply_inplace(whole, ref, Y.MODE_TILED))
     out["s_per_circuit_tiled"] = t_tiled
     forms = {}
-    for name, prec, k in (("fused_f64_k5", Y.C128, 5), ("fused_c64_k5", Y.C64, 5), ("fused_c64_k4", Y.C64, 4),
-                          ("fused_c64_auto", Y.C64, 0), ("fused_f64_auto", Y.C128, 0)):
+    for name, prec, k in (("fused_f64_k5", Y.C128, 5), ("fused_f64_k4", Y.C128, 4), ("fused_c64_k5", Y.C64, 5),
+                          ("fused_c64_k4", Y.C64, 4), ("fused_c64_k3", Y.C64, 3), ("fused_c64_auto", Y.C64, 0),
+                          ("fused_f64_auto", Y.C128, 0)):
         r = Y.ArrayReg.zero_state(n, prec, device=dev)
         chosen[name] = Y.autotune(whole, r, Y.MODE_FUSED, k)
         Y.apply_inplace(circuits[0], r, Y.MODE_FUSED, k)
@@ -667,11 +668,18 @@ def summary(x, plain_s, first_gates):
         return sig(s)
     L = s["layered30"]
     L["tiled_s"] = x["s_per_circuit_tiled"]
-    L["fused"] = {k: [v["s_per_circuit"], v["one_minus_fidelity"], v["max_abs_err"]] for k, v in x["fused"].items()}
+    L["fused"] = {k.replace("fused_", ""): [sig(v["s_per_circuit"], 3), sig(v["one_minus_fidelity"], 2)]
+                  for k, v in x["fused"].items()}
     L["autotuned"] = {k: [c["k"], c["tile_bits"], c["reg_bits"]] for k, c in x["autotuned"].items()
                       if k in ("tiled", "fused_c64_auto", "fused_f64_auto")}
-    L["c64_auto_speedup_vs_plain"] = plain_s / x["fused"]["fused_c64_auto"]["s_per_circuit"]
-    L["c128_auto_speedup_vs_plain"] = plain_s / x["fused"]["fused_f64_auto"]["s_per_circuit"]
+    fs = {k: v["s_per_circuit"] for k, v in x["fused"].items()}
+    L["c64_auto_speedup_vs_plain"] = plain_s / fs["fused_c64_auto"]
+    L["c128_auto_speedup_vs_plain"] = plain_s / fs["fused_f64_auto"]
+    L["c64_auto_over_c128_auto"] = fs["fused_c64_auto"] / fs["fused_f64_auto"]
+    # the autotuner's choice against the best fixed width (1.0 = as good)
+    L["auto_over_best_fixed"] = {
+        "c64": fs["fused_c64_auto"] / min(v for k, v in fs.items() if k.startswith("fused_c64_k")),
+        "c128": fs["fused_f64_auto"] / min(v for k, v in fs.items() if k.startswith("fused_f64_k"))}
     v = x["vqe"]
     s["vqe24"] = {k: v[k] for k in ("grads_per_s", "fd_max_rel_err", "oracle_energy_diff", "oracle_max_abs_grad_diff",
                                     "cpu_oracle_s_per_grad")}

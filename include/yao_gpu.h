@@ -321,6 +321,47 @@ int yao_expect_grad_batch(const yao_term* terms, size_t nterms, const yao_circui
                           const double* params, size_t nsets, const yao_reg* psi0,
                           double* values, double* grads);
 
+/* ------------------------------------------------------- tensor networks */
+/* A tensor network: tensors with labelled legs (row-major data, first leg
+ * slowest, interleaved complex), a size per label, output labels. */
+typedef struct yao_tn yao_tn;
+
+/* Network builders of src/einsum.rs. */
+enum yao_tn_kind {
+    YAO_TN_EINSUM = 0,         /* circuit_to_einsum (src/einsum.rs:34-119): input legs 0..n-1 open */
+    YAO_TN_BOUNDARY = 1,       /* circuit_to_einsum_with_boundary (:151-252): |0> inputs, `pinned` outputs <0| */
+    YAO_TN_OVERLAP = 2,        /* circuit_to_overlap (:127-131): <0|U|0> */
+    YAO_TN_EXPECTATION = 3,    /* circuit_to_expectation (:274-500): <0|U^dagger O U|0>, single-term O */
+    YAO_TN_DM = 4,             /* circuit_to_einsum_dm (:519-665): ket labels 1..n, bra labels negative */
+    YAO_TN_EXPECTATION_DM = 5  /* circuit_to_expectation_dm (:673-761): tr(O rho), single-term O */
+};
+/* The network of a circuit (kind: enum yao_tn_kind).  `pinned` is used by
+ * YAO_TN_BOUNDARY, `terms` (exactly one term, or none for the zero
+ * operator) by the expectation kinds. */
+int yao_tn_from_circuit(const yao_circuit* c, int32_t kind, const uint32_t* pinned, uint32_t npinned,
+                        const yao_term* terms, size_t nterms, yao_tn** out);
+/* A network from arrays (TensorNetwork { code, tensors, size_dict },
+ * src/einsum.rs:16-21): tensor t has ranks[t] legs, its labels next in
+ * `labels` and its data next in `data` (2 doubles per element, nelems
+ * elements over all tensors); the sizes are label_dims[i] for label_ids[i]. */
+int yao_tn_create(size_t ntensors, const uint32_t* ranks, const int64_t* labels, const double* data, size_t nelems,
+                  size_t nlabels, const int64_t* label_ids, const uint32_t* label_dims, uint32_t nout,
+                  const int64_t* out_labels, yao_tn** out);
+void yao_tn_free(yao_tn* tn);
+/* Sizes of the arrays yao_tn_export fills: tensors, legs over all tensors,
+ * elements over all tensors, output labels, labels with a size. */
+int yao_tn_counts(const yao_tn* tn, size_t* ntensors, size_t* nlegs, size_t* nelems, uint32_t* nout,
+                  size_t* nlabels);
+int yao_tn_export(const yao_tn* tn, uint32_t* ranks, int64_t* labels, double* data, int64_t* out_labels,
+                  int64_t* label_ids, uint32_t* label_dims);
+/* Elements of the contraction result (product of the output legs' sizes). */
+int yao_tn_output_len(const yao_tn* tn, size_t* out);
+/* Contracts the network on the context's GPU (src/contractor.rs contract,
+ * src/torch_contractor.rs:33 contract on Device::Cuda): pairwise in a greedy
+ * order, complex128; `out` receives the result, legs in the order of the
+ * output labels, row-major (2 * out_len doubles). */
+int yao_tn_contract(yao_ctx* ctx, const yao_tn* tn, double* out, size_t out_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -3,8 +3,8 @@
     python tests/golden/make_golden.py --ref PATH_TO_YAO_RS
 
 1. Copies yao-rs's committed golden vectors (tests/data/{instruct,apply,
-   measure,gates,noise}.json, generated by yao-rs from Yao.jl) as compact
-   JSON.  The tensor-network file (einsum.json) is not on this path.
+   measure,gates,noise,einsum}.json, generated by yao-rs from Yao.jl) as
+   compact JSON.
 2. Runs yao-rs's own numpy simulator (scripts/reference_simulate.py, which
    supports H, X, Y, Z, Rx, Ry, Rz, Phase and SWAP with controls) on seeded
    random circuits and stores the final states as pysim.json.
@@ -26,7 +26,7 @@ HERE = Path(__file__).resolve().parent
 
 
 def copy_reference_data(ref: Path):
-    for name in ["instruct", "apply", "measure", "gates", "noise"]:
+    for name in ["instruct", "apply", "measure", "gates", "noise", "einsum"]:
         data = json.loads((ref / "tests" / "data" / f"{name}.json").read_text())
         (HERE / f"{name}.json").write_text(json.dumps(data, separators=(",", ":")))
 

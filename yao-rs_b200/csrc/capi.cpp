@@ -14,13 +14,6 @@
 
 #include "yao_internal.h"
 
-// The opaque handle types of the C ABI; every object is created as one of
-// these, so the casts between the handle and its base type are valid.
-struct yao_ctx : yao::Ctx {};
-struct yao_circuit : yao::Circuit {};
-struct yao_reg : yao::Reg {};
-struct yao_dm : yao::DM {};
-
 namespace yao {
 
 // ------------------------------------------------------------------ errors
@@ -545,26 +538,11 @@ int yao_noise_superop(const yao_element* ch, double* out, uint32_t* dim2) {
     Element el;
     int s = read_element(*ch, el);
     if (s) return s;
-    std::vector<Cx> k;
-    uint32_t nk, d;
-    s = channel_kraus(el.ch, k, nk, d);
+    std::vector<Cx> S;
+    uint32_t d2;
+    s = channel_superop(el.ch, S, d2);
     if (s) return s;
-    uint32_t d2 = d * d;
-    Cx* S = (Cx*)out;
-    for (uint32_t i = 0; i < d2 * d2; i++) S[i] = Cx{0, 0};
-    for (uint32_t q = 0; q < nk; q++) {
-        const Cx* K = k.data() + (size_t)q * d * d;
-        for (uint32_t i = 0; i < d; i++)
-            for (uint32_t j = 0; j < d; j++)
-                for (uint32_t kr = 0; kr < d; kr++)
-                    for (uint32_t kc = 0; kc < d; kc++) {
-                        Cx kcj = Cx{K[i * d + j].re, -K[i * d + j].im};
-                        Cx p = cxmul(kcj, K[kr * d + kc]);
-                        Cx& t = S[(i * d + kr) * d2 + j * d + kc];
-                        t.re += p.re;
-                        t.im += p.im;
-                    }
-    }
+    memcpy(out, S.data(), S.size() * sizeof(Cx));
     *dim2 = d2;
     return YAO_OK;
 }

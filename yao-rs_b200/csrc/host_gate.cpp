@@ -525,3 +525,31 @@ void lower_gate(const GateElem& ge, uint32_t nbits, uint32_t shift, bool conj, s
 }
 
 }  // namespace yao
+
+namespace yao {
+
+// NoiseChannel::superop (src/noise.rs:359-379): S = sum_K kron(conj(K), K),
+// S[(i d + kr), (j d + kc)] += conj(K[i][j]) K[kr][kc], in that loop order.
+int channel_superop(const ChannelElem& c, std::vector<Cx>& S, uint32_t& d2) {
+    std::vector<Cx> k;
+    uint32_t nk, d;
+    const int s = channel_kraus(c, k, nk, d);
+    if (s) return s;
+    d2 = d * d;
+    S.assign((size_t)d2 * d2, Cx{0, 0});
+    for (uint32_t q = 0; q < nk; q++) {
+        const Cx* K = k.data() + (size_t)q * d * d;
+        for (uint32_t i = 0; i < d; i++)
+            for (uint32_t j = 0; j < d; j++)
+                for (uint32_t kr = 0; kr < d; kr++)
+                    for (uint32_t kc = 0; kc < d; kc++) {
+                        const Cx a{K[i * d + j].re, -K[i * d + j].im}, b = K[kr * d + kc];
+                        Cx& t = S[(size_t)(i * d + kr) * d2 + j * d + kc];
+                        t.re += a.re * b.re - a.im * b.im;
+                        t.im += a.re * b.im + a.im * b.re;
+                    }
+    }
+    return YAO_OK;
+}
+
+}  // namespace yao

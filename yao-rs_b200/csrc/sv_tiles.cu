@@ -54,6 +54,8 @@ struct TileHdr {
     int32_t use_tma; // tiles move by TMA (tma, nstage); else by cp.async
     int32_t nstage;  // TMA tile buffers in flight (2..3)
     int32_t tc_variant;  // tensor-core block variant bits (kTcVar*)
+    int32_t tc_resident; // tensor-core ops whose B operands stay in shared memory for the pass (0: one slot, reloaded)
+    int32_t pad2_;
     TmaPlan tma;
 };
 
@@ -307,7 +309,8 @@ constexpr int kTcN = 64;                // real outputs = MMA N
 constexpr int kTcKr = 64;               // real inputs = reduction length
 constexpr int kTcOpFloats = 3 * kTcN * kTcKr;  // Bh, Bl, then Bll (B - Bh - Bl rounded to TF32)
 constexpr uint32_t kTcSbo = (kTcKr / 4) * 128;  // bytes between 8-row groups
-constexpr size_t kTcSmemBytes = 2 * (size_t)kTcRows * kTcKr * 4 + 3 * (size_t)kTcN * kTcKr * 4;  // Xh, Xl, Bh, Bl, Bll
+constexpr size_t kTcXBytes = 2 * (size_t)kTcRows * kTcKr * 4;  // Xh, Xl
+constexpr size_t kTcBPart = (size_t)kTcN * kTcKr * 4;            // one of Bh, Bl, Bll
 constexpr int kTcCols = 128;  // tensor-memory columns: the main accumulator, then the correction accumulator
 // Variants of the tensor-core block (hdr.tc_variant bits, from YAO_TC_VARIANT):
 //   1: X's low part rounded to TF32 (round to nearest) before the MMAs read it
@@ -335,6 +338,8 @@ struct TcCtx {
     float* bl;
     float* bll;
     int variant;         // kTcVar* bits
+    int resident;        // B operands of every op resident (slot = op.mma / kTcOpFloats)
+    uint32_t bfloats;    // floats of one op's B operands in shared memory
     const float* mmat;   // every tensor-core op's Bh, Bl, Bll of the pass (global)
     int loaded;          // op offset whose B operands are in shared memory
     int failed;          // a completion wait ran out (results of the pass are void)
@@ -356,11 +361,12 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
         // B operands of this op (Bh, Bl[, Bll]: 32 or 48 KiB contiguous): one
         // bulk copy started now, waited for by the MMA-issuing thread
         const bool split = tc.variant & kTcVarSplitAcc, b3 = tc.variant & kTcVarB3;
-        const uint32_t bbytes = (b3 ? 3u : 2u) * kTcN * kTcKr * 4;
-        const bool need_b = tc.loaded != op.mma;
+        const uint32_t bbytes = tc.bfloats * 4;
+        float* bslot = tc.resident ? tc.bh + (size_t)(op.mma / kTcOpFloats) * tc.bfloats : tc.bh;
+        const bool need_b = !tc.resident && tc.loaded != op.mma;
         if (need_b && tid == 0 && !tc.stall) {
             tc::mbar_arrive_expect_tx(tc.bbar, bbytes);
-            tc::bulk_g2s(tc.bh, tc.mmat + op.mma, bbytes, tc.bbar);
+            tc::bulk_g2s(bslot, tc.mmat + op.mma, bbytes, tc.bbar);
         }
         if (tid < (1u << kTcK)) {
             uint32_t o = 0;
@@ -397,7 +403,7 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
         bool b_ok = true;
         constexpr uint32_t idesc = tc::idesc_tf32(kTcRows, kTcN);
         const uint32_t xh = tc::smem_u32(tc.xh), xl = tc::smem_u32(tc.xl);
-        const uint32_t bh = tc::smem_u32(tc.bh), bl = tc::smem_u32(tc.bl), bll = tc::smem_u32(tc.bll);
+        const uint32_t bh = tc::smem_u32(bslot), bl = bh + (uint32_t)kTcBPart, bll = bl + (uint32_t)kTcBPart;
         const uint32_t acc_c = tc.tmem + (split ? (uint32_t)kTcN : 0u);  // correction accumulator
         auto issue = [&](int k0) {
             tc::fence_after_sync();
@@ -888,6 +894,8 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         tcx.bl = tcx.bh + kTcN * kTcKr;
         tcx.bll = tcx.bl + kTcN * kTcKr;
         tcx.variant = hdr.tc_variant;
+        tcx.resident = hdr.tc_resident > 0;
+        tcx.bfloats = (hdr.tc_variant & kTcVarB3 ? 3u : 2u) * kTcN * kTcKr;
         tcx.mmat = mmat;
         tcx.loaded = -1;
         tcx.failed = 0;
@@ -910,6 +918,25 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         __syncthreads();
         tc::fence_after_sync();
         tcx.tmem = tc_tmem;
+        if (tcx.resident) {
+            // every op's B operands in their slots, once for the whole pass
+            // (thread 0 issues the MMAs: it alone waits, bounded)
+            if (threadIdx.x == 0) {
+                tc::mbar_arrive_expect_tx(tcx.bbar, (uint32_t)hdr.tc_resident * tcx.bfloats * 4);
+                for (int j = 0; j < hdr.tc_resident; j++)
+                    tc::bulk_g2s(tcx.bh + (size_t)j * tcx.bfloats, mmat + (size_t)j * kTcOpFloats, tcx.bfloats * 4,
+                                 tcx.bbar);
+                const uint64_t t0 = global_ns_tc();
+                bool ok;
+                while (!(ok = tc::mbar_try_wait(tcx.bbar, 0)))
+                    if (global_ns_tc() - t0 > tcx.wait_ns) break;
+                if (!ok) {
+                    tcx.failed = 1;
+                    atomicExch(err, 1);
+                }
+            }
+            tcx.loaded = -2;
+        }
     }
     const uint32_t T = 1u << hdr.tbits;
     const uint32_t tile_bytes = T * (uint32_t)sizeof(V);
@@ -994,6 +1021,8 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
             }
             while (tcx.loaded >= 0 && !tc::mbar_try_wait(tcx.bbar, tcx.bphase ^ 1u) &&
                    global_ns_tc() - t0 < 2 * tcx.wait_ns) {
+            }
+            while (tcx.resident && !tc::mbar_try_wait(tcx.bbar, 0) && global_ns_tc() - t0 < 3 * tcx.wait_ns) {
             }
         }
         tc::fence_before_sync();
@@ -1780,20 +1809,31 @@ static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
     static int optin = 0;
     if (!optin) YAO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
     const size_t budget = (size_t)optin - 16 * 1024 - 1024;
-    const size_t tcb = hdr.mma ? 1024 + kTcSmemBytes : 0;
-    hdr.staged = 2 * tile_bytes + tcb + stg <= budget ? 1 : 0;
-    hdr.nstage = 2;
-    if (hdr.use_tma && 3 * tile_bytes + tcb + (hdr.staged ? stg : 0) <= budget) hdr.nstage = 3;
-    hdr.dmma = dm ? 1 : 0;
-    // YAO_TEST_TC_STALL=1 (failure-path test): the tensor-core ops issue
-    // neither their operand copy nor their MMAs, so both bounded waits of
-    // each op run out (0.1 s each) and the call reports YAO_ERR_TIMEOUT
+    // tensor-core passes: X operands and the B operand slots; every op's B
+    // stays resident for the pass when the slots fit beside two tiles,
+    // else one slot is reloaded per op and tile
+    size_t bslot = 0;
+    int ntc = 0;
     if (hdr.mma) {
+        // YAO_TEST_TC_STALL=1 (failure-path test): the tensor-core ops issue
+        // neither their operand copy nor their MMAs, so both bounded waits of
+        // each op run out (0.1 s each) and the call reports YAO_ERR_TIMEOUT
         if (const char* e = getenv("YAO_TEST_TC_STALL")) hdr.tc_test = e[0] == '1';
         hdr.tc_variant = tc_variant();
+        bslot = (hdr.tc_variant & kTcVarB3 ? 3 : 2) * kTcBPart;
+        for (const TOp& op : ops) ntc += op.mma >= 0;
     }
+    auto tcb = [&](int slots) { return hdr.mma ? 1024 + kTcXBytes + (size_t)slots * bslot : 0; };
+    const char* re = getenv("YAO_TC_RESIDENT");
+    const bool allow_res = !(re && re[0] == '0');
+    hdr.tc_resident = hdr.mma && !hdr.tc_test && allow_res && 2 * tile_bytes + tcb(ntc) + stg <= budget ? ntc : 0;
+    const int slots = hdr.tc_resident ? ntc : 1;
+    hdr.staged = 2 * tile_bytes + tcb(slots) + stg <= budget ? 1 : 0;
+    hdr.nstage = 2;
+    if (hdr.use_tma && 3 * tile_bytes + tcb(slots) + (hdr.staged ? stg : 0) <= budget) hdr.nstage = 3;
+    hdr.dmma = dm ? 1 : 0;
     size_t smem = (size_t)(hdr.use_tma ? hdr.nstage : 1) * tile_bytes + (hdr.staged ? stg : 0);
-    if (hdr.mma) smem = ((smem + 1023) & ~(size_t)1023) + kTcSmemBytes;
+    if (hdr.mma) smem = ((smem + 1023) & ~(size_t)1023) + kTcXBytes + (size_t)slots * bslot;
     smem += 1024;
     const TOp* dops = (const TOp*)dbuf;
     const TSeg* dsegs = (const TSeg*)((char*)dbuf + sb_off);

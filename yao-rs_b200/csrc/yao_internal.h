@@ -96,6 +96,7 @@ void gate_matrix(const GateElem& g, std::vector<Cx>& m, uint32_t& dim, bool& dia
 GateElem gate_dagger(const GateElem& g);
 void gate_generator(const GateElem& g, int i, std::vector<Cx>& m, uint32_t& dim);
 int channel_kraus(const ChannelElem& ch, std::vector<Cx>& kraus, uint32_t& nkraus, uint32_t& dim);
+int channel_superop(const ChannelElem& ch, std::vector<Cx>& S, uint32_t& d2);
 bool matrix_is_diagonal(const Cx* m, uint32_t d);
 
 // Lower one gate on an nbits-qubit register with location offset `shift`
@@ -260,3 +261,10 @@ int reduce_dm_marginal(Ctx* ctx, const DM* d, const uint32_t* bits, int32_t nl, 
 int launch_dm_partial_tr(Ctx* ctx, const DM* d, const uint32_t* traced, uint32_t nt, DM* out);
 
 }  // namespace yao
+
+// The opaque handle types of the C ABI; every object is created as one of
+// these, so the casts between the handle and its base type are valid.
+struct yao_ctx : yao::Ctx {};
+struct yao_circuit : yao::Circuit {};
+struct yao_reg : yao::Reg {};
+struct yao_dm : yao::DM {};

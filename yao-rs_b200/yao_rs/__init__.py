@@ -5,7 +5,7 @@ Circuits, gates, noise channels and operators are host values; registers
 and density matrices live in GPU memory.  Every compute call goes through
 the C ABI of include/yao_gpu.h; there is no CPU fallback.
 """
-from . import _abi
+from . import _abi, einsum
 from ._abi import (C64, C128, MODE_FUSED, MODE_PLAIN, MODE_TILED, CircuitError, YaoError, context,
                    launch_count)
 from .circuit import (Circuit, PositionedAnnotation, PositionedChannel, PositionedGate, channel, control,
@@ -15,6 +15,8 @@ from .noise import NoiseChannel
 from .operator import Op, OperatorPolynomial, OperatorString, op_matrix
 from .ops import (MeasureResult, PostProcess, apply, apply_inplace, autotune, batch_apply, expect_arrayreg, expect_dm, expect_grad_batch,
                   expect_grad, measure_with_postprocess, plan_info, probs)
+from .einsum import (TensorNetwork, circuit_to_einsum, circuit_to_einsum_dm, circuit_to_einsum_with_boundary,
+                     circuit_to_expectation, circuit_to_expectation_dm, circuit_to_overlap)
 from .register import ArrayReg, DensityMatrix, Register, density_matrix_from_reg
 
 __all__ = [
@@ -23,5 +25,7 @@ __all__ = [
     "PositionedAnnotation", "PositionedChannel", "PositionedGate", "PostProcess", "Register", "YaoError",
     "apply", "apply_inplace", "autotune", "batch_apply", "channel", "context", "control", "density_matrix_from_reg",
     "elements_array", "expect_arrayreg", "expect_dm", "expect_grad", "expect_grad_batch", "label", "launch_count",
-    "measure_with_postprocess", "op_matrix", "plan_info", "probs", "put",
+    "measure_with_postprocess", "op_matrix", "plan_info", "probs", "put", "TensorNetwork", "circuit_to_einsum",
+    "circuit_to_einsum_dm", "circuit_to_einsum_with_boundary", "circuit_to_expectation", "circuit_to_expectation_dm",
+    "circuit_to_overlap", "einsum",
 ]

@@ -150,7 +150,19 @@ SIGNATURES = {
                                                C.POINTER(C.c_uint8), pp]),
     "yao_batch_apply": (C.c_int, [pp, pp, sz, i32, i32]),
     "yao_expect_grad_batch": (C.c_int, [C.POINTER(yao_term), sz, vp, dptr, sz, vp, dptr, dptr]),
+    "yao_tn_from_circuit": (C.c_int, [vp, i32, u32p, u32, C.POINTER(yao_term), sz, pp]),
+    "yao_tn_create": (C.c_int, [sz, u32p, C.POINTER(C.c_int64), dptr, sz, sz, C.POINTER(C.c_int64), u32p, u32,
+                                C.POINTER(C.c_int64), pp]),
+    "yao_tn_free": (None, [vp]),
+    "yao_tn_counts": (C.c_int, [vp, C.POINTER(sz), C.POINTER(sz), C.POINTER(sz), u32p, C.POINTER(sz)]),
+    "yao_tn_export": (C.c_int, [vp, u32p, C.POINTER(C.c_int64), dptr, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                u32p]),
+    "yao_tn_output_len": (C.c_int, [vp, C.POINTER(sz)]),
+    "yao_tn_contract": (C.c_int, [vp, vp, dptr, sz]),
 }
+
+# enum yao_tn_kind
+TN_EINSUM, TN_BOUNDARY, TN_OVERLAP, TN_EXPECTATION, TN_DM, TN_EXPECTATION_DM = range(6)
 
 _lib = None
 _lock = threading.Lock()
