@@ -292,7 +292,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--profile-case", default=None,
                     choices=["plain", "tiled", "fused64", "fused32", "fused32_tc", "pass1q", "fused64_dmma",
-                             "fused64_cuda", "vqe", "grad24", "dm", "batch", "vqe_batch", "tc_drift"],
+                             "fused64_cuda", "vqe", "grad24", "dm", "dm_channel", "batch", "vqe_batch", "tc_drift"],
                     help="run one small case of a kernel family (for ncu captures) and exit")
     args = ap.parse_args()
     if args.profile_case:
@@ -492,6 +492,11 @@ def profile_case(args):
         c = Y.Circuit.qubits(n, [el for l in range(8) for el in layer_elements(Y, n, l)])
         r = Y.ArrayReg.zero_state(n, Y.C128)
         Y.apply_inplace(c, r, Y.MODE_FUSED, 4)
+    elif args.profile_case == "dm_channel":
+        # one noisy layer at n = 12 (PLAIN): gate and channel passes, the
+        # 2-qubit depolarizing channels through the register kernel
+        d = Y.DensityMatrix.zero_state(12)
+        d.apply(noisy_dm_circuit(Y, 12, 1))
     elif args.profile_case == "dm":
         nd = 12
         els = []
@@ -520,9 +525,9 @@ def tc_drift(Y, A, n):
     """Complex64 FUSED k = 5 on the layered circuit (40 layers) without the
     FP64 norm restore: the norm drift per tensor-core block, 1 - F and max
     |error| against the FP64 PLAIN result, for every tensor-core variant
-    (YAO_TC_VARIANT bits: 1 X low part rounded, 2 separate correction
-    accumulator, 4 three-part B) and for the CUDA-core split form; one JSON
-    line per form."""
+    (YAO_TC_VARIANT bits: 2 separate correction accumulator, 8 the integer
+    form with exact int32 accumulation) and for the CUDA-core split form; one
+    JSON line per form."""
     import torch
     os.environ.update(YAO_TILE_BITS="12", YAO_REG_BITS="3", YAO_AUTOTUNE="0", YAO_NORM_RESTORE="0")
     c = Y.Circuit.qubits(n, [el for l in range(LAYERS) for el in layer_elements(Y, n, l)])
@@ -530,7 +535,7 @@ def tc_drift(Y, A, n):
     Y.apply_inplace(c, ref)
     info = Y.plan_info(c, Y.C64, Y.MODE_FUSED, 5, 12, 3)
     stream = torch.cuda.ExternalStream(A.stream_ptr(0), device=torch.device("cuda", 0))
-    forms = [("tc_v%d" % v, "1", str(v)) for v in range(8)] + [("cuda_core", "0", "0")]
+    forms = [("tc_v%d" % v, "1", str(v)) for v in (0, 2, 8)] + [("cuda_core", "0", "0")]
     for name, tc, var in forms:
         os.environ.update(YAO_TC=tc, YAO_TC_VARIANT=var)
         r = Y.ArrayReg.zero_state(n, Y.C64)
@@ -655,7 +660,33 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
         del d
     out["noisy_dm14"]["n12_layer_vs_oracle"] = {"max_abs_diff": d12, "cpu_oracle_s": bg_dm.s}
     out["batched_circuits"] = batch_extra(Y, A, torch, stream, dev, timed)
+    out["tn20"] = tn_extra(Y, A, dev)
     return out
+
+
+def tn_extra(Y, A, dev):
+    """The tensor network of the layered circuit at n = 20 (4 layers, |0>
+    inputs, open outputs: circuit_to_einsum_with_boundary) contracted on the
+    GPU (pairwise, greedy order), against the PLAIN state vector; the
+    oracle's numpy contraction of the same network timed beside it."""
+    n, layers = 20, 4
+    c = Y.Circuit.qubits(n, [el for l in range(layers) for el in layer_elements(Y, n, l)])
+    net = Y.circuit_to_einsum_with_boundary(c)
+    Y.einsum.contract(net)  # warm-up
+    t0 = time.perf_counter()
+    out = Y.einsum.contract(net).reshape(-1)
+    t_gpu = time.perf_counter() - t0
+    r = Y.ArrayReg.zero_state(n, device=dev)
+    Y.apply_inplace(c, r)
+    diff = float(np.max(np.abs(out - r.state_vec())))
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import tn as OT
+    ref = {"ixs": net.ixs, "iy": net.iy, "tensors": net.tensors, "size": net.size_dict}
+    t0 = time.perf_counter()
+    OT.contract(ref)
+    t_cpu = time.perf_counter() - t0
+    return {"qubits": n, "tensors": len(net.tensors), "s_gpu": t_gpu, "s_cpu_numpy": t_cpu,
+            "max_abs_diff_vs_state_vector": diff}
 
 
 def summary(x, plain_s, first_gates):
@@ -700,6 +731,9 @@ def summary(x, plain_s, first_gates):
     q = x["qft20"]
     s["qft20"] = {k: q[k] for k in ("s_per_circuit_plain", "s_per_circuit_tiled", "cpu_s_per_circuit",
                                     "max_abs_diff_vs_oracle")}
+    t = x.get("tn20")
+    if t:
+        s["tn20"] = {k: t[k] for k in ("s_gpu", "s_cpu_numpy", "max_abs_diff_vs_state_vector")}
     return sig(s, 4)
 
 

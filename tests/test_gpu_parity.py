@@ -661,6 +661,30 @@ def test_tensor_core_bounded_waits_report_timeout(monkeypatch):
     assert 1 - abs(np.vdot(ref, out)) ** 2 < 1e-6
 
 
+@pytest.mark.parametrize("n", [12, 16])
+def test_integer_tensor_core_blocks_keep_the_norm(monkeypatch, n):
+    """The integer form of the complex64 tensor-core blocks (exact int8
+    products summed in int32, every rounding to nearest) on the layered
+    circuit, without the FP64 norm restore: 1 - F <= 1e-9 against the
+    oracle and a norm drift below 1e-10 per block, where the FP32-accumulating
+    form shrinks the norm by about 8e-7 per block."""
+    c = layered_circuit(n, 12, seed=n)
+    psi = random_state(np.random.default_rng(900 + n), n)
+    ref = O.apply_circuit(c, psi)
+    monkeypatch.setenv("YAO_TILE_BITS", "12")
+    monkeypatch.setenv("YAO_REG_BITS", "3")
+    monkeypatch.setenv("YAO_AUTOTUNE", "0")
+    monkeypatch.setenv("YAO_NORM_RESTORE", "0")
+    monkeypatch.setenv("YAO_TC_VARIANT", "8")
+    blocks = Y.plan_info(c, Y.C64, Y.MODE_FUSED, 5, 12, 3)["tensor_core_ops"]
+    assert blocks >= 4
+    r = Y.ArrayReg.from_vec(n, psi).to_precision(Y.C64)
+    Y.apply_inplace(c, r, Y.MODE_FUSED, 5)
+    out = r.state_vec().astype(np.complex128)
+    assert 1 - abs(np.vdot(ref, out)) ** 2 <= 1e-9
+    assert abs(np.vdot(out, out).real - 1.0) / blocks < 1e-10
+
+
 @pytest.mark.parametrize("n,k", [(13, 5), (16, 5), (14, 4), (15, 3)])
 def test_tensor_core_blocks(monkeypatch, n, k):
     """Dense 3..5-qubit blocks of complex64 FUSED runs on the tensor cores

@@ -33,8 +33,8 @@ namespace yao {
 constexpr int kAdjThreads = 512;
 constexpr int kAdjLowBits = 4;      // contiguous low bits of every tile (256-byte runs)
 constexpr int kAdjScatter = 7;      // scattered tile bits at most
-constexpr int kAdjMaxOps = 96;      // reverse-sweep ops per pass
-constexpr int kAdjMaxSlots = 64;    // generator dots per pass
+constexpr int kAdjMaxOps = 64;      // reverse-sweep ops per pass
+constexpr int kAdjMaxSlots = 48;    // generator dots per pass
 
 // A run of uncontrolled 1-qubit reverse-sweep steps on one target bit,
 // folded on the host into one op (cls kAdjFused): with A the product of the
@@ -102,8 +102,9 @@ __device__ __forceinline__ double redot(double2 l, double2 y) { return fma(l.x, 
 constexpr int kAdjRun = 8;
 
 template <int K>
-__device__ __forceinline__ void adj_run(const AdjTileOp* rops, int nr, uint64_t base, double2* sp, double2* sl,
-                                        uint32_t T, double* acc, uint32_t nw) {
+__device__ __forceinline__ void adj_run(const AdjTileOp* __restrict__ rops, int nr, uint64_t base,
+                                        double2* __restrict__ sp, double2* __restrict__ sl, uint32_t T,
+                                        double* __restrict__ acc, uint32_t nw) {
     constexpr int NL = 1 << K;
     const uint32_t ngroups = T >> K;
     const int p0 = rops[0].tl[0], p1 = K == 2 ? rops[0].tl[1] : 0;
@@ -199,11 +200,31 @@ __device__ __forceinline__ void adj_run(const AdjTileOp* rops, int nr, uint64_t 
         }
 }
 
+// A run of one X step (the CNOTs of the sweep: X on one target under
+// controls): the pairs whose controls match swap in psi and lambda.
+__device__ __forceinline__ void adj_x1(const AdjTileOp& op, uint64_t base, double2* __restrict__ sp,
+                                       double2* __restrict__ sl, uint32_t T) {
+    if ((base & op.gcmask) != op.gcval) return;  // uniform over the tile
+    const int p = op.tl[0];
+    const uint32_t cm = op.lcmask, cv = op.lcval;
+    const uint32_t ngroups = T >> 1;
+    for (uint32_t g = threadIdx.x; g < ngroups; g += blockDim.x) {
+        const uint32_t b = adj_ins0(g, p);
+        if ((b & cm) != cv) continue;
+        const uint32_t i0 = adj_swz(b), i1 = adj_swz(b | (1u << p));
+        const double2 x0 = sp[i0], x1 = sp[i1], l0 = sl[i0], l1 = sl[i1];
+        sp[i0] = x1;
+        sp[i1] = x0;
+        sl[i0] = l1;
+        sl[i1] = l0;
+    }
+}
+
 // A fused run (kAdjFused) on the groups of the tile owned by this thread:
 // coefficients in registers, every group read once, P = conj(lambda_r) psi_c
 // formed once for all the run's dots, A applied once.
-__device__ __forceinline__ void adj_fused1(const AdjTileOp& op, double2* sp, double2* sl, uint32_t T, double* acc,
-                                           uint32_t nw) {
+__device__ __forceinline__ void adj_fused1(const AdjTileOp& op, double2* __restrict__ sp, double2* __restrict__ sl,
+                                           uint32_t T, double* __restrict__ acc, uint32_t nw) {
     const uint32_t ngroups = T >> 1;
     const int p = op.tl[0];
     const int ng = op.ngen;
@@ -254,7 +275,7 @@ __device__ __forceinline__ void adj_fused1(const AdjTileOp& op, double2* sp, dou
 }
 
 constexpr uint64_t kAdjWaitNs = 1000000000ull;  // 1 s
-constexpr int kAdjMaxStages = 2;
+constexpr int kAdjMaxStages = 3;
 
 __device__ __forceinline__ uint64_t adj_ns() {
     uint64_t t;
@@ -317,10 +338,11 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
         tma::prefetch_map(&mpsi);
         tma::prefetch_map(&mlam);
         for (int q = 0; q < nbuf; q++) tc::mbar_init(&full_bar[q], 1);
-        if (blockIdx.x < hdr.ntiles) {
-            issue(blockIdx.x, 0);
-            pending |= 1u;
-        }
+        for (int q = 0; q < (nbuf > 2 ? nbuf - 1 : 1); q++)
+            if (blockIdx.x + (uint64_t)q * gridDim.x < hdr.ntiles) {
+                issue(blockIdx.x + (uint64_t)q * gridDim.x, q);
+                pending |= 1u << q;
+            }
     }
     __syncthreads();
     const uint32_t lmask = (1u << nlow) - 1;
@@ -332,8 +354,8 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
         double2* sp = (double2*)(smem + (size_t)b * 2 * tile_bytes);
         double2* sl = sp + T;
         if (use_tma) {
-            if (threadIdx.x == 0 && nbuf > 1 && t + gridDim.x < hdr.ntiles) {
-                const int bn = (int)((it + 1) % (uint32_t)nbuf);
+            if (threadIdx.x == 0 && nbuf == 2 && t + gridDim.x < hdr.ntiles) {
+                const int bn = (int)((it + 1) & 1u);
                 tma::wait_group_read<0>();  // the previous tile's stores have read buffer bn
                 issue(t + gridDim.x, bn);
                 pending |= 1u << bn;
@@ -371,6 +393,8 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
             e++;
             if (ops[oi].cls == kAdjFused)
                 adj_fused1(ops[oi], sp, sl, T, acc, nw);
+            else if (e - oi == 1 && ops[oi].k == 1 && ops[oi].cls == GC_X && !ops[oi].gen)
+                adj_x1(ops[oi], base, sp, sl, T);
             else if (ops[oi].k == 1)
                 adj_run<1>(ops + oi, e - oi, base, sp, sl, T, acc, nw);
             else
@@ -390,6 +414,16 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
                     tma::wait_group_read<0>();
                     issue(t + gridDim.x, 0);
                     pending |= 1u;
+                }
+                // three buffers: the tile nbuf - 1 ahead into the buffer of
+                // the previous tile, whose stores have had this tile's
+                // compute to read it
+                const uint64_t tn = t + (uint64_t)(nbuf - 1) * gridDim.x;
+                if (nbuf > 2 && tn < hdr.ntiles) {
+                    const int bn = (int)((it + (uint32_t)nbuf - 1) % (uint32_t)nbuf);
+                    tma::wait_group_read<1>();
+                    issue(tn, bn);
+                    pending |= 1u << bn;
                 }
             }
         } else {
@@ -704,7 +738,7 @@ int adjoint_tiles(Ctx* ctx, Reg* psi, Reg* lam, const Circuit* c, double* grad, 
     if (!optin) YAO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
     const size_t rest = kAdjMaxOps * sizeof(AdjTileOp) + (size_t)kAdjMaxSlots * (kAdjThreads / 32) * 8 + 1024;
     const size_t budget = (size_t)optin - 4096;  // static shared memory of the kernel
-    const int nstage = 2 * tile_bytes + rest <= budget ? 2 : 1;
+    const int nstage = 3 * tile_bytes + rest <= budget ? 3 : (2 * tile_bytes + rest <= budget ? 2 : 1);
     const size_t smem_max = (size_t)nstage * tile_bytes + rest;
     static bool attr = false;
     if (!attr) {

@@ -224,6 +224,7 @@ struct DMChan {
     uint32_t active[kMaxKraus];
     int32_t mono[kMaxKraus];
     int8_t perm[kMaxKraus][2][4];
+    int32_t xmask[kMaxKraus][2];  // XOR channels: row / column permutation a -> a ^ xmask
     double2 kr[kMaxKraus * 16], kc[kMaxKraus * 16];  // row / column matrices, 2^k x 2^k each
 };
 
@@ -330,6 +331,87 @@ __global__ void __launch_bounds__(kDCT, DENSE ? 1 : 4) k_dm_channel(double2* __r
     }
 }
 
+// Channels whose every Kraus operator (and its conjugate) is a permutation
+// a -> a ^ x times one coefficient per row (the Pauli products of the
+// depolarizing and Pauli channels, bit and phase flips; diagonal operators
+// with x = 0): the group stays in registers, and each operator is one of
+// NL^2 code paths with compile-time source indices (no shared-memory reads
+// of the group).  Operation per entry and operator as in k_dm_channel's
+// monomial path: acc += cmul(kc[b], cmul(kr[a], orig[a ^ xr][b ^ xc])).
+template <int K, int XR, int XC>
+__device__ __forceinline__ void xor_op(const double2 (&x)[1 << K][1 << K], double2 (&acc)[1 << K][1 << K],
+                                       const double2* mr, const double2* mc) {
+    constexpr int NL = 1 << K;
+#pragma unroll
+    for (int a = 0; a < NL; a++) {
+        const double2 cr = mr[a * NL + (a ^ XR)];
+#pragma unroll
+        for (int b = 0; b < NL; b++) {
+            const double2 y = cmul_sparse(mc[b * NL + (b ^ XC)], cmul_sparse(cr, x[a ^ XR][b ^ XC]));
+            acc[a][b] = cadd_x(acc[a][b], y);
+        }
+    }
+}
+
+template <int K, int XR>
+__device__ __forceinline__ void xor_op_c(int xc, const double2 (&x)[1 << K][1 << K], double2 (&acc)[1 << K][1 << K],
+                                         const double2* mr, const double2* mc) {
+    if constexpr (K == 1) {
+        if (xc == 0) xor_op<K, XR, 0>(x, acc, mr, mc); else xor_op<K, XR, 1>(x, acc, mr, mc);
+    } else {
+        switch (xc) {
+        case 0: xor_op<K, XR, 0>(x, acc, mr, mc); break;
+        case 1: xor_op<K, XR, 1>(x, acc, mr, mc); break;
+        case 2: xor_op<K, XR, 2>(x, acc, mr, mc); break;
+        default: xor_op<K, XR, 3>(x, acc, mr, mc); break;
+        }
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(kDCT, 2) k_dm_channel_xor(double2* __restrict__ rho, uint64_t ngroups,
+                                                            const __grid_constant__ DMChan op) {
+    constexpr int NL = 1 << K, MS = NL * NL;
+    __shared__ double2 smr[kMaxKraus * MS], smc[kMaxKraus * MS];
+    __shared__ int sx[kMaxKraus][2];
+    for (int i = threadIdx.x; i < op.nk * MS; i += blockDim.x) {
+        smr[i] = op.kr[i];
+        smc[i] = op.kc[i];
+    }
+    for (int i = threadIdx.x; i < op.nk * 2; i += blockDim.x) (&sx[0][0])[i] = (&op.xmask[0][0])[i];
+    __syncthreads();
+    GRID_STRIDE(g, ngroups) {
+        const uint64_t base = insert_zeros(g, op.locked, op.nlocked);
+        double2 x[NL][NL], acc[NL][NL];
+#pragma unroll
+        for (int a = 0; a < NL; a++)
+#pragma unroll
+            for (int b = 0; b < NL; b++) {
+                x[a][b] = rho[base + op.roff[a] + op.coff[b]];
+                acc[a][b] = make_double2(0.0, 0.0);
+            }
+        for (int q = 0; q < op.nk; q++) {
+            const double2* mr = smr + q * MS;
+            const double2* mc = smc + q * MS;
+            const int xr = sx[q][0], xc = sx[q][1];
+            if constexpr (K == 1) {
+                if (xr == 0) xor_op_c<K, 0>(xc, x, acc, mr, mc); else xor_op_c<K, 1>(xc, x, acc, mr, mc);
+            } else {
+                switch (xr) {
+                case 0: xor_op_c<K, 0>(xc, x, acc, mr, mc); break;
+                case 1: xor_op_c<K, 1>(xc, x, acc, mr, mc); break;
+                case 2: xor_op_c<K, 2>(xc, x, acc, mr, mc); break;
+                default: xor_op_c<K, 3>(xc, x, acc, mr, mc); break;
+                }
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < NL; a++)
+#pragma unroll
+            for (int b = 0; b < NL; b++) rho[base + op.roff[a] + op.coff[b]] = acc[a][b];
+    }
+}
+
 // Column of the single non-zero entry of each row of a d x d matrix (-1 for
 // a zero row); false when some row has two or more.
 static bool monomial_rows(const std::vector<Cx>& m, int d, int8_t* perm) {
@@ -382,9 +464,42 @@ int launch_dm_channel(Ctx* ctx, DM* d, const std::vector<LGate>& rows, const std
         }
         op.mono[q] = monomial_rows(rows[q].m, NL, op.perm[q][0]) && monomial_rows(cols[q].m, NL, op.perm[q][1]);
     }
+    // XOR channels: every operator a monomial whose permutation is a ^ x on
+    // rows and columns (diagonal operators: x = 0); their diagonal entries
+    // sit at m[a * NL + a] already
+    bool xr_ok = true;
+    for (int q = 0; q < nk && xr_ok; q++) {
+        if (rows[q].cls == GC_DIAG) {
+            op.xmask[q][0] = op.xmask[q][1] = 0;
+            continue;
+        }
+        if (!op.mono[q]) {
+            xr_ok = false;
+            break;
+        }
+        for (int ax = 0; ax < 2 && xr_ok; ax++) {
+            const int x0 = op.perm[q][ax][0];
+            if (x0 < 0) {
+                xr_ok = false;
+                break;
+            }
+            for (int a = 0; a < NL; a++)
+                if (op.perm[q][ax][a] != (a ^ x0)) xr_ok = false;
+            op.xmask[q][ax] = x0;
+        }
+    }
     uint64_t ngroups = (uint64_t)1 << (2 * d->nbits - op.nlocked);
     unsigned grid = grid_for(ngroups, kDT, ctx->num_sms);
     ProfScope prof(ctx, "dm_channel", (double)ngroups * (double)(1 << (2 * k)) * 32.0);
+    if (xr_ok && !(getenv("YAO_DM_XOR") && getenv("YAO_DM_XOR")[0] == '0')) {
+        if (k == 1)
+            k_dm_channel_xor<1><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);
+        else
+            k_dm_channel_xor<2><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);
+        ctx->launches++;
+        YAO_CUDA(cudaGetLastError());
+        return YAO_OK;
+    }
     bool dense = false;
     for (int q = 0; q < nk; q++) dense |= op.cls[q] != GC_DIAG && !op.mono[q];
     if (k == 1)

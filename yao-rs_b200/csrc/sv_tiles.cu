@@ -52,7 +52,7 @@ struct TileHdr {
     int32_t dmma;    // complex128 FUSED: some dense 3..5-qubit block runs on the FP64 tensor cores
     int32_t tc_test; // failure-path test: tensor-core ops issue no copy and no MMA, waits give up after 0.1 s
     int32_t use_tma; // tiles move by TMA (tma, nstage); else by cp.async
-    int32_t nstage;  // TMA tile buffers in flight (2..3)
+    int32_t nstage;  // TMA tile buffers in flight (2..4)
     int32_t tc_variant;  // tensor-core block variant bits (kTcVar*)
     int32_t tc_resident; // tensor-core ops whose B operands stay in shared memory for the pass (0: one slot, reloaded)
     int32_t pad2_;
@@ -307,7 +307,10 @@ constexpr int kTcTileBits = 12;         // tile of a tensor-core pass (2^12 comp
 constexpr int kTcRows = 128;            // groups per tile = MMA M
 constexpr int kTcN = 64;                // real outputs = MMA N
 constexpr int kTcKr = 64;               // real inputs = reduction length
-constexpr int kTcOpFloats = 3 * kTcN * kTcKr;  // Bh, Bl, then Bll (B - Bh - Bl rounded to TF32)
+// One op's operand slot (floats): Bh, Bl, Bll (B - Bh - Bl rounded to TF32),
+// then the five int8 digit arrays of the integer form (kTc8Off on)
+constexpr int kTc8Off = 3 * kTcN * kTcKr;
+constexpr int kTcOpFloats = kTc8Off + 5 * kTcN * kTcKr / 4;
 constexpr uint32_t kTcSbo = (kTcKr / 4) * 128;  // bytes between 8-row groups
 constexpr size_t kTcXBytes = 2 * (size_t)kTcRows * kTcKr * 4;  // Xh, Xl
 constexpr size_t kTcBPart = (size_t)kTcN * kTcKr * 4;            // one of Bh, Bl, Bll
@@ -317,7 +320,27 @@ constexpr int kTcCols = 128;  // tensor-memory columns: the main accumulator, th
 //   2: the correction products (Xh Bl + Xl Bh [+ Xh Bll]) accumulate apart from
 //      Xh Bh, and the two are added in FP32 (round to nearest) on read-back
 //   4: B in three TF32 parts, a fourth product Xh Bll
-constexpr int kTcVarXlRound = 1, kTcVarSplitAcc = 2, kTcVarB3 = 4;
+//   8: the integer form (wide_tc8): exact int8 products, int32 accumulation
+constexpr int kTcVarXlRound = 1, kTcVarSplitAcc = 2, kTcVarB3 = 4, kTcVarInt8 = 8;
+
+// Integer form of the tensor-core block.  The tensor cores' FP32
+// accumulation truncates (every accumulation step biases the sum toward
+// zero, so the norm shrinks block by block); integer MMAs accumulate
+// exactly.  X (the tile's amplitudes) is scaled by a power of two 2^(20 - e)
+// with 2^e above the tile's largest |x| and rounded to the nearest integer
+// (|q| <= 2^20), then written as three balanced base-2^7 digits
+// q = d0 2^14 + d1 2^7 + d2 (|d| <= 64, int8).  B (|b| <= 1) is rounded to
+// 2^-34 on the host, five digits b 2^34 = e0 2^28 + ... + e4.  The products
+// d_i e_j are summed exactly in int32 per level L = i + j (accumulator L,
+// TMEM columns 64 L): levels 0..2 complete, level 3 and 4 only d0 e3, d0 e4
+// (the other terms are below 2^-21 of the result).  The read-back combines
+// y = 2^e (A0 2^-12 + A1 2^-19 + A2 2^-26 + A3 2^-33 + A4 2^-40) with two
+// FP32 roundings to nearest: every rounding of the block is unbiased.
+constexpr int kTc8XDigits = 3, kTc8BDigits = 5;
+constexpr uint32_t kTc8Sbo = (kTcKr / 16) * 128;       // bytes between 8-row groups (64 int8 a row)
+constexpr uint32_t kTc8XDigit = kTcRows * kTcKr;       // bytes of one X digit array
+constexpr uint32_t kTc8BDigit = kTcN * kTcKr;          // bytes of one B digit array
+constexpr uint32_t kTc8BBytes = kTc8BDigits * kTc8BDigit;
 constexpr uint64_t kTcWaitNs = 1000000000ull;  // 1 s
 
 __device__ __forceinline__ uint64_t global_ns_tc() {
@@ -475,6 +498,170 @@ __device__ __noinline__ void wide_tc(const TOp& op, V* s, TcCtx& tc) {
                 for (int i = 0; i < 8; i++)
                     t[swz(b | co[(c >> 1) + i], (float2*)nullptr)] =
                         make_float2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
+            }
+        }
+        tc::fence_before_sync();
+    }
+}
+
+__device__ __forceinline__ uint32_t tc8_off(uint32_t r, uint32_t k) {
+    return (r >> 3) * kTc8Sbo + (k >> 4) * 128 + (r & 7) * 16 + (k & 15);
+}
+
+__device__ __forceinline__ uint32_t tc8_digits(int q, int c, uint32_t (&w)[kTc8XDigits]) {
+    const int d0 = (q + 8192) >> 14;
+    const int r0 = q - (d0 << 14);
+    const int d1 = (r0 + 64) >> 7;
+    const int d2 = r0 - (d1 << 7);
+    w[0] |= (uint32_t)(uint8_t)(int8_t)d0 << (8 * c);
+    w[1] |= (uint32_t)(uint8_t)(int8_t)d1 << (8 * c);
+    w[2] |= (uint32_t)(uint8_t)(int8_t)d2 << (8 * c);
+    return 0;
+}
+
+template <typename V>
+__device__ __noinline__ void wide_tc8(const TOp& op, V* s, TcCtx& tc) {
+    if constexpr (sizeof(V) == 8) {
+        float2* t = (float2*)s;
+        const uint32_t nt = blockDim.x, tid = threadIdx.x;
+        __shared__ uint32_t co[1 << kTcK];
+        __shared__ float wmax[32];
+        __shared__ int sexp;
+        const uint32_t bbytes = tc.bfloats * 4;
+        float* bslot = tc.resident ? tc.bh + (size_t)(op.mma / kTcOpFloats) * tc.bfloats : tc.bh;
+        const bool need_b = !tc.resident && tc.loaded != op.mma;
+        if (need_b && tid == 0 && !tc.stall) {
+            tc::mbar_arrive_expect_tx(tc.bbar, bbytes);
+            tc::bulk_g2s(bslot, tc.mmat + op.mma + kTc8Off, bbytes, tc.bbar);
+        }
+        if (tid < (1u << kTcK)) {
+            uint32_t o = 0;
+#pragma unroll
+            for (int q = 0; q < kTcK; q++) o |= (uint32_t)((tid >> q) & 1) << op.tl[q];
+            co[tid] = o;
+        }
+        // 1. the scale: 2^e above the largest |x| of the tile
+        float mx = 0.f;
+        for (uint32_t l = tid; l < (1u << kTcTileBits); l += nt) {
+            const float2 v = t[l];
+            mx = fmaxf(mx, fmaxf(fabsf(v.x), fabsf(v.y)));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if ((tid & 31) == 0) wmax[tid >> 5] = mx;
+        __syncthreads();
+        if (tid == 0) {
+            float m = 0.f;
+            for (uint32_t w = 0; w < (nt >> 5); w++) m = fmaxf(m, wmax[w]);
+            int e = 0;
+            frexpf(m, &e);  // m < 2^e
+            sexp = e;
+        }
+        __syncthreads();
+        const int e = sexp;
+        const float f = ldexpf(1.f, 20 - e);
+        // 2. X as three int8 digit arrays (row g = group, 64 bytes a row)
+        unsigned char* xd = (unsigned char*)tc.xh;
+        const uint32_t g = tid & (kTcRows - 1);
+        uint32_t gb = g;
+#pragma unroll
+        for (int q = 0; q < kTcK; q++) gb = ins0(gb, op.ts[q]);
+        for (uint32_t jp = tid >> 7; jp < 16; jp += nt >> 7) {
+            const float2 v0 = t[swz(gb | co[2 * jp], (float2*)nullptr)];
+            const float2 v1 = t[swz(gb | co[2 * jp + 1], (float2*)nullptr)];
+            uint32_t w[kTc8XDigits] = {0, 0, 0};
+            tc8_digits(__float2int_rn(v0.x * f), 0, w);
+            tc8_digits(__float2int_rn(v0.y * f), 1, w);
+            tc8_digits(__float2int_rn(v1.x * f), 2, w);
+            tc8_digits(__float2int_rn(v1.y * f), 3, w);
+            const uint32_t off = tc8_off(g, 4 * jp);
+#pragma unroll
+            for (int d = 0; d < kTc8XDigits; d++) *(uint32_t*)(xd + d * kTc8XDigit + off) = w[d];
+        }
+        tc::fence_proxy_async();
+        tc::fence_before_sync();
+        __syncthreads();
+        // 3. one thread issues the MMAs: 8 digit products x 2 K-steps
+        bool b_ok = true;
+        if (need_b) {
+            tc.loaded = op.mma;
+            if (tid == 0) {
+                const uint64_t tb = global_ns_tc();
+                while (!(b_ok = tc::mbar_try_wait(tc.bbar, tc.bphase)))
+                    if (global_ns_tc() - tb > tc.wait_ns) break;
+            }
+            tc.bphase ^= 1u;
+        }
+        if (tid == 0) {
+            if (!b_ok) {
+                tc.failed = 1;
+                atomicExch(tc.err, 1);
+                if (!tc.stall) tc::commit(tc.bar);
+            } else {
+                tc::fence_after_sync();
+                constexpr uint32_t idesc = tc::idesc_i8(kTcRows, kTcN);
+                const uint32_t xa = tc::smem_u32(xd), ba = tc::smem_u32(bslot);
+                // (X digit, B digit, level): first product of each level initialises it
+                const int prod[8][3] = {{0, 0, 0}, {0, 1, 1}, {1, 0, 1}, {0, 2, 2},
+                                        {1, 1, 2}, {2, 0, 2}, {0, 3, 3}, {0, 4, 4}};
+#pragma unroll
+                for (int p = 0; p < 8; p++) {
+                    const int i = prod[p][0], j = prod[p][1], L = prod[p][2];
+                    const bool first = p == 0 || prod[p - 1][2] != L;
+#pragma unroll
+                    for (int ks = 0; ks < 2; ks++) {
+                        const uint32_t o = (uint32_t)ks * 256;
+                        tc::mma_i8(tc.tmem + (uint32_t)(64 * L),
+                                   tc::smem_desc(xa + (uint32_t)i * kTc8XDigit + o, 128, kTc8Sbo),
+                                   tc::smem_desc(ba + (uint32_t)j * kTc8BDigit + o, 128, kTc8Sbo), idesc,
+                                   (first && ks == 0) ? 0u : 1u);
+                    }
+                }
+                tc::commit(tc.bar);
+            }
+        }
+        // 4. every thread waits for completion (bounded)
+        bool done = false;
+        const uint64_t t0 = global_ns_tc();
+        while (!(done = tc::mbar_try_wait(tc.bar, tc.phase))) {
+            if (global_ns_tc() - t0 > tc.wait_ns) break;
+        }
+        tc.phase ^= 1u;
+        if (!done) {
+            tc.failed = 1;
+            if (tid == 0) atomicExch(tc.err, 1);
+        }
+        tc::fence_after_sync();
+        // 5. read-back: warp w reads accumulator lanes 32 (w % 4) .. + 31
+        // (lane = group) of its share of the 64 columns of every level
+        const uint32_t warp = tid >> 5, nwarp = nt >> 5;
+        const uint32_t cpw = 64 / (nwarp >> 2);
+        if (done) {
+            const uint32_t g2 = ((warp & 3) << 5) | (tid & 31);
+            uint32_t b = g2;
+#pragma unroll
+            for (int q = 0; q < kTcK; q++) b = ins0(b, op.ts[q]);
+            const uint32_t c0 = (warp >> 2) * cpw;
+            const uint32_t lane_base = tc.tmem + ((((warp & 3) << 5)) << 16);
+            for (uint32_t c = c0; c < c0 + cpw; c += 16) {
+                uint32_t r0[16], r1[16], r2[16], r3[16], r4[16];
+                tc::tmem_ld16(lane_base + c, r0);
+                tc::tmem_ld16(lane_base + 64 + c, r1);
+                tc::tmem_ld16(lane_base + 128 + c, r2);
+                tc::tmem_ld16(lane_base + 192 + c, r3);
+                tc::tmem_ld16(lane_base + 256 + c, r4);
+                tc::tmem_wait_ld();
+                float y[16];
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    const int H = (int)r0[i] * 128 + (int)r1[i];
+                    const int Lo = (int)r2[i] * 128 + (int)r3[i];
+                    const float v = fmaf((float)(int)r4[i], 0x1p-21f, fmaf((float)Lo, 0x1p-14f, (float)H));
+                    y[i] = ldexpf(v, e - 19);
+                }
+#pragma unroll
+                for (int i = 0; i < 8; i++)
+                    t[swz(b | co[(c >> 1) + i], (float2*)nullptr)] = make_float2(y[2 * i], y[2 * i + 1]);
             }
         }
         tc::fence_before_sync();
@@ -661,7 +848,10 @@ __device__ __forceinline__ void tile_compute(const TileHdr& hdr, uint64_t base, 
             const bool on = (base & op.gcmask) == op.gcval;
             if constexpr (TC) {
                 if (op.mma >= 0) {  // no controls, 5 targets, 2^12 tile (host-checked)
-                    wide_tc<V>(op, s, *tcx);
+                    if (tcx->variant & kTcVarInt8)
+                        wide_tc8<V>(op, s, *tcx);
+                    else
+                        wide_tc<V>(op, s, *tcx);
                     __syncthreads();
                     continue;
                 }
@@ -835,7 +1025,7 @@ __device__ __forceinline__ void tma_store_tile(const CUtensorMap* map, const Til
 }
 
 constexpr uint64_t kTileWaitNs = 1000000000ull;  // 1 s
-constexpr int kMaxStages = 3;
+constexpr int kMaxStages = 4;
 
 // One pass over every tile.  Persistent: each CTA loops over the tiles t =
 // blockIdx.x, blockIdx.x + gridDim.x, ...
@@ -895,7 +1085,7 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         tcx.bll = tcx.bl + kTcN * kTcKr;
         tcx.variant = hdr.tc_variant;
         tcx.resident = hdr.tc_resident > 0;
-        tcx.bfloats = (hdr.tc_variant & kTcVarB3 ? 3u : 2u) * kTcN * kTcKr;
+        tcx.bfloats = hdr.tc_variant & kTcVarInt8 ? kTc8BBytes / 4 : (hdr.tc_variant & kTcVarB3 ? 3u : 2u) * kTcN * kTcKr;
         tcx.mmat = mmat;
         tcx.loaded = -1;
         tcx.failed = 0;
@@ -911,7 +1101,7 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
             tc::mbar_init(&tc_bbar, 1);
         }
         if (threadIdx.x < 32) {
-            tc::tmem_alloc(&tc_tmem, kTcCols);
+            tc::tmem_alloc(&tc_tmem, hdr.tc_variant & kTcVarInt8 ? 512u : (uint32_t)kTcCols);
             tc::tmem_relinquish();
         }
         tc::fence_before_sync();
@@ -923,9 +1113,10 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
             // (thread 0 issues the MMAs: it alone waits, bounded)
             if (threadIdx.x == 0) {
                 tc::mbar_arrive_expect_tx(tcx.bbar, (uint32_t)hdr.tc_resident * tcx.bfloats * 4);
+                const size_t src0 = hdr.tc_variant & kTcVarInt8 ? (size_t)kTc8Off : 0;
                 for (int j = 0; j < hdr.tc_resident; j++)
-                    tc::bulk_g2s(tcx.bh + (size_t)j * tcx.bfloats, mmat + (size_t)j * kTcOpFloats, tcx.bfloats * 4,
-                                 tcx.bbar);
+                    tc::bulk_g2s(tcx.bh + (size_t)j * tcx.bfloats, mmat + (size_t)j * kTcOpFloats + src0,
+                                 tcx.bfloats * 4, tcx.bbar);
                 const uint64_t t0 = global_ns_tc();
                 bool ok;
                 while (!(ok = tc::mbar_try_wait(tcx.bbar, 0)))
@@ -966,11 +1157,13 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         V* cur = (V*)(smem + (size_t)b * tile_bytes);
         const uint64_t base = tile_base(t, bt);
         if (use_tma) {
-            if (threadIdx.x == 0) {
-                const uint64_t tn = t + (uint64_t)(nbuf - 1) * grid;
+            // two buffers: the next tile's load goes out now, once the
+            // previous tile's store has read the buffer it needs
+            if (threadIdx.x == 0 && nbuf == 2) {
+                const uint64_t tn = t + grid;
                 if (tn < hdr.ntiles) {
-                    const uint32_t bn = (it + (uint32_t)nbuf - 1) % (uint32_t)nbuf;
-                    tma::wait_group_read<0>();  // the previous tile's store has read buffer bn
+                    const uint32_t bn = (it + 1) & 1u;
+                    tma::wait_group_read<0>();
                     tma_load_tile(&tmap, hdr, tile_base(tn, bt), sbase + bn * tile_bytes, &full_bar[bn], tile_bytes);
                     pending |= 1u << bn;
                 }
@@ -997,7 +1190,20 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         if (use_tma) {
             tc::fence_proxy_async();  // this thread's tile writes are visible to the bulk store
             __syncthreads();
-            if (threadIdx.x == 0) tma_store_tile(&tmap, hdr, base, sbase + b * tile_bytes);
+            if (threadIdx.x == 0) {
+                tma_store_tile(&tmap, hdr, base, sbase + b * tile_bytes);
+                // three or more buffers: the load of tile it + nbuf - 1 goes
+                // into the buffer of tile it - 1, whose store has had this
+                // whole tile's compute to read it (at most this tile's store
+                // may still be reading), so no thread waits before computing
+                const uint64_t tn = t + (uint64_t)(nbuf - 1) * grid;
+                if (nbuf > 2 && tn < hdr.ntiles) {
+                    const uint32_t bn = (it + (uint32_t)nbuf - 1) % (uint32_t)nbuf;
+                    tma::wait_group_read<1>();
+                    tma_load_tile(&tmap, hdr, tile_base(tn, bt), sbase + bn * tile_bytes, &full_bar[bn], tile_bytes);
+                    pending |= 1u << bn;
+                }
+            }
         } else {
             tile_store<V>(st, hdr, hoff, base, cur);
             __syncthreads();  // `cur` is read out before it receives the next tile
@@ -1029,7 +1235,7 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         __syncthreads();
         if (threadIdx.x < 32) {
             tc::fence_after_sync();
-            tc::tmem_dealloc(tcx.tmem, kTcCols);
+            tc::tmem_dealloc(tcx.tmem, tcx.variant & kTcVarInt8 ? 512u : (uint32_t)kTcCols);
         }
     }
 }
@@ -1678,7 +1884,7 @@ static int grow_host(void** p, size_t* have, size_t bytes) {
 // Tensor-core block variant (kTcVar* bits; YAO_TC_VARIANT overrides).
 static int tc_variant() {
     const char* e = getenv("YAO_TC_VARIANT");
-    return e ? (atoi(e) & 7) : 0;
+    return e ? (atoi(e) & 15) : 0;
 }
 
 // ------------------------------------------------------------- TMA maps
@@ -1820,7 +2026,7 @@ static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
         // each op run out (0.1 s each) and the call reports YAO_ERR_TIMEOUT
         if (const char* e = getenv("YAO_TEST_TC_STALL")) hdr.tc_test = e[0] == '1';
         hdr.tc_variant = tc_variant();
-        bslot = (hdr.tc_variant & kTcVarB3 ? 3 : 2) * kTcBPart;
+        bslot = hdr.tc_variant & kTcVarInt8 ? (size_t)kTc8BBytes : (hdr.tc_variant & kTcVarB3 ? 3 : 2) * kTcBPart;
         for (const TOp& op : ops) ntc += op.mma >= 0;
     }
     auto tcb = [&](int slots) { return hdr.mma ? 1024 + kTcXBytes + (size_t)slots * bslot : 0; };
@@ -1830,7 +2036,11 @@ static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
     const int slots = hdr.tc_resident ? ntc : 1;
     hdr.staged = 2 * tile_bytes + tcb(slots) + stg <= budget ? 1 : 0;
     hdr.nstage = 2;
-    if (hdr.use_tma && 3 * tile_bytes + tcb(slots) + (hdr.staged ? stg : 0) <= budget) hdr.nstage = 3;
+    for (int ns = 4; ns > 2 && hdr.use_tma; ns--)
+        if ((size_t)ns * tile_bytes + tcb(slots) + (hdr.staged ? stg : 0) <= budget) {
+            hdr.nstage = ns;
+            break;
+        }
     hdr.dmma = dm ? 1 : 0;
     size_t smem = (size_t)(hdr.use_tma ? hdr.nstage : 1) * tile_bytes + (hdr.staged ? stg : 0);
     if (hdr.mma) smem = ((smem + 1023) & ~(size_t)1023) + kTcXBytes + (size_t)slots * bslot;
@@ -1901,6 +2111,7 @@ static void tc_prepare(PassPlan& pp) {
         float* bh = pp.mmat.data() + op.mma;
         float* bl = bh + kTcN * kTcKr;
         float* bll = bl + kTcN * kTcKr;
+        unsigned char* b8dig = (unsigned char*)(bh + kTc8Off);
         const int nl = 1 << kTcK;
         for (int i = 0; i < nl; i++)
             for (int j = 0; j < nl; j++) {
@@ -1917,6 +2128,15 @@ static void tc_prepare(PassPlan& pp) {
                         bh[at] = h;
                         bl[at] = l;
                         bll[at] = host_tf32((float)(v[q][p2] - (double)h - (double)l));
+                        // integer form: v 2^34 rounded, five balanced base-2^7 digits
+                        int64_t r = std::llround(std::ldexp(std::max(-1.0, std::min(1.0, v[q][p2])), 34));
+                        const size_t b8 = (size_t)((o >> 3) * kTc8Sbo + (kk >> 4) * 128 + (o & 7) * 16 + (kk & 15));
+                        for (int d = 0; d < 5; d++) {
+                            const int sh = 7 * (4 - d);
+                            const int64_t dig = d < 4 ? (r + ((int64_t)1 << (sh - 1))) >> sh : r;
+                            r -= dig << sh;
+                            b8dig[(size_t)d * kTc8BDigit + b8] = (unsigned char)(int8_t)dig;
+                        }
                     }
             }
         pp.hdr.mma = 1;

@@ -43,6 +43,24 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a_desc, uint6
         : "memory");
 }
 
+// Instruction descriptor of kind::i8: D in S32 (bits 4-5 = 2), A and B
+// signed 8-bit (bits 7-9, 10-12 = 1), both K-major, N >> 3 in bits 17-22,
+// M >> 4 in bits 24-28.  Products and sums are exact (integer arithmetic).
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// D[tmem] (+)= A * B^T over K = 32 signed 8-bit values, issued by one thread.
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
 // The mbarrier receives one arrival when every MMA issued before by this
 // thread has completed.
 __device__ __forceinline__ void commit(uint64_t* bar) {
