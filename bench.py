@@ -186,6 +186,17 @@ def job_gbps(bytes_per_rank, world, ms):
     return world * bytes_per_rank / (ms / 1e3) / 1e9
 
 
+def host_cpus():
+    """CPUs this process may use: the machine's count, the affinity mask and
+    the cgroup quota (cpu.max), which bounds how much host work can overlap."""
+    out = {"cpu_count": os.cpu_count(), "affinity": len(os.sched_getaffinity(0))}
+    try:
+        out["cgroup_cpu_max"] = open("/sys/fs/cgroup/cpu.max").read().strip()
+    except OSError:
+        pass
+    return out
+
+
 def host_ram_gb():
     try:
         for line in open("/proc/meminfo"):
@@ -429,6 +440,7 @@ def main():
         # the full record (kernel tables, per-run lists, the DM <Z_i>) on a
         # line of its own; the last line stays short
         detail = {"detail": {"kernels": kernels, "profiled_bytes": prof_bytes, "first_gates_n30": first_gates,
+                             "host_cpus": host_cpus(),
                              **extras}}
         print(json.dumps(detail), flush=True)
         line["summary"] = summary(extras, plain_s, first_gates)
@@ -526,42 +538,56 @@ def tc_drift(Y, A, n):
     FP64 norm restore: the norm drift per tensor-core block, 1 - F and max
     |error| against the FP64 PLAIN result, for every tensor-core variant
     (YAO_TC_VARIANT bits: 2 separate correction accumulator, 8 the integer
-    form with exact int32 accumulation) and for the CUDA-core split form; one
-    JSON line per form."""
+    form with exact int32 accumulation) and for the CUDA-core split form,
+    from |0...0> and from a random state; one JSON line per form and start."""
     import torch
     os.environ.update(YAO_TILE_BITS="12", YAO_REG_BITS="3", YAO_AUTOTUNE="0", YAO_NORM_RESTORE="0")
     c = Y.Circuit.qubits(n, [el for l in range(LAYERS) for el in layer_elements(Y, n, l)])
-    ref = Y.ArrayReg.zero_state(n)
-    Y.apply_inplace(c, ref)
     info = Y.plan_info(c, Y.C64, Y.MODE_FUSED, 5, 12, 3)
     stream = torch.cuda.ExternalStream(A.stream_ptr(0), device=torch.device("cuda", 0))
-    forms = [("tc_v%d" % v, "1", str(v)) for v in (0, 2, 8)] + [("cuda_core", "0", "0")]
-    for name, tc, var in forms:
-        os.environ.update(YAO_TC=tc, YAO_TC_VARIANT=var)
-        r = Y.ArrayReg.zero_state(n, Y.C64)
-        Y.apply_inplace(c, r, Y.MODE_FUSED, 5)  # warm-up
-        r = Y.ArrayReg.zero_state(n, Y.C64)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        A.synchronize()
-        e0.record(stream)
-        Y.apply_inplace(c, r, Y.MODE_FUSED, 5)
-        e1.record(stream)
-        e1.synchronize()
-        nrm2 = r.norm() ** 2
-        blocks = info["tensor_core_ops"] if tc == "1" else info["blocks"]
-        print(json.dumps({"form": name, "qubits": n, "tc_blocks": info["tensor_core_ops"], "blocks": info["blocks"],
-                          "norm2_minus_1": nrm2 - 1.0, "norm2_drift_per_tc_block": (nrm2 - 1.0) / max(1, blocks),
-                          "one_minus_fidelity": 1.0 - ref.fidelity(r), "max_abs_err": ref.max_abs_diff(r),
-                          "ms": e0.elapsed_time(e1)}), flush=True)
+    rng = np.random.default_rng(77)
+    v = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    v /= np.linalg.norm(v)
+    starts = {"zero": None, "random": v}
+    forms = [("tc_v%d" % v_, "1", str(v_)) for v_ in (0, 2, 8)] + [("cuda_core", "0", "0")]
+    for sname, sv in starts.items():
+        def fresh(prec):
+            if sv is None:
+                return Y.ArrayReg.zero_state(n, prec)
+            r0 = Y.ArrayReg.from_vec(n, sv)
+            return r0 if prec == Y.C128 else r0.to_precision(prec)
+        ref = fresh(Y.C128)
+        Y.apply_inplace(c, ref)
+        n0 = fresh(Y.C64).norm() ** 2
+        for name, tc, var in forms:
+            os.environ.update(YAO_TC=tc, YAO_TC_VARIANT=var)
+            r = fresh(Y.C64)
+            Y.apply_inplace(c, r, Y.MODE_FUSED, 5)  # warm-up
+            r = fresh(Y.C64)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            A.synchronize()
+            e0.record(stream)
+            Y.apply_inplace(c, r, Y.MODE_FUSED, 5)
+            e1.record(stream)
+            e1.synchronize()
+            nrm2 = r.norm() ** 2
+            blocks = info["tensor_core_ops"] if tc == "1" else info["blocks"]
+            print(json.dumps({"form": name, "start": sname, "qubits": n, "tc_blocks": info["tensor_core_ops"],
+                              "blocks": info["blocks"], "norm2_minus_start": nrm2 - n0,
+                              "norm2_drift_per_tc_block": (nrm2 - n0) / max(1, blocks),
+                              "one_minus_fidelity": 1.0 - ref.fidelity(r), "max_abs_err": ref.max_abs_diff(r),
+                              "ms": e0.elapsed_time(e1)}), flush=True)
 
 
 def run_extras(Y, A, torch, stream, circuits, n, dev):
     """Full 40-layer circuit through the TILED and FUSED forms, 1 - F against
     the FP64 result, and the VQE gradient rate."""
     out = {}
-    # the oracle at the configurations' own sizes, in threads while the GPU
-    # works: the VQE energy and all 384 gradient entries at n = 24, and one
-    # full noisy layer of the density-matrix workload at n = 12
+    # the oracle at the configurations' own sizes: the VQE energy and all 384
+    # gradient entries at n = 24, and one full noisy layer of the
+    # density-matrix workload at n = 12, in threads while the FUSED forms run
+    # (seconds-long kernels timed by CUDA events); joined before any
+    # wall-clock or launch-bound measurement, which CPU contention would skew
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
     O.lib()
@@ -572,11 +598,9 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
     op = tfim(Y, nv)
     z24 = np.zeros(1 << nv, complex)
     z24[0] = 1
-    bg_vqe = Background(O.expect_grad, op, vc, z24)
     dm12 = noisy_dm_circuit(Y, 12, 1)
     rho12 = np.zeros(1 << 24, complex)
     rho12[0] = 1
-    bg_dm = Background(O.dm_apply_circuit, dm12, rho12)
 
     def timed(fn):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -598,6 +622,8 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
     ref = Y.ArrayReg.zero_state(n, device=dev)
     t_tiled = timed(lambda: Y.apply_inplace(whole, ref, Y.MODE_TILED))
     out["s_per_circuit_tiled"] = t_tiled
+    bg_vqe = Background(O.expect_grad, op, vc, z24)
+    bg_dm = Background(O.dm_apply_circuit, dm12, rho12)
     forms = {}
     for name, prec, k in (("fused_f64_k5", Y.C128, 5), ("fused_f64_k4", Y.C128, 4), ("fused_c64_k5", Y.C64, 5),
                           ("fused_c64_k4", Y.C64, 4), ("fused_c64_k3", Y.C64, 3), ("fused_c64_auto", Y.C64, 0),
@@ -619,6 +645,8 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
     out["fused"] = forms
     out["autotuned"] = chosen
     del ref
+    vo, go = bg_vqe.result()
+    ref12 = bg_dm.result()
     # VQE: n=24, 8 layers of Ry.Rz on every qubit + CNOT ring, TFIM
     z = Y.ArrayReg.zero_state(nv, device=dev)
     Y.expect_grad(op, vc, z)
@@ -639,7 +667,6 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
         fd_err = max(fd_err, abs(fd - g[i]) / max(1e-12, abs(g[i])))
     # the oracle's expect_grad at n = 24 on the same angles (one thread,
     # run in the background since the start of the extras)
-    vo, go = bg_vqe.result()
     out["vqe"] = {"qubits": nv, "params": len(g), "gates": len(vc.elements), "grads_per_s": 1.0 / dt,
                   "s_per_grad": dt, "energy": val, "fd_max_rel_err": fd_err,
                   "oracle_energy_diff": abs(val - vo),
@@ -651,7 +678,6 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
     out["noisy_dm14"] = dm_extra(Y, A, torch, stream, dev, timed)
     # one noisy layer at n = 12 against the oracle: PLAIN bit for bit, FUSED
     # (superoperators through the tile passes) to rounding
-    ref12 = bg_dm.result()
     d12 = {}
     for name, mode in (("plain", Y.MODE_PLAIN), ("fused", Y.MODE_FUSED)):
         d = Y.DensityMatrix.zero_state(12, device=dev)

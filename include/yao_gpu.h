@@ -287,6 +287,12 @@ int yao_expect_dm(const yao_dm* d, const yao_term* terms, size_t nterms, double 
  * state is computed in FUSED form (within ~1e-15 of the PLAIN state) and the
  * reverse sweep runs over shared-memory tiles of psi and lambda (circuits
  * with gates on more than 2 qubits, or YAO_ADJ_TILES=0: one step per gate). */
+/* The plan of expect_grad's tiled reverse sweep for c, computed on the host
+ * only (no device needed): info[3] = {passes, ops, generator dots}.  Steps
+ * on disjoint qubits may share a pass out of sweep order (YAO_ADJ_REORDER=0:
+ * consecutive steps only).  YAO_ERR_UNSUPPORTED when c takes the per-gate
+ * form (a gate on more than 2 qubits). */
+int yao_grad_plan_info(const yao_circuit* c, int64_t info[3]);
 int yao_expect_grad(const yao_term* terms, size_t nterms, const yao_circuit* c,
                     const yao_reg* psi0, double* value, double* grad, size_t ngrad);
 

@@ -148,6 +148,33 @@ def random_circuit(rng, n, depth, max_ctrl=2, custom=True, diag_custom=True):
     return Y.Circuit.qubits(n, els)
 
 
+def reverse_index_bits(m, k):
+    """The k-qubit matrix m with the bit order of its row and column index
+    reversed."""
+    p = [int(format(i, f"0{k}b")[::-1], 2) for i in range(1 << k)]
+    return np.asarray(m)[np.ix_(p, p)]
+
+
+def as_tensor_export_reads(circuit):
+    """The circuit whose state-vector apply equals the contraction of yao-rs's
+    tensor-network export of `circuit`.  The state-vector path reads a k-qubit
+    matrix with target_locs[0] as the least significant index bit
+    (sort_unitary_2q / instruct_nq, src/instruct_qubit.rs:214-231), the
+    export reshapes it row-major with target_locs[0] as the most significant
+    axis (gate_to_tensor, src/tensors.rs:26-80); the two agree for matrices
+    symmetric under that reversal (SWAP, ISWAP, FSim, CZ-like diagonals), so
+    only Custom multi-target matrices are rewritten."""
+    els = []
+    for e in circuit.elements:
+        if isinstance(e, Y.PositionedGate) and e.gate._matrix is not None and len(e.target_locs) > 1:
+            m = reverse_index_bits(e.gate._matrix, len(e.target_locs))
+            g = Gate.Custom(m, e.gate._is_diagonal, "R")
+            els.append(Y.PositionedGate(g, list(e.target_locs), list(e.control_locs), list(e.control_configs)))
+        else:
+            els.append(e)
+    return Y.Circuit.qubits(circuit.nbits, els)
+
+
 def random_state(rng, n):
     v = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
     return v / np.linalg.norm(v)

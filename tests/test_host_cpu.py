@@ -194,3 +194,23 @@ def test_planner_low_bits_and_one_qubit_runs():
     assert f1["blocks"] <= ngates - 2 * n * layers
     f5 = Y.plan_info(c, Y.C64, Y.MODE_FUSED, 5, 12, 3)
     assert f5["blocks"] == 130 and f5["passes"] <= 70 and f5["tensor_core_ops"] == 109
+
+
+def test_grad_plan_reorders_commuting_steps(monkeypatch):
+    """expect_grad's tiled reverse sweep for the VQE ansatz at n = 24 (8
+    layers of Ry.Rz on every qubit and a CNOT ring, 384 parameters): list
+    scheduling over the steps' qubits lets a pass take steps on disjoint
+    qubits out of sweep order, halving the passes of the in-order plan; every
+    parameter keeps one generator dot, and every Ry.Rz pair folds into one
+    op next to its CNOT."""
+    from helpers import vqe_ansatz
+    rng = np.random.default_rng(2024)
+    c = vqe_ansatz(24, 8, rng.uniform(-3, 3, size=2 * 24 * 8))
+    got = Y.grad_plan_info(c)
+    assert got == {"passes": 23, "ops": 384, "dots": 384}
+    monkeypatch.setenv("YAO_ADJ_REORDER", "0")
+    assert Y.grad_plan_info(c) == {"passes": 45, "ops": 384, "dots": 384}
+    # a 3-qubit gate sends expect_grad to the per-gate form
+    wide = Y.Circuit.qubits(4, [Y.put([0, 1, 2], Gate.Custom(np.eye(8), False, "I3"))])
+    with pytest.raises(Y.YaoError):
+        Y.grad_plan_info(wide)

@@ -10,6 +10,12 @@ GPU: the library's contraction agrees with the oracle's to 1e-12, with the
 state-vector oracle on qubit circuits, and with the golden outputs; edge
 cases (empty circuit, scalar networks, outer products, labels on more than
 two tensors) and the rejected inputs.
+
+yao-rs's export and its state-vector apply read a Custom k-qubit matrix with
+opposite index bit orders (see helpers.as_tensor_export_reads); the golden
+cases hold only 2-qubit gates symmetric under that reversal.  The
+state-vector comparisons therefore run the oracle on the circuit with those
+matrices' index bits reversed, and one test pins the difference itself.
 """
 import ctypes as C
 import math
@@ -20,7 +26,7 @@ import pytest
 import oracle as O
 import tn as OT
 import yao_rs as Y
-from helpers import circuit_from_case, random_circuit, random_state, state
+from helpers import as_tensor_export_reads, circuit_from_case, random_circuit, random_state, state
 from yao_rs import Gate, NoiseChannel
 
 
@@ -92,6 +98,21 @@ def test_networks_match_oracle_random(n):
         same_network(Y.circuit_to_expectation_dm(nc, op), OT.circuit_to_expectation_dm(nc, op))
 
 
+def test_export_reads_multi_qubit_matrices_msb_first():
+    """A Custom 2-qubit matrix: the export's contraction equals the state
+    vector of the bit-reversed matrix, not of the matrix itself (yao-rs's
+    own behaviour, restated by the oracle and the library alike)."""
+    rng = np.random.default_rng(3)
+    u = np.linalg.qr(rng.normal(size=(4, 4)) + 1j * rng.normal(size=(4, 4)))[0]
+    c = Y.Circuit.qubits(2, [Y.put([0], Gate.H), Y.put([0, 1], Gate.Custom(u, False, "U"))])
+    z = np.zeros(4, complex)
+    z[0] = 1
+    out = OT.contract(OT.circuit_to_einsum(c, boundary=True)).reshape(-1)
+    assert np.max(np.abs(out - O.apply_circuit(as_tensor_export_reads(c), z))) < 1e-14
+    assert np.max(np.abs(out - O.apply_circuit(c, z))) > 1e-3
+    same_network(Y.circuit_to_einsum_with_boundary(c), OT.circuit_to_einsum(c, boundary=True))
+
+
 def test_network_builders_reject_what_yao_rs_rejects():
     c = Y.Circuit.qubits(2, [Y.put([0], Gate.H)])
     two = Y.OperatorPolynomial([1.0, 1.0], [Y.OperatorString([(0, Y.Op.Z)]), Y.OperatorString([(1, Y.Op.Z)])])
@@ -137,7 +158,7 @@ def test_contract_matches_oracle_and_state_vector(n):
     c = random_circuit(rng, n, 40, max_ctrl=min(2, n - 1) if n > 1 else 0)
     z = np.zeros(1 << n, complex)
     z[0] = 1
-    psi = O.apply_circuit(c, z)
+    psi = O.apply_circuit(as_tensor_export_reads(c), z)
     out = Y.einsum.contract(Y.circuit_to_einsum_with_boundary(c)).reshape(-1)
     assert np.max(np.abs(out - psi)) < 1e-12
     assert np.max(np.abs(out - OT.contract(OT.circuit_to_einsum(c, boundary=True)).reshape(-1))) < 1e-12
@@ -163,7 +184,7 @@ def test_contract_density_matrix_networks(n):
     rho = Y.einsum.contract(Y.circuit_to_einsum_dm(c)).reshape(1 << n, 1 << n)
     z = np.zeros(1 << n, complex)
     z[0] = 1
-    ref = O.dm_apply_circuit(c, O.dm_from_reg(z, n)).reshape(1 << n, 1 << n)
+    ref = O.dm_apply_circuit(as_tensor_export_reads(c), O.dm_from_reg(z, n)).reshape(1 << n, 1 << n)
     assert np.max(np.abs(rho - ref)) < 1e-12
     assert np.max(np.abs(rho - OT.contract(OT.circuit_to_einsum_dm(c)).reshape(1 << n, 1 << n))) < 1e-12
     op = one_term(rng, n)

@@ -601,26 +601,58 @@ static void fuse_runs(std::vector<AdjTileOp>& ops) {
     ops.swap(out);
 }
 
-// Greedy passes: consecutive ops while the targets above the low bits fit
-// the scattered tile bits, and the op / slot limits hold.
+// Passes by list scheduling over the reverse sweep's dependencies.  Steps
+// on disjoint qubits (targets and controls) commute exactly (in
+// arithmetic they differ by rounding only), and a generator dot taken
+// before or after a step on other qubits is the same number
+// (<l| h G h^dagger |p> = <l|G|p> when h and G act on different qubits).
+// So a pass scans the remaining steps in sweep order and takes every step
+// that no skipped earlier step shares a qubit with, while the targets above
+// the low bits fit the tile's scattered bits and the op / slot limits hold;
+// a skipped step blocks its qubits for the rest of the scan.  The steps of
+// a pass keep their sweep order.
 void plan_adj(const std::vector<HostOp>& hops, uint32_t nbits, std::vector<AdjPass>& out) {
     const int tbits = (int)std::min<uint32_t>(nbits, kAdjLowBits + kAdjScatter);
     const int nlow = std::min(kAdjLowBits, tbits), S = tbits - nlow;
-    size_t i = 0;
-    while (i < hops.size()) {
+    const uint64_t all = nbits >= 64 ? ~0ull : ((1ull << nbits) - 1);
+    std::vector<uint64_t> qm(hops.size(), 0);
+    for (size_t j = 0; j < hops.size(); j++) {
+        for (int q = 0; q < hops[j].op.k; q++) qm[j] |= 1ull << hops[j].tb[q];
+        for (int b : hops[j].cb) qm[j] |= 1ull << b;
+    }
+    std::vector<char> used(hops.size(), 0);
+    const char* env = getenv("YAO_ADJ_REORDER");
+    const bool reorder = !(env && env[0] == '0');  // YAO_ADJ_REORDER=0: consecutive steps only
+    size_t first = 0;
+    while (first < hops.size()) {
         std::set<int> H;
-        size_t j = i;
+        std::vector<size_t> take;
+        uint64_t blocked = 0;
         int nslots = 0;
-        while (j < hops.size() && (int)(j - i) < kAdjMaxOps) {
+        for (size_t j = first; j < hops.size(); j++) {
+            if (used[j]) continue;
+            if (qm[j] & blocked) {
+                blocked |= qm[j];
+                if ((blocked & all) == all) break;
+                continue;
+            }
             std::set<int> need;
             for (int q = 0; q < hops[j].op.k; q++)
                 if (hops[j].tb[q] >= nlow && !H.count(hops[j].tb[q])) need.insert(hops[j].tb[q]);
-            if ((int)(H.size() + need.size()) > S) break;
-            if (hops[j].op.gen && nslots >= kAdjMaxSlots) break;
+            const bool fits = (int)(H.size() + need.size()) <= S && (int)take.size() < kAdjMaxOps &&
+                              !(hops[j].op.gen && nslots >= kAdjMaxSlots);
+            if (!fits) {
+                if (!reorder) break;
+                blocked |= qm[j];
+                if ((blocked & all) == all) break;
+                continue;
+            }
             H.insert(need.begin(), need.end());
             if (hops[j].op.gen) nslots++;
-            j++;
+            take.push_back(j);
         }
+        for (size_t j : take) used[j] = 1;
+        while (first < hops.size() && used[first]) first++;
         // the tile's scattered bits: the targets', then the lowest free bits
         for (int b = nlow; (int)H.size() < S && b < (int)nbits; b++) H.insert(b);
         AdjPass pass;
@@ -639,7 +671,7 @@ void plan_adj(const std::vector<HostOp>& hops, uint32_t nbits, std::vector<AdjPa
             if (local[b] < 0) pass.hdr.outb[no++] = (int8_t)b;
         pass.hdr.nouts = no;
         pass.hdr.ntiles = (uint64_t)1 << (nbits - tbits);
-        for (size_t q = i; q < j; q++) {
+        for (size_t q : take) {
             AdjTileOp op = hops[q].op;
             op.tl[0] = (int8_t)local[hops[q].tb[0]];
             if (op.k == 2) op.tl[1] = (int8_t)local[hops[q].tb[1]];
@@ -680,19 +712,23 @@ void plan_adj(const std::vector<HostOp>& hops, uint32_t nbits, std::vector<AdjPa
         pass.hdr.nops = (int32_t)pass.ops.size();
         pass.hdr.nslots = (int32_t)pass.slot_grad.size();
         out.push_back(std::move(pass));
-        i = j;
     }
 }
 
 }  // namespace
 
-// The reverse sweep of expect_grad over tiles; psi holds the forward state
-// and lambda = H psi on entry.  Returns YAO_ERR_UNSUPPORTED, with nothing
-// launched, when some step is not a 1- or 2-qubit gate (the caller then runs
-// the per-gate form).  grad receives 2 Re <lambda | G psi> per parameter.
-int adjoint_tiles(Ctx* ctx, Reg* psi, Reg* lam, const Circuit* c, double* grad, size_t np) {
-    const uint32_t n = psi->nbits;
-    if (n < 3 || n > 62 || psi->precision != YAO_C128) return YAO_ERR_UNSUPPORTED;
+// The host plan of a reverse sweep: its passes, their op and dot counts.
+struct AdjPlan {
+    std::vector<AdjPass> passes;
+    size_t nops = 0, ndots = 0;
+};
+
+// The plan of expect_grad's reverse sweep over tiles (host only).  *status
+// is YAO_ERR_UNSUPPORTED, and the result null, when some step is not a 1- or
+// 2-qubit gate (the caller then runs the per-gate form).
+AdjPlan* adjoint_plan_new(const Circuit* c, uint32_t n, int32_t precision, size_t np, int* status) {
+    *status = YAO_ERR_UNSUPPORTED;
+    if (n < 3 || n > 62 || precision != YAO_C128) return nullptr;
     std::vector<HostOp> hops;
     size_t slot = np;
     for (size_t ei = c->elems.size(); ei-- > 0;) {
@@ -703,7 +739,7 @@ int adjoint_tiles(Ctx* ctx, Reg* psi, Reg* lam, const Circuit* c, double* grad, 
         lower_gate(gate_dagger(g), n, 0, false, dag);
         const int npar = gate_num_params(g.type);
         if (npar > 0) {
-            if (slot < (size_t)npar) return YAO_ERR_UNSUPPORTED;
+            if (slot < (size_t)npar) return nullptr;
             for (int i = 0; i < npar; i++) {
                 std::vector<Cx> gm;
                 uint32_t gd;
@@ -711,25 +747,44 @@ int adjoint_tiles(Ctx* ctx, Reg* psi, Reg* lam, const Circuit* c, double* grad, 
                 HostOp h;
                 if (!to_host_op(lower_matrix(gm, gd, false, g.targets, g.ctrls, g.cfgs, n, 0), true,
                                 (int)(slot - npar + i), h))
-                    return YAO_ERR_UNSUPPORTED;
+                    return nullptr;
                 hops.push_back(h);
             }
             slot -= npar;
         }
         for (const LGate& d : dag) {
             HostOp h;
-            if (!to_host_op(d, false, -1, h)) return YAO_ERR_UNSUPPORTED;
+            if (!to_host_op(d, false, -1, h)) return nullptr;
             hops.push_back(h);
         }
     }
-    std::vector<AdjPass> passes;
-    plan_adj(hops, n, passes);
-    if (passes.empty()) return YAO_OK;
-    size_t nops = 0, ndots = 0;
-    for (const AdjPass& p : passes) {
-        nops += p.ops.size();
-        ndots += p.slot_grad.size();
+    AdjPlan* plan = new AdjPlan();
+    plan_adj(hops, n, plan->passes);
+    for (const AdjPass& p : plan->passes) {
+        plan->nops += p.ops.size();
+        plan->ndots += p.slot_grad.size();
     }
+    *status = YAO_OK;
+    return plan;
+}
+
+void adjoint_plan_free(AdjPlan* p) { delete p; }
+
+void adjoint_plan_counts(const AdjPlan* p, int64_t out[3]) {
+    out[0] = (int64_t)p->passes.size();
+    out[1] = (int64_t)p->nops;
+    out[2] = (int64_t)p->ndots;
+}
+
+// The reverse sweep of a plan; psi holds the forward state and lambda =
+// H psi on entry.  grad receives 2 Re <lambda | G psi> per parameter.
+// Synchronises at the end; a set error word (from this sweep's bounded
+// waits or from work queued before it) is reported as YAO_ERR_TIMEOUT.
+int adjoint_run(Ctx* ctx, Reg* psi, Reg* lam, const AdjPlan* plan, double* grad) {
+    const uint32_t n = psi->nbits;
+    const std::vector<AdjPass>& passes = plan->passes;
+    const size_t nops = plan->nops, ndots = plan->ndots;
+    if (passes.empty()) return read_device_err(ctx, "expect_grad");
     const int tbits = passes[0].hdr.tbits;
     const size_t tile_bytes = (size_t)2 * ((size_t)1 << tbits) * sizeof(double2);  // psi's and lambda's tile
     // shared memory: the tile buffers (two when they fit), every op and slot
@@ -810,12 +865,21 @@ int adjoint_tiles(Ctx* ctx, Reg* psi, Reg* lam, const Circuit* c, double* grad, 
     YAO_CUDA(cudaStreamSynchronize(ctx->stream));
     if (herr) {
         YAO_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
-        return fail(YAO_ERR_TIMEOUT, "adjoint sweep: a tile copy wait gave up");
+        return fail(YAO_ERR_TIMEOUT, "expect_grad: a bounded wait of a kernel (tile copy) gave up");
     }
     doff = 0;
     for (const AdjPass& p : passes)
         for (size_t s = 0; s < p.slot_grad.size(); s++) grad[p.slot_grad[s]] = 2.0 * dots[doff++];
     return YAO_OK;
+}
+
+int adjoint_tiles(Ctx* ctx, Reg* psi, Reg* lam, const Circuit* c, double* grad, size_t np) {
+    int st = YAO_OK;
+    AdjPlan* plan = adjoint_plan_new(c, psi->nbits, psi->precision, np, &st);
+    if (!plan) return st;
+    st = adjoint_run(ctx, psi, lam, plan, grad);
+    adjoint_plan_free(plan);
+    return st;
 }
 
 }  // namespace yao

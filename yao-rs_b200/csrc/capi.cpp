@@ -849,6 +849,24 @@ int yao_plan_info(const yao_circuit* cc, int32_t precision, int32_t mode, int32_
     return plan_info(lowered(c), c->nbits, precision, mode, k, tile_bits, reg_bits, info);
 }
 
+int yao_grad_plan_info(const yao_circuit* cc, int64_t info[3]) {
+    CHECK_NULL(cc);
+    CHECK_NULL(info);
+    clear_error();
+    yao_circuit* c = const_cast<yao_circuit*>(cc);
+    if (!c->qubit_only) return fail(YAO_ERR_QUBIT_ONLY, "ArrayReg only supports qubit-only circuits");
+    for (const Element& el : c->elems)
+        if (el.kind == YAO_ELEM_CHANNEL) return fail(YAO_ERR_CHANNEL_IN_AD, "expect_grad: circuit contains a noise channel");
+    size_t np = 0;
+    yao_circuit_num_params(c, &np);
+    int st = YAO_OK;
+    AdjPlan* p = adjoint_plan_new(c, c->nbits, YAO_C128, np, &st);
+    if (!p) return fail(st, "expect_grad runs this circuit one gate at a time (no tiled plan)");
+    adjoint_plan_counts(p, info);
+    adjoint_plan_free(p);
+    return YAO_OK;
+}
+
 int yao_apply_inplace(const yao_circuit* c, yao_reg* r) { return yao_apply_inplace_mode(c, r, YAO_MODE_PLAIN, 0); }
 
 int yao_apply(const yao_circuit* c, const yao_reg* r, yao_reg** out) {
@@ -1183,44 +1201,82 @@ int yao_expect_grad(const yao_term* terms, size_t nterms, const yao_circuit* cc,
     if (s) return s;
     Ctx* ctx = psi0->ctx;
     YAO_CUDA(cudaSetDevice(ctx->device));
-    yao_reg* psi = nullptr;
-    yao_reg* lam = nullptr;
-    s = yao_reg_clone(psi0, &psi);
-    if (s) return s;
-    struct Guard {
-        yao_reg** a;
-        yao_reg** b;
-        ~Guard() {
-            yao_reg_free(*a);
-            yao_reg_free(*b);
+    // psi (a copy of psi0) and lambda in stream-ordered memory: nothing below
+    // synchronises before the reverse sweep's readback
+    Reg psi_r = *static_cast<const Reg*>(psi0), lam_r = *static_cast<const Reg*>(psi0);
+    psi_r.d = lam_r.d = nullptr;
+    struct Pool {
+        Ctx* ctx;
+        void* a = nullptr;
+        void* b = nullptr;
+        ~Pool() {
+            if (a) cudaFreeAsync(a, ctx->stream);
+            if (b) cudaFreeAsync(b, ctx->stream);
         }
-    } guard{&psi, &lam};
-    // forward pass: FUSED (FP64 blocks; within ~1e-15 of the PLAIN state)
-    s = launch_program(ctx, psi, lowered(c), YAO_MODE_FUSED, 0);
+    } pool{ctx};
+    const size_t bytes = psi_r.bytes();
+    if (cudaMallocAsync(&pool.a, bytes, ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        pool.a = nullptr;
+        return fail(YAO_ERR_OUT_OF_MEMORY, "expect_grad: cannot allocate the forward state");
+    }
+    psi_r.d = pool.a;
+    YAO_CUDA(cudaMemcpyAsync(psi_r.d, psi0->d, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    // forward pass: FUSED (FP64 blocks; within ~1e-15 of the PLAIN state);
+    // its error word is read with the sweep's
+    s = launch_program(ctx, &psi_r, lowered(c), YAO_MODE_FUSED, 0, false);
+    if (s) return s;
+    // the reverse sweep's plan, on the host while the forward pass runs
+    // (YAO_ADJ_TILES=0, or a wider gate: the per-gate form below)
+    struct PlanHold {
+        AdjPlan* p = nullptr;
+        ~PlanHold() {
+            if (p) adjoint_plan_free(p);
+        }
+    } plan;
+    const char* at = getenv("YAO_ADJ_TILES");
+    if (np && !(at && at[0] == '0')) {
+        int pst = YAO_OK;
+        plan.p = adjoint_plan_new(c, psi0->nbits, YAO_C128, np, &pst);
+        if (!plan.p && pst != YAO_ERR_UNSUPPORTED) return pst;
+    }
+    ExpectPending pend;
+    s = expect_terms_launch(ctx, &psi_r, mt, pend);
     if (s) return s;
     std::vector<Cx> vals;
-    s = expect_terms(ctx, psi, mt, vals);
-    if (s) return s;
-    Cx acc{0, 0};
-    for (size_t t = 0; t < mt.size(); t++) {
-        Cx p = cxmul(mt[t].coeff, vals[t]);
-        acc.re += p.re;
-        acc.im += p.im;
+    auto energy = [&]() {
+        expect_terms_collect(ctx, pend, vals);
+        Cx acc{0, 0};
+        for (size_t t = 0; t < mt.size(); t++) {
+            Cx p = cxmul(mt[t].coeff, vals[t]);
+            acc.re += p.re;
+            acc.im += p.im;
+        }
+        *value = acc.re;
+    };
+    if (np == 0 || !plan.p) {
+        // the per-gate form reuses the reduction buffers: collect first
+        s = read_device_err(ctx, "expect_grad");
+        if (s) return s;
+        energy();
+        if (np == 0) return YAO_OK;
     }
-    *value = acc.re;
-    if (np == 0) return YAO_OK;
-    Reg* l;
-    s = alloc_reg(ctx, psi0->nbits, YAO_C128, &l);
-    if (s) return s;
-    lam = static_cast<yao_reg*>(l);
+    if (cudaMallocAsync(&pool.b, bytes, ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        pool.b = nullptr;
+        return fail(YAO_ERR_OUT_OF_MEMORY, "expect_grad: cannot allocate lambda");
+    }
+    lam_r.d = pool.b;
+    Reg* psi = &psi_r;
+    Reg* lam = &lam_r;
     s = build_lambda(ctx, psi, mt, lam);
     if (s) return s;
-    // reverse sweep over shared-memory tiles of psi and lambda; circuits with
-    // wider gates (or YAO_ADJ_TILES=0) take the per-gate form below
-    const char* at = getenv("YAO_ADJ_TILES");
-    if (!(at && at[0] == '0')) {
-        s = adjoint_tiles(ctx, psi, lam, c, grad, np);
-        if (s != YAO_ERR_UNSUPPORTED) return s;
+    // reverse sweep over shared-memory tiles of psi and lambda
+    if (plan.p) {
+        s = adjoint_run(ctx, psi, lam, plan.p, grad);
+        if (s) return s;
+        energy();  // adjoint_run synchronised
+        return YAO_OK;
     }
     size_t slot = np;
     for (size_t ei = c->elems.size(); ei-- > 0;) {

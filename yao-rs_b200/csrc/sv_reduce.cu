@@ -493,43 +493,87 @@ static MonoDev to_dev(const MonoTerm& m) {
     return d;
 }
 
-// values[t] = <psi|O_t|psi> (without the coefficient)
-int expect_terms(Ctx* ctx, const Reg* r, const std::vector<MonoTerm>& terms, std::vector<Cx>& values) {
-    values.assign(terms.size(), Cx{0, 0});
-    uint64_t n = (uint64_t)1 << r->nbits;
+// values[t] = <psi|O_t|psi> (without the coefficient), in two halves: the
+// launch half groups the terms by X mask, runs one reduction per group into
+// its own part of the scratch (partials, then the group's sums) and queues
+// one copy of every group's sums into pinned host memory; the collect half,
+// after the stream has passed that copy, reads them.  Nothing synchronises
+// in between, so callers can queue more work before collecting.
+int expect_terms_launch(Ctx* ctx, const Reg* r, const std::vector<MonoTerm>& terms, ExpectPending& pend) {
+    pend.idx.clear();
+    pend.nv.clear();
+    pend.nterms = terms.size();
+    const uint64_t n = (uint64_t)1 << r->nbits;
     std::vector<bool> done(terms.size(), false);
+    std::vector<MonoGroup> groups;
     for (size_t t0 = 0; t0 < terms.size(); t0++) {
         if (done[t0]) continue;
         MonoGroup grp;
         memset(&grp, 0, sizeof(grp));
         grp.xmask = terms[t0].xmask;
         grp.hbit = grp.xmask ? 63 - __builtin_clzll(grp.xmask) : 0;
-        std::vector<size_t> idx;
-        for (size_t t = t0; t < terms.size() && (int)idx.size() < kMaxGroupTerms; t++)
+        for (size_t t = t0; t < terms.size() && grp.nt < kMaxGroupTerms; t++)
             if (!done[t] && terms[t].xmask == grp.xmask) {
-                grp.t[idx.size()] = to_dev(terms[t]);
-                idx.push_back(t);
+                grp.t[grp.nt++] = to_dev(terms[t]);
+                pend.idx.push_back(t);
                 done[t] = true;
             }
-        grp.nt = (int)idx.size();
-        uint64_t nwork = grp.xmask ? n / 2 : n;
-        int nb = reduce_blocks(ctx, nwork);
-        double* part;
-        if (reduce_scratch(ctx, nb, 2 * grp.nt, &part)) return YAO_ERR_OUT_OF_MEMORY;
+        groups.push_back(grp);
+        pend.nv.push_back(2 * grp.nt);
+    }
+    // scratch: every group's partials, then all groups' sums back to back
+    size_t nres = 0, npart = 0;
+    std::vector<int> nbs;
+    for (const MonoGroup& grp : groups) {
+        const int nb = reduce_blocks(ctx, grp.xmask ? n / 2 : n);
+        nbs.push_back(nb);
+        npart += (size_t)nb * 2 * grp.nt;
+        nres += 2 * (size_t)grp.nt;
+    }
+    if (groups.empty()) return YAO_OK;
+    if (ctx->ensure_scratch(sizeof(double) * (npart + nres))) return YAO_ERR_OUT_OF_MEMORY;
+    if (ctx->ensure_host_pinned(sizeof(double) * nres)) return YAO_ERR_OUT_OF_MEMORY;
+    double* part = (double*)ctx->scratch;
+    double* res = part + npart;
+    size_t po = 0, ro = 0;
+    for (size_t g = 0; g < groups.size(); g++) {
+        const MonoGroup& grp = groups[g];
+        const uint64_t nwork = grp.xmask ? n / 2 : n;
         {
             ProfScope prof(ctx, "expect_group", (double)n * (r->precision == YAO_C128 ? 16.0 : 8.0));
             if (r->precision == YAO_C128)
-                k_expect_group<double2><<<nb, kRT, 0, ctx->stream>>>((const double2*)r->d, nwork, grp, part);
+                k_expect_group<double2><<<nbs[g], kRT, 0, ctx->stream>>>((const double2*)r->d, nwork, grp, part + po);
             else
-                k_expect_group<float2><<<nb, kRT, 0, ctx->stream>>>((const float2*)r->d, nwork, grp, part);
+                k_expect_group<float2><<<nbs[g], kRT, 0, ctx->stream>>>((const float2*)r->d, nwork, grp, part + po);
         }
         ctx->launches++;
         YAO_CUDA(cudaGetLastError());
-        std::vector<double> res(2 * grp.nt);
-        int s = finish_sum(ctx, part, nb, 2 * grp.nt, res.data());
-        if (s) return s;
-        for (size_t q = 0; q < idx.size(); q++) values[idx[q]] = Cx{res[2 * q], res[2 * q + 1]};
+        k_final_sum<<<1, kRT, 0, ctx->stream>>>(part + po, nbs[g], 2 * grp.nt, res + ro);
+        ctx->launches++;
+        YAO_CUDA(cudaGetLastError());
+        po += (size_t)nbs[g] * 2 * grp.nt;
+        ro += 2 * (size_t)grp.nt;
     }
+    YAO_CUDA(cudaMemcpyAsync(ctx->host_pinned, res, sizeof(double) * nres, cudaMemcpyDeviceToHost, ctx->stream));
+    return YAO_OK;
+}
+
+void expect_terms_collect(Ctx* ctx, const ExpectPending& pend, std::vector<Cx>& values) {
+    values.assign(pend.nterms, Cx{0, 0});
+    const double* h = (const double*)ctx->host_pinned;
+    size_t k = 0, o = 0;
+    for (int nv : pend.nv) {
+        for (int q = 0; q < nv / 2; q++, k++) values[pend.idx[k]] = Cx{h[o + 2 * q], h[o + 2 * q + 1]};
+        o += (size_t)nv;
+    }
+}
+
+int expect_terms(Ctx* ctx, const Reg* r, const std::vector<MonoTerm>& terms, std::vector<Cx>& values) {
+    ExpectPending pend;
+    int s = expect_terms_launch(ctx, r, terms, pend);
+    if (s) return s;
+    YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+    expect_terms_collect(ctx, pend, values);
     return YAO_OK;
 }
 
@@ -1017,7 +1061,7 @@ int expect_noalloc(Ctx* ctx, const Reg* r, const yao_term* terms, size_t nterms,
     if (nterms > (size_t)kNoAllocMaxTerms)
         return fail(YAO_ERR_INVALID_ARGUMENT, "noalloc expectation: more than 64 terms");
     if (nterms && !terms) return fail(YAO_ERR_INVALID_ARGUMENT, "null terms");
-    double* scratch;
+    double* scratch = nullptr;
     int s = noalloc_scratch(ctx->device, &scratch);
     if (s) return s;
     MonoTerm mt[kNoAllocMaxTerms];

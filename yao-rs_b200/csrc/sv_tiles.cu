@@ -2145,7 +2145,7 @@ static void tc_prepare(PassPlan& pp) {
 
 template <typename V>
 static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, const std::vector<LGate>& prog,
-                           int32_t mode, const TileConfig& cfg) {
+                           int32_t mode, const TileConfig& cfg, bool check_err = true) {
     std::vector<LGate> work;
     const bool exact = (mode == YAO_MODE_TILED) && sizeof(V) == 16;
     if (mode == YAO_MODE_FUSED)
@@ -2186,7 +2186,9 @@ static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, c
     ctx->tc_used = any_tc;
     // a bounded wait of some pass (a tile's TMA copies, a tensor-core
     // operand copy or MMA completion) gave up: the run's result is void
-    if (ctx->d_err) {
+    // (check_err false: the caller reads the error word at its own
+    // synchronisation)
+    if (ctx->d_err && check_err) {
         int herr = 0;
         YAO_CUDA(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         YAO_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -2316,6 +2318,9 @@ static int tune_program(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog, 
     // cap the SM clock drifts over seconds; interleaving gives every
     // candidate the same clocks, so a drift does not pick a slower one.
     constexpr int kRounds = 3;
+    // YAO_TUNE_LOG=1: every candidate's best time on stderr
+    const char* tl = getenv("YAO_TUNE_LOG");
+    const bool log = tl && tl[0] == '1';
     auto best_of = [&](const std::vector<TileConfig>& cand, size_t* pick, float* pick_ms) -> int {
         std::vector<float> bestv(cand.size(), 0.f);
         float ms = 0.f;
@@ -2329,6 +2334,11 @@ static int tune_program(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog, 
         for (size_t i = 1; i < cand.size(); i++)
             if (bestv[i] < bestv[*pick]) *pick = i;
         *pick_ms = bestv[*pick];
+        if (log)
+            for (size_t i = 0; i < cand.size(); i++)
+                fprintf(stderr, "[yao tune] n=%u %s mode=%d k=%d tbits=%d rb=%d: %.3f ms over %zu gates%s\n", n,
+                        sizeof(V) == 8 ? "c64" : "c128", mode, cand[i].k, cand[i].tbits, cand[i].rb, bestv[i],
+                        sample.size(), i == *pick ? "  <- chosen" : "");
         return YAO_OK;
     };
     std::vector<TileConfig> shapes;
@@ -2406,7 +2416,7 @@ static int choose_config(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog,
 }
 
 template <typename V>
-static int run_program_t(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k) {
+static int run_program_t(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k, bool check_err) {
     V* st = (V*)r->d;
     if (mode == YAO_MODE_PLAIN) {
         for (const LGate& g : prog) {
@@ -2418,12 +2428,22 @@ static int run_program_t(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32
     TileConfig cfg;
     int s = choose_config<V>(ctx, r, prog, mode, k, false, &cfg);
     if (s) return s;
-    return run_program_cfg<V>(ctx, st, r->nbits, r->precision, prog, mode, cfg);
+    return run_program_cfg<V>(ctx, st, r->nbits, r->precision, prog, mode, cfg, check_err);
 }
 
-int launch_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k) {
-    if (r->precision == YAO_C128) return run_program_t<double2>(ctx, r, prog, mode, k);
-    return run_program_t<float2>(ctx, r, prog, mode, k);
+int launch_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k, bool check_err) {
+    if (r->precision == YAO_C128) return run_program_t<double2>(ctx, r, prog, mode, k, check_err);
+    return run_program_t<float2>(ctx, r, prog, mode, k, check_err);
+}
+
+int read_device_err(Ctx* ctx, const char* what) {
+    if (!ctx->d_err) return YAO_OK;
+    int herr = 0;
+    YAO_CUDA(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    YAO_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (!herr) return YAO_OK;
+    YAO_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    return fail(YAO_ERR_TIMEOUT, std::string(what) + ": a bounded wait of a kernel gave up");
 }
 
 int plan_info(const std::vector<LGate>& prog, uint32_t nbits, int32_t precision, int32_t mode, int32_t k,
@@ -2614,10 +2634,12 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
             for (const Cx& x : *cx) {
                 C cc;
                 if (sizeof(V) == 16) {
-                    *(double2*)&cc = make_double2(x.re, x.im);
+                    const double2 v = make_double2(x.re, x.im);
+                    memcpy(&cc, &v, sizeof(cc));
                 } else {
                     float hr = (float)x.re, hi = (float)x.im;
-                    *(float4*)&cc = make_float4(hr, hi, (float)(x.re - (double)hr), (float)(x.im - (double)hi));
+                    const float4 v = make_float4(hr, hi, (float)(x.re - (double)hr), (float)(x.im - (double)hi));
+                    memcpy(&cc, &v, sizeof(cc));
                 }
                 *dst++ = cc;
             }

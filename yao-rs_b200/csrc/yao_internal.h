@@ -190,7 +190,11 @@ struct DM {
 // ------------------------------------------------------- device launchers
 // All launchers enqueue on ctx->stream and return YAO_OK or an error.
 int launch_gate(Ctx* ctx, void* state, int32_t precision, uint32_t nbits, const LGate& g);
-int launch_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k);
+// check_err false: the error word of the passes' bounded waits is left for
+// the caller to read (read_device_err) at its own synchronisation
+int launch_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k, bool check_err = true);
+// Synchronises, and turns a set error word into YAO_ERR_TIMEOUT (clearing it)
+int read_device_err(Ctx* ctx, const char* what);
 // Time TILED / FUSED candidates for this program and register (always
 // re-tunes); out = {k, tile bits, register bits}.
 int autotune_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k, int32_t out[3]);
@@ -209,6 +213,13 @@ int launch_convert(Ctx* ctx, const Reg* src, Reg* dst);
 int reduce_norm_sqr(Ctx* ctx, const Reg* r, double* out);
 int launch_scale(Ctx* ctx, Reg* r, double inv_norm);
 int adjoint_tiles(Ctx* ctx, Reg* psi, Reg* lam, const Circuit* c, double* grad, size_t np);
+// adjoint_tiles in two halves: the host plan (null with *status
+// YAO_ERR_UNSUPPORTED when the per-gate form must run) and its sweep
+struct AdjPlan;
+AdjPlan* adjoint_plan_new(const Circuit* c, uint32_t n, int32_t precision, size_t np, int* status);
+void adjoint_plan_free(AdjPlan* p);
+void adjoint_plan_counts(const AdjPlan* p, int64_t out[3]);  // passes, ops, generator dots
+int adjoint_run(Ctx* ctx, Reg* psi, Reg* lam, const AdjPlan* plan, double* grad);
 int launch_batch_norm_sqr(Ctx* ctx, const std::vector<Reg*>& regs, double* out);
 int launch_batch_rescale(Ctx* ctx, const std::vector<Reg*>& regs, const double* n0, const double* n1);
 int reduce_inner(Ctx* ctx, const Reg* a, const Reg* b, Cx* out);
@@ -228,6 +239,15 @@ struct MonoTerm {
 int build_mono_terms(const yao_term* terms, size_t nterms, uint32_t nbits, bool msb_first,
                      std::vector<MonoTerm>& out);
 int expect_terms(Ctx* ctx, const Reg* r, const std::vector<MonoTerm>& terms, std::vector<Cx>& values);
+// expect_terms in two halves (the sums land in ctx->host_pinned once the
+// stream has passed the launch half's copy)
+struct ExpectPending {
+    size_t nterms = 0;
+    std::vector<size_t> idx;  // term of each result pair, group by group
+    std::vector<int> nv;      // doubles per group
+};
+int expect_terms_launch(Ctx* ctx, const Reg* r, const std::vector<MonoTerm>& terms, ExpectPending& pend);
+void expect_terms_collect(Ctx* ctx, const ExpectPending& pend, std::vector<Cx>& values);
 // The allocation-free expectation value (static device scratch), sv_reduce.cu.
 int expect_noalloc(Ctx* ctx, const Reg* r, const yao_term* terms, size_t nterms, double* out);
 int build_lambda(Ctx* ctx, const Reg* psi, const std::vector<MonoTerm>& terms, Reg* lambda);

@@ -14,7 +14,7 @@ from .gate import Gate
 from .noise import NoiseChannel
 from .operator import Op, OperatorPolynomial, OperatorString, op_matrix
 from .ops import (MeasureResult, PostProcess, apply, apply_inplace, autotune, batch_apply, expect_arrayreg, expect_dm, expect_grad_batch,
-                  expect_grad, measure_with_postprocess, plan_info, probs)
+                  expect_grad, grad_plan_info, measure_with_postprocess, plan_info, probs)
 from .einsum import (TensorNetwork, circuit_to_einsum, circuit_to_einsum_dm, circuit_to_einsum_with_boundary,
                      circuit_to_expectation, circuit_to_expectation_dm, circuit_to_overlap)
 from .register import ArrayReg, DensityMatrix, Register, density_matrix_from_reg
@@ -24,7 +24,7 @@ __all__ = [
     "MODE_TILED", "MeasureResult", "NoiseChannel", "Op", "OperatorPolynomial", "OperatorString",
     "PositionedAnnotation", "PositionedChannel", "PositionedGate", "PostProcess", "Register", "YaoError",
     "apply", "apply_inplace", "autotune", "batch_apply", "channel", "context", "control", "density_matrix_from_reg",
-    "elements_array", "expect_arrayreg", "expect_dm", "expect_grad", "expect_grad_batch", "label", "launch_count",
+    "elements_array", "expect_arrayreg", "expect_dm", "expect_grad", "expect_grad_batch", "grad_plan_info", "label", "launch_count",
     "measure_with_postprocess", "op_matrix", "plan_info", "probs", "put", "TensorNetwork", "circuit_to_einsum",
     "circuit_to_einsum_dm", "circuit_to_einsum_with_boundary", "circuit_to_expectation", "circuit_to_expectation_dm",
     "circuit_to_overlap", "einsum",

@@ -127,6 +127,7 @@ SIGNATURES = {
     "yao_apply_inplace_mode": (C.c_int, [vp, vp, i32, i32]),
     "yao_autotune": (C.c_int, [vp, vp, i32, i32, C.POINTER(i32)]),
     "yao_plan_info": (C.c_int, [vp, i32, i32, i32, i32, i32, C.POINTER(C.c_int64)]),
+    "yao_grad_plan_info": (C.c_int, [vp, C.POINTER(C.c_int64)]),
     "yao_dm_from_reg": (C.c_int, [vp, pp]),
     "yao_dm_zero_state": (C.c_int, [vp, u32, pp]),
     "yao_dm_from_host": (C.c_int, [vp, u32, dptr, pp]),

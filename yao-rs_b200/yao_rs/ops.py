@@ -43,6 +43,13 @@ def plan_info(circuit, precision=A.C128, mode=A.MODE_FUSED, k=5, tile_bits=12, r
     return dict(zip(keys, [int(x) for x in out]))
 
 
+def grad_plan_info(circuit) -> dict:
+    """The host plan of expect_grad's tiled reverse sweep (no device needed)."""
+    out = (C.c_int64 * 3)()
+    A.check(A.lib().yao_grad_plan_info(circuit.handle, out))
+    return dict(zip(("passes", "ops", "dots"), [int(x) for x in out]))
+
+
 def batch_apply(circuits, regs, mode: int = A.MODE_PLAIN, k: int = 0):
     cs = (C.c_void_p * max(1, len(circuits)))(*[c.handle for c in circuits])
     rs = (C.c_void_p * max(1, len(regs)))(*[r.handle for r in regs])
