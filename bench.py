@@ -572,11 +572,13 @@ def tc_drift(Y, A, n):
             e1.synchronize()
             nrm2 = r.norm() ** 2
             blocks = info["tensor_core_ops"] if tc == "1" else info["blocks"]
+            f = ref.fidelity(r)
             print(json.dumps({"form": name, "start": sname, "qubits": n, "tc_blocks": info["tensor_core_ops"],
                               "blocks": info["blocks"], "norm2_minus_start": nrm2 - n0,
                               "norm2_drift_per_tc_block": (nrm2 - n0) / max(1, blocks),
-                              "one_minus_fidelity": 1.0 - ref.fidelity(r), "max_abs_err": ref.max_abs_diff(r),
-                              "ms": e0.elapsed_time(e1)}), flush=True)
+                              "one_minus_fidelity": 1.0 - f,
+                              "one_minus_fidelity_normalised": 1.0 - f / (nrm2 * ref.norm() ** 2),
+                              "max_abs_err": ref.max_abs_diff(r), "ms": e0.elapsed_time(e1)}), flush=True)
 
 
 def run_extras(Y, A, torch, stream, circuits, n, dev):
@@ -627,7 +629,12 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
     forms = {}
     for name, prec, k in (("fused_f64_k5", Y.C128, 5), ("fused_f64_k4", Y.C128, 4), ("fused_c64_k5", Y.C64, 5),
                           ("fused_c64_k4", Y.C64, 4), ("fused_c64_k3", Y.C64, 3), ("fused_c64_auto", Y.C64, 0),
-                          ("fused_f64_auto", Y.C128, 0)):
+                          ("fused_f64_auto", Y.C128, 0), ("fused_c64_k5_int8_norestore", Y.C64, 5)):
+        # the integer tensor-core form (exact int32 accumulation) without the
+        # FP64 norm restore: its accuracy is its own
+        extra = {"YAO_TC_VARIANT": "8", "YAO_NORM_RESTORE": "0"} if name.endswith("int8_norestore") else {}
+        saved = {key: os.environ.get(key) for key in extra}
+        os.environ.update(extra)
         r = Y.ArrayReg.zero_state(n, prec, device=dev)
         chosen[name] = Y.autotune(whole, r, Y.MODE_FUSED, k)
         Y.apply_inplace(circuits[0], r, Y.MODE_FUSED, k)
@@ -639,9 +646,16 @@ def run_extras(Y, A, torch, stream, circuits, n, dev):
             r = Y.ArrayReg.zero_state(n, prec, device=dev)
             ts.append(timed(lambda: Y.apply_inplace(whole, r, Y.MODE_FUSED, k)))
         f = ref.fidelity(r)
+        nrm2 = r.norm() ** 2
         forms[name] = {"s_per_circuit": sorted(ts)[1], "s_runs": ts, "one_minus_fidelity": max(0.0, 1.0 - f),
+                       "one_minus_fidelity_normalised": 1.0 - f / nrm2, "norm2_minus_1": nrm2 - 1.0,
                        "max_abs_err": ref.max_abs_diff(r)}
         del r
+        for key, v in saved.items():
+            if v is None:
+                os.environ.pop(key, None)
+            else:
+                os.environ[key] = v
     out["fused"] = forms
     out["autotuned"] = chosen
     del ref
@@ -725,17 +739,24 @@ def summary(x, plain_s, first_gates):
         return sig(s)
     L = s["layered30"]
     L["tiled_s"] = x["s_per_circuit_tiled"]
-    L["fused"] = {k.replace("fused_", ""): [sig(v["s_per_circuit"], 3), sig(v["one_minus_fidelity"], 2)]
+    # [s/circuit, 1 - F (normalised), |norm^2 - 1|]
+    L["fused"] = {k.replace("fused_", ""): [sig(v["s_per_circuit"], 3), sig(v["one_minus_fidelity_normalised"], 2),
+                                            sig(abs(v["norm2_minus_1"]), 2)]
                   for k, v in x["fused"].items()}
-    L["autotuned"] = {k: [c["k"], c["tile_bits"], c["reg_bits"]] for k, c in x["autotuned"].items()
-                      if k in ("tiled", "fused_c64_auto", "fused_f64_auto")}
+    # the tuned choices of the auto forms (and of c64 k = 5): [k, tile bits,
+    # register bits(, tensor cores for complex64)]
+    L["autotuned"] = {k.replace("fused_", ""): [c["k"], c["tile_bits"], c["reg_bits"]] +
+                      ([c["tensor_cores"]] if "c64" in k else [])
+                      for k, c in x["autotuned"].items()
+                      if k in ("tiled", "fused_c64_auto", "fused_f64_auto", "fused_c64_k5")}
     fs = {k: v["s_per_circuit"] for k, v in x["fused"].items()}
     L["c64_auto_speedup_vs_plain"] = plain_s / fs["fused_c64_auto"]
     L["c128_auto_speedup_vs_plain"] = plain_s / fs["fused_f64_auto"]
     L["c64_auto_over_c128_auto"] = fs["fused_c64_auto"] / fs["fused_f64_auto"]
     # the autotuner's choice against the best fixed width (1.0 = as good)
     L["auto_over_best_fixed"] = {
-        "c64": fs["fused_c64_auto"] / min(v for k, v in fs.items() if k.startswith("fused_c64_k")),
+        "c64": fs["fused_c64_auto"] / min(v for k, v in fs.items() if k.startswith("fused_c64_k") and
+                                         not k.endswith("norestore")),
         "c128": fs["fused_f64_auto"] / min(v for k, v in fs.items() if k.startswith("fused_f64_k"))}
     v = x["vqe"]
     s["vqe24"] = {k: v[k] for k in ("grads_per_s", "fd_max_rel_err", "oracle_energy_diff", "oracle_max_abs_grad_diff",

@@ -227,8 +227,8 @@ int yao_apply_inplace_mode(const yao_circuit* c, yao_reg* r, int32_t mode, int32
  * shapes (and, for FUSED with k = 0, fusion widths 2..6) on a prefix of c
  * applied to a scratch copy of r (r is not changed) and records the fastest
  * for r's qubit count, precision and mode; later apply calls with the same
- * (qubits, precision, mode, k) use it.  choice[3] = {k, tile bits, register
- * bits}.  Apply calls tune on first use by themselves unless YAO_AUTOTUNE=0;
+ * (qubits, precision, mode, k) use it.  choice[4] = {k, tile bits, register
+ * bits, 1 when complex64 FUSED blocks may run on the tensor cores}.  Apply calls tune on first use by themselves unless YAO_AUTOTUNE=0;
  * YAO_TUNE_CACHE=<file> keeps the choices across processes. */
 int yao_autotune(const yao_circuit* c, yao_reg* r, int32_t mode, int32_t k, int32_t* choice);
 /* The TILED / FUSED plan of c for a given shape, computed on the host only

@@ -54,7 +54,8 @@ struct AdjTileOp {
     int8_t tl[2];    // local target positions; tl[0] is bit 0 of the gate-local index
     int8_t sync;     // barrier after this op (the next op moves amplitudes along other bits)
     int8_t ngen;     // kAdjFused: generator dots of the run
-    int8_t pad[4];
+    int8_t seg[2];   // 1-qubit ops: the segment's two local positions (seg[0] < seg[1])
+    int8_t pad[2];
     int32_t gslot[kAdjFusedGens];
     int32_t a_id;    // kAdjFused: A is the identity (no U^dagger in the run)
     uint32_t lcmask, lcval;  // in-tile controls (local positions)
@@ -274,6 +275,147 @@ __device__ __forceinline__ void adj_fused1(const AdjTileOp& op, double2* __restr
         }
 }
 
+// A segment: consecutive 1-qubit ops of a pass whose targets lie on two
+// local positions p0 < p1.  Thread g owns group g (the 4 amplitudes of psi
+// and lambda at local indices b, b + 2^p0, b + 2^p1, b + 2^p0 + 2^p1, b with
+// zeros at p0 and p1), loads it once, applies every op of the segment in
+// registers in order (pairs along the op's position; in-tile controls
+// checked per pair, out-of-tile controls per tile) and stores it once.
+// Each generator dot is reduced over the warp right after its op and added
+// to the warp's slot (lane 0), as in the one-op forms.
+template <int S>
+__device__ __forceinline__ void seg_pair_idx(int q, int& a, int& b) {
+    // q-th pair (q = 0, 1) along segment bit S of the group's index 0..3
+    if (S == 0) {
+        a = 2 * q;
+        b = 2 * q + 1;
+    } else {
+        a = q;
+        b = q + 2;
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void seg_op(const AdjTileOp& op, double2 (&x)[4], double2 (&l)[4], const uint32_t (&li)[4],
+                                       double* __restrict__ acc, uint32_t nw, bool valid) {
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (op.cls == kAdjFused) {
+        const int ng = op.ngen;
+        double dot[kAdjFusedGens] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            int ia, ib;
+            seg_pair_idx<S>(q, ia, ib);
+            const double2 x0 = x[ia], x1 = x[ib], l0 = l[ia], l1 = l[ib];
+            if (valid && ng > 0) {
+                // P[r][c] = conj(l_r) x_c; Re sum G'[r][c] P[r][c]
+                const double2 p00 = make_double2(fma(l0.x, x0.x, l0.y * x0.y), fma(l0.x, x0.y, -l0.y * x0.x));
+                const double2 p01 = make_double2(fma(l0.x, x1.x, l0.y * x1.y), fma(l0.x, x1.y, -l0.y * x1.x));
+                const double2 p10 = make_double2(fma(l1.x, x0.x, l1.y * x0.y), fma(l1.x, x0.y, -l1.y * x0.x));
+                const double2 p11 = make_double2(fma(l1.x, x1.x, l1.y * x1.y), fma(l1.x, x1.y, -l1.y * x1.x));
+#pragma unroll
+                for (int j = 0; j < kAdjFusedGens; j++)
+                    if (j < ng) {
+                        const double2* G = op.m + 4 + 4 * j;
+                        double d = fma(G[0].x, p00.x, -G[0].y * p00.y);
+                        d = fma(G[1].x, p01.x, fma(-G[1].y, p01.y, d));
+                        d = fma(G[2].x, p10.x, fma(-G[2].y, p10.y, d));
+                        d = fma(G[3].x, p11.x, fma(-G[3].y, p11.y, d));
+                        dot[j] += d;
+                    }
+            }
+            if (!op.a_id) {
+                const double2 a0 = op.m[0], a1 = op.m[1], a2 = op.m[2], a3 = op.m[3];
+                x[ia] = cfma2(cmul2(a0, x0), a1, x1);
+                x[ib] = cfma2(cmul2(a2, x0), a3, x1);
+                l[ia] = cfma2(cmul2(a0, l0), a1, l1);
+                l[ib] = cfma2(cmul2(a2, l0), a3, l1);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kAdjFusedGens; j++)
+            if (j < ng) {
+                const double d = warp_sum(dot[j]);
+                if (lane == 0) acc[op.gslot[j] * nw + warp] += d;
+            }
+        return;
+    }
+    double dot = 0.0;
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        int ia, ib;
+        seg_pair_idx<S>(q, ia, ib);
+        if ((li[ia] & op.lcmask) != op.lcval) continue;
+        if (op.gen) {
+            if (!valid) continue;
+            const double2 y0 = cfma2(cmul2(op.m[0], x[ia]), op.m[1], x[ib]);
+            const double2 y1 = cfma2(cmul2(op.m[2], x[ia]), op.m[3], x[ib]);
+            dot += redot(l[ia], y0) + redot(l[ib], y1);
+        } else if (op.cls == GC_X) {
+            double2 t = x[ia];
+            x[ia] = x[ib];
+            x[ib] = t;
+            t = l[ia];
+            l[ia] = l[ib];
+            l[ib] = t;
+        } else if (op.cls == GC_DIAG) {
+            if (op.active & 1) {
+                x[ia] = cmul2(op.m[0], x[ia]);
+                l[ia] = cmul2(op.m[0], l[ia]);
+            }
+            if (op.active & 2) {
+                x[ib] = cmul2(op.m[1], x[ib]);
+                l[ib] = cmul2(op.m[1], l[ib]);
+            }
+        } else {
+            const double2 x0 = x[ia], x1 = x[ib], l0 = l[ia], l1 = l[ib];
+            x[ia] = cfma2(cmul2(op.m[0], x0), op.m[1], x1);
+            x[ib] = cfma2(cmul2(op.m[2], x0), op.m[3], x1);
+            l[ia] = cfma2(cmul2(op.m[0], l0), op.m[1], l1);
+            l[ib] = cfma2(cmul2(op.m[2], l0), op.m[3], l1);
+        }
+    }
+    if (op.gen) {
+        const double d = warp_sum(dot);
+        if (lane == 0) acc[op.slot * nw + warp] += d;
+    }
+}
+
+__device__ __forceinline__ void adj_seg(const AdjTileOp* __restrict__ sops, int nr, uint64_t base,
+                                        double2* __restrict__ sp, double2* __restrict__ sl, uint32_t T,
+                                        double* __restrict__ acc, uint32_t nw) {
+    const int p0 = sops[0].seg[0], p1 = sops[0].seg[1];
+    const uint32_t g = threadIdx.x;
+    const bool valid = g < (T >> 2);
+    const uint32_t b = valid ? adj_ins0(adj_ins0(g, p0), p1) : 0u;
+    uint32_t li[4];
+    double2 x[4], l[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        li[q] = b | ((uint32_t)(q & 1) << p0) | ((uint32_t)(q >> 1) << p1);
+        if (valid) {
+            x[q] = sp[adj_swz(li[q])];
+            l[q] = sl[adj_swz(li[q])];
+        } else {
+            x[q] = l[q] = make_double2(0.0, 0.0);
+        }
+    }
+    for (int j = 0; j < nr; j++) {
+        const AdjTileOp& op = sops[j];
+        if ((base & op.gcmask) != op.gcval) continue;  // uniform over the tile
+        if (op.tl[0] == p0)
+            seg_op<0>(op, x, l, li, acc, nw, valid);
+        else
+            seg_op<1>(op, x, l, li, acc, nw, valid);
+    }
+    if (valid)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            sp[adj_swz(li[q])] = x[q];
+            sl[adj_swz(li[q])] = l[q];
+        }
+}
+
 constexpr uint64_t kAdjWaitNs = 1000000000ull;  // 1 s
 constexpr int kAdjMaxStages = 3;
 
@@ -391,7 +533,9 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
             int e = oi;
             while (!ops[e].sync) e++;
             e++;
-            if (ops[oi].cls == kAdjFused)
+            if (ops[oi].k == 1 && ops[oi].seg[0] != ops[oi].seg[1])
+                adj_seg(ops + oi, e - oi, base, sp, sl, T, acc, nw);
+            else if (ops[oi].cls == kAdjFused)
                 adj_fused1(ops[oi], sp, sl, T, acc, nw);
             else if (e - oi == 1 && ops[oi].k == 1 && ops[oi].cls == GC_X && !ops[oi].gen)
                 adj_x1(ops[oi], base, sp, sl, T);
@@ -601,6 +745,114 @@ static void fuse_runs(std::vector<AdjTileOp>& ops) {
     ops.swap(out);
 }
 
+// YAO_ADJ_SEGMENTS=0: one-op forms only (no register segments)
+static bool segments_on() {
+    const char* e = getenv("YAO_ADJ_SEGMENTS");
+    return !(e && e[0] == '0');
+}
+
+// The steps of a pass re-sequenced for register segments: a scan in sweep
+// order emits every ready 1-qubit step whose target is one of the current
+// segment's two bits (or becomes its second); when a scan emits nothing the
+// segment closes and the next one starts at the first remaining step (a
+// 2-qubit step is emitted alone).  A step is ready when no earlier
+// remaining step of the pass shares a qubit with it, so the dependencies of
+// the sweep hold.
+static std::vector<size_t> segment_order(const std::vector<HostOp>& hops, const std::vector<uint64_t>& qm,
+                                         const std::vector<size_t>& take) {
+    std::vector<size_t> order;
+    order.reserve(take.size());
+    std::vector<char> done(take.size(), 0);
+    size_t left = take.size();
+    int sb[2] = {-1, -1}, nsb = 0;
+    while (left) {
+        bool emitted = false;
+        uint64_t blocked = 0;
+        for (size_t i = 0; i < take.size(); i++) {
+            if (done[i]) continue;
+            const HostOp& h = hops[take[i]];
+            const uint64_t m = qm[take[i]];
+            if (m & blocked) {
+                blocked |= m;
+                continue;
+            }
+            bool fit = false;
+            if (h.op.k == 1) {
+                const int t = h.tb[0];
+                if (t == sb[0] || t == sb[1]) {
+                    fit = true;
+                } else if (nsb < 2) {
+                    sb[nsb++] = t;
+                    fit = true;
+                }
+            }
+            if (!fit) {
+                blocked |= m;
+                continue;
+            }
+            order.push_back(take[i]);
+            done[i] = 1;
+            left--;
+            emitted = true;
+        }
+        if (emitted) continue;
+        sb[0] = sb[1] = -1;
+        nsb = 0;
+        for (size_t i = 0; i < take.size(); i++)
+            if (!done[i]) {
+                if (hops[take[i]].op.k == 2) {
+                    order.push_back(take[i]);
+                    done[i] = 1;
+                    left--;
+                }
+                break;
+            }
+    }
+    return order;
+}
+
+// Barriers and segments of a pass's ops.  Segments (on): maximal runs of
+// 1-qubit ops on at most two local positions, seg[] = those positions (a
+// second one added when the run uses one), a barrier after the last.  Runs
+// of 2-qubit ops (and, segments off, of 1-qubit ops) on the same positions
+// share a barrier up to kAdjRun ops; fused ops stand alone.
+static void mark_barriers(std::vector<AdjTileOp>& ops, bool seg) {
+    size_t i = 0;
+    while (i < ops.size()) {
+        if (seg && ops[i].k == 1) {
+            int P[2] = {ops[i].tl[0], -1};
+            size_t j = i + 1;
+            for (; j < ops.size() && ops[j].k == 1; j++) {
+                const int t = ops[j].tl[0];
+                if (t == P[0] || t == P[1]) continue;
+                if (P[1] >= 0) break;
+                P[1] = t;
+            }
+            if (P[1] < 0) P[1] = P[0] == 0 ? 1 : 0;
+            const int lo = std::min(P[0], P[1]), hi = std::max(P[0], P[1]);
+            for (size_t q = i; q < j; q++) {
+                ops[q].seg[0] = (int8_t)lo;
+                ops[q].seg[1] = (int8_t)hi;
+                ops[q].sync = (int8_t)(q + 1 == j ? 1 : 0);
+            }
+            i = j;
+            continue;
+        }
+        ops[i].seg[0] = ops[i].seg[1] = 0;
+        size_t j = i + 1;
+        if (ops[i].cls != kAdjFused)
+            while (j < ops.size() && (int)(j - i) < kAdjRun && ops[j].cls != kAdjFused && ops[j].k == ops[i].k &&
+                   ops[j].tl[0] == ops[i].tl[0] && (ops[i].k == 1 || ops[j].tl[1] == ops[i].tl[1]) &&
+                   !(seg && ops[j].k == 1)) {
+                ops[j].seg[0] = ops[j].seg[1] = 0;
+                ops[j - 1].sync = 0;
+                j++;
+            }
+        ops[j - 1].sync = 1;
+        i = j;
+    }
+}
+
 // Passes by list scheduling over the reverse sweep's dependencies.  Steps
 // on disjoint qubits (targets and controls) commute exactly (in
 // arithmetic they differ by rounding only), and a generator dot taken
@@ -653,6 +905,7 @@ void plan_adj(const std::vector<HostOp>& hops, uint32_t nbits, std::vector<AdjPa
         }
         for (size_t j : take) used[j] = 1;
         while (first < hops.size() && used[first]) first++;
+        if (segments_on()) take = segment_order(hops, qm, take);
         // the tile's scattered bits: the targets', then the lowest free bits
         for (int b = nlow; (int)H.size() < S && b < (int)nbits; b++) H.insert(b);
         AdjPass pass;
@@ -692,23 +945,7 @@ void plan_adj(const std::vector<HostOp>& hops, uint32_t nbits, std::vector<AdjPa
             pass.ops.push_back(op);
         }
         fuse_runs(pass.ops);
-        // a thread owns the same groups in consecutive ops on the same
-        // target positions (controls only skip groups): a barrier is needed
-        // only before an op that moves amplitudes along other bits
-        int run = 0;
-        for (size_t q = 0; q < pass.ops.size(); q++) {
-            AdjTileOp& a = pass.ops[q];
-            bool same = false;
-            if (q + 1 < pass.ops.size()) {
-                const AdjTileOp& b = pass.ops[q + 1];
-                same = a.k == b.k && a.tl[0] == b.tl[0] && (a.k == 1 || a.tl[1] == b.tl[1]);
-            }
-            run++;
-            if (run >= kAdjRun || a.cls == kAdjFused || (q + 1 < pass.ops.size() && pass.ops[q + 1].cls == kAdjFused))
-                same = false;
-            a.sync = (int8_t)(same ? 0 : 1);
-            if (a.sync) run = 0;
-        }
+        mark_barriers(pass.ops, segments_on());
         pass.hdr.nops = (int32_t)pass.ops.size();
         pass.hdr.nslots = (int32_t)pass.slot_grad.size();
         out.push_back(std::move(pass));

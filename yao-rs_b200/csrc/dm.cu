@@ -412,6 +412,68 @@ __global__ void __launch_bounds__(kDCT, 2) k_dm_channel_xor(double2* __restrict_
     }
 }
 
+// 1-qubit channels whose every Kraus operator has at most one non-zero
+// entry per row (and so its conjugate: amplitude and phase damping, resets,
+// and the Pauli channels): the 2 x 2 group stays in registers and each
+// branch entry (a, b) is the one original entry it depends on, chosen by a
+// select, times the two coefficients — k_dm_channel's monomial path with
+// the same operations on the same values, a zero row contributing nothing.
+__device__ __forceinline__ double2 pick2(const double2 (&x)[2][2], int r, int c) {
+    const double2 a = c ? x[0][1] : x[0][0];
+    const double2 b = c ? x[1][1] : x[1][0];
+    return r ? b : a;
+}
+
+__global__ void __launch_bounds__(kDCT, 2) k_dm_channel_mono1(double2* __restrict__ rho, uint64_t ngroups,
+                                                              const __grid_constant__ DMChan op) {
+    __shared__ double2 smr[kMaxKraus * 4], smc[kMaxKraus * 4];
+    __shared__ int8_t sp[kMaxKraus][4];  // row sources of rows 0, 1, column sources of columns 0, 1
+    for (int i = threadIdx.x; i < op.nk * 4; i += blockDim.x) {
+        smr[i] = op.kr[i];
+        smc[i] = op.kc[i];
+    }
+    for (int q = threadIdx.x; q < op.nk; q += blockDim.x) {
+        const bool diag = op.cls[q] == GC_DIAG;
+        sp[q][0] = diag ? 0 : op.perm[q][0][0];
+        sp[q][1] = diag ? 1 : op.perm[q][0][1];
+        sp[q][2] = diag ? 0 : op.perm[q][1][0];
+        sp[q][3] = diag ? 1 : op.perm[q][1][1];
+    }
+    __syncthreads();
+    GRID_STRIDE(g, ngroups) {
+        const uint64_t base = insert_zeros(g, op.locked, op.nlocked);
+        double2 x[2][2], acc[2][2];
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                x[a][b] = rho[base + op.roff[a] + op.coff[b]];
+                acc[a][b] = make_double2(0.0, 0.0);
+            }
+        for (int q = 0; q < op.nk; q++) {
+            const double2* mr = smr + q * 4;
+            const double2* mc = smc + q * 4;
+#pragma unroll
+            for (int a = 0; a < 2; a++) {
+                const int ra = sp[q][a];
+                if (ra < 0) continue;
+                const double2 cr = mr[a * 2 + ra];
+#pragma unroll
+                for (int b = 0; b < 2; b++) {
+                    const int cb = sp[q][2 + b];
+                    if (cb < 0) continue;
+                    const double2 y = cmul_sparse(mc[b * 2 + cb], cmul_sparse(cr, pick2(x, ra, cb)));
+                    acc[a][b] = cadd_x(acc[a][b], y);
+                }
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++) rho[base + op.roff[a] + op.coff[b]] = acc[a][b];
+    }
+}
+
 // Column of the single non-zero entry of each row of a d x d matrix (-1 for
 // a zero row); false when some row has two or more.
 static bool monomial_rows(const std::vector<Cx>& m, int d, int8_t* perm) {
@@ -502,6 +564,14 @@ int launch_dm_channel(Ctx* ctx, DM* d, const std::vector<LGate>& rows, const std
     }
     bool dense = false;
     for (int q = 0; q < nk; q++) dense |= op.cls[q] != GC_DIAG && !op.mono[q];
+    // 1-qubit channels of diagonal and row-monomial operators: registers
+    // (YAO_DM_MONO=0: the shared-memory form)
+    if (k == 1 && !dense && !(getenv("YAO_DM_MONO") && getenv("YAO_DM_MONO")[0] == '0')) {
+        k_dm_channel_mono1<<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);
+        ctx->launches++;
+        YAO_CUDA(cudaGetLastError());
+        return YAO_OK;
+    }
     if (k == 1)
         dense ? k_dm_channel<1, true><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op)
               : k_dm_channel<1, false><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);

@@ -326,17 +326,20 @@ constexpr int kTcVarXlRound = 1, kTcVarSplitAcc = 2, kTcVarB3 = 4, kTcVarInt8 = 
 // Integer form of the tensor-core block.  The tensor cores' FP32
 // accumulation truncates (every accumulation step biases the sum toward
 // zero, so the norm shrinks block by block); integer MMAs accumulate
-// exactly.  X (the tile's amplitudes) is scaled by a power of two 2^(20 - e)
+// exactly.  X (the tile's amplitudes) is scaled by a power of two 2^(27 - e)
 // with 2^e above the tile's largest |x| and rounded to the nearest integer
-// (|q| <= 2^20), then written as three balanced base-2^7 digits
-// q = d0 2^14 + d1 2^7 + d2 (|d| <= 64, int8).  B (|b| <= 1) is rounded to
-// 2^-34 on the host, five digits b 2^34 = e0 2^28 + ... + e4.  The products
-// d_i e_j are summed exactly in int32 per level L = i + j (accumulator L,
-// TMEM columns 64 L): levels 0..2 complete, level 3 and 4 only d0 e3, d0 e4
-// (the other terms are below 2^-21 of the result).  The read-back combines
-// y = 2^e (A0 2^-12 + A1 2^-19 + A2 2^-26 + A3 2^-33 + A4 2^-40) with two
-// FP32 roundings to nearest: every rounding of the block is unbiased.
-constexpr int kTc8XDigits = 3, kTc8BDigits = 5;
+// (|q| < 2^27; exact for every amplitude within 2^3 of the largest, since
+// an FP32 value has 24 significant bits), then written as four balanced
+// base-2^7 digits q = d0 2^21 + d1 2^14 + d2 2^7 + d3 (|d| <= 64, int8).  B
+// (|b| <= 1) is rounded to 2^-34 on the host, five digits b 2^34 = e0 2^28 +
+// ... + e4.  The products d_i e_j are summed exactly in int32 per level
+// L = i + j <= 3 (accumulator L, TMEM columns 64 L; 10 products), and
+// y = 2^(e - 12) (A0 + A1 2^-7 + A2 2^-14 + A3 2^-21) is formed exactly in
+// 64-bit integers and rounded to FP32 once (to nearest).  Levels 4 and above
+// weigh below 2^-30 of the block's largest output and are left out: a
+// level's K = 64 sum of digit products reaches 2^15 and more, so every
+// level up to 3 is kept whole.
+constexpr int kTc8XDigits = 4, kTc8BDigits = 5;
 constexpr uint32_t kTc8Sbo = (kTcKr / 16) * 128;       // bytes between 8-row groups (64 int8 a row)
 constexpr uint32_t kTc8XDigit = kTcRows * kTcKr;       // bytes of one X digit array
 constexpr uint32_t kTc8BDigit = kTcN * kTcKr;          // bytes of one B digit array
@@ -508,15 +511,17 @@ __device__ __forceinline__ uint32_t tc8_off(uint32_t r, uint32_t k) {
     return (r >> 3) * kTc8Sbo + (k >> 4) * 128 + (r & 7) * 16 + (k & 15);
 }
 
-__device__ __forceinline__ uint32_t tc8_digits(int q, int c, uint32_t (&w)[kTc8XDigits]) {
-    const int d0 = (q + 8192) >> 14;
-    const int r0 = q - (d0 << 14);
-    const int d1 = (r0 + 64) >> 7;
-    const int d2 = r0 - (d1 << 7);
+__device__ __forceinline__ void tc8_digits(int q, int c, uint32_t (&w)[kTc8XDigits]) {
+    const int d0 = (q + (1 << 20)) >> 21;
+    const int r0 = q - (d0 << 21);
+    const int d1 = (r0 + (1 << 13)) >> 14;
+    const int r1 = r0 - (d1 << 14);
+    const int d2 = (r1 + 64) >> 7;
+    const int d3 = r1 - (d2 << 7);
     w[0] |= (uint32_t)(uint8_t)(int8_t)d0 << (8 * c);
     w[1] |= (uint32_t)(uint8_t)(int8_t)d1 << (8 * c);
     w[2] |= (uint32_t)(uint8_t)(int8_t)d2 << (8 * c);
-    return 0;
+    w[3] |= (uint32_t)(uint8_t)(int8_t)d3 << (8 * c);
 }
 
 template <typename V>
@@ -559,8 +564,8 @@ __device__ __noinline__ void wide_tc8(const TOp& op, V* s, TcCtx& tc) {
         }
         __syncthreads();
         const int e = sexp;
-        const float f = ldexpf(1.f, 20 - e);
-        // 2. X as three int8 digit arrays (row g = group, 64 bytes a row)
+        const float f = ldexpf(1.f, 27 - e);
+        // 2. X as four int8 digit arrays (row g = group, 64 bytes a row)
         unsigned char* xd = (unsigned char*)tc.xh;
         const uint32_t g = tid & (kTcRows - 1);
         uint32_t gb = g;
@@ -569,7 +574,7 @@ __device__ __noinline__ void wide_tc8(const TOp& op, V* s, TcCtx& tc) {
         for (uint32_t jp = tid >> 7; jp < 16; jp += nt >> 7) {
             const float2 v0 = t[swz(gb | co[2 * jp], (float2*)nullptr)];
             const float2 v1 = t[swz(gb | co[2 * jp + 1], (float2*)nullptr)];
-            uint32_t w[kTc8XDigits] = {0, 0, 0};
+            uint32_t w[kTc8XDigits] = {0, 0, 0, 0};
             tc8_digits(__float2int_rn(v0.x * f), 0, w);
             tc8_digits(__float2int_rn(v0.y * f), 1, w);
             tc8_digits(__float2int_rn(v1.x * f), 2, w);
@@ -581,7 +586,7 @@ __device__ __noinline__ void wide_tc8(const TOp& op, V* s, TcCtx& tc) {
         tc::fence_proxy_async();
         tc::fence_before_sync();
         __syncthreads();
-        // 3. one thread issues the MMAs: 8 digit products x 2 K-steps
+        // 3. one thread issues the MMAs: 10 digit products x 2 K-steps
         bool b_ok = true;
         if (need_b) {
             tc.loaded = op.mma;
@@ -602,10 +607,10 @@ __device__ __noinline__ void wide_tc8(const TOp& op, V* s, TcCtx& tc) {
                 constexpr uint32_t idesc = tc::idesc_i8(kTcRows, kTcN);
                 const uint32_t xa = tc::smem_u32(xd), ba = tc::smem_u32(bslot);
                 // (X digit, B digit, level): first product of each level initialises it
-                const int prod[8][3] = {{0, 0, 0}, {0, 1, 1}, {1, 0, 1}, {0, 2, 2},
-                                        {1, 1, 2}, {2, 0, 2}, {0, 3, 3}, {0, 4, 4}};
+                const int prod[10][3] = {{0, 0, 0}, {0, 1, 1}, {1, 0, 1}, {0, 2, 2}, {1, 1, 2},
+                                         {2, 0, 2}, {0, 3, 3}, {1, 2, 3}, {2, 1, 3}, {3, 0, 3}};
 #pragma unroll
-                for (int p = 0; p < 8; p++) {
+                for (int p = 0; p < 10; p++) {
                     const int i = prod[p][0], j = prod[p][1], L = prod[p][2];
                     const bool first = p == 0 || prod[p - 1][2] != L;
 #pragma unroll
@@ -644,20 +649,20 @@ __device__ __noinline__ void wide_tc8(const TOp& op, V* s, TcCtx& tc) {
             const uint32_t c0 = (warp >> 2) * cpw;
             const uint32_t lane_base = tc.tmem + ((((warp & 3) << 5)) << 16);
             for (uint32_t c = c0; c < c0 + cpw; c += 16) {
-                uint32_t r0[16], r1[16], r2[16], r3[16], r4[16];
+                uint32_t r0[16], r1[16], r2[16], r3[16];
                 tc::tmem_ld16(lane_base + c, r0);
                 tc::tmem_ld16(lane_base + 64 + c, r1);
                 tc::tmem_ld16(lane_base + 128 + c, r2);
                 tc::tmem_ld16(lane_base + 192 + c, r3);
-                tc::tmem_ld16(lane_base + 256 + c, r4);
                 tc::tmem_wait_ld();
                 float y[16];
 #pragma unroll
                 for (int i = 0; i < 16; i++) {
-                    const int H = (int)r0[i] * 128 + (int)r1[i];
-                    const int Lo = (int)r2[i] * 128 + (int)r3[i];
-                    const float v = fmaf((float)(int)r4[i], 0x1p-21f, fmaf((float)Lo, 0x1p-14f, (float)H));
-                    y[i] = ldexpf(v, e - 19);
+                    // 2^(e-33) (H 2^14 + Lo), H = A0 2^7 + A1, Lo = A2 2^7 + A3:
+                    // exact in 64 bits (|.| < 2^41), one rounding to FP32
+                    const long long H = (long long)(int)r0[i] * 128 + (int)r1[i];
+                    const long long Lo = (long long)(int)r2[i] * 128 + (int)r3[i];
+                    y[i] = (float)ldexp((double)(H * 16384 + Lo), e - 33);
                 }
 #pragma unroll
                 for (int i = 0; i < 8; i++)
@@ -1101,7 +1106,7 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
             tc::mbar_init(&tc_bbar, 1);
         }
         if (threadIdx.x < 32) {
-            tc::tmem_alloc(&tc_tmem, hdr.tc_variant & kTcVarInt8 ? 512u : (uint32_t)kTcCols);
+            tc::tmem_alloc(&tc_tmem, hdr.tc_variant & kTcVarInt8 ? 256u : (uint32_t)kTcCols);
             tc::tmem_relinquish();
         }
         tc::fence_before_sync();
@@ -1235,7 +1240,7 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         __syncthreads();
         if (threadIdx.x < 32) {
             tc::fence_after_sync();
-            tc::tmem_dealloc(tcx.tmem, tcx.variant & kTcVarInt8 ? 512u : (uint32_t)kTcCols);
+            tc::tmem_dealloc(tcx.tmem, tcx.variant & kTcVarInt8 ? 256u : (uint32_t)kTcCols);
         }
     }
 }
@@ -1428,6 +1433,12 @@ static void plan_segments(PassPlan& pp, int rb, bool pair0 = false) {
 }
 
 // Bits a gate moves amplitudes along (DIAG moves none).
+// YAO_PASS_REORDER=0: FUSED passes keep program order too
+static bool pass_reorder() {
+    const char* e = getenv("YAO_PASS_REORDER");
+    return !(e && e[0] == '0');
+}
+
 static uint64_t moving_mask(const LGate& g) {
     uint64_t m = 0;
     if (g.cls == GC_DIAG) return 0;
@@ -1436,35 +1447,60 @@ static uint64_t moving_mask(const LGate& g) {
 }
 
 // Split a gate list into passes: each pass is a maximal contiguous run whose
-// moving bits fit in `tbits` tile bits together with the low bits.
-static void plan_passes(const std::vector<LGate>& prog, uint32_t nbits, int tbits_max, std::vector<PassPlan>& out) {
+// moving bits fit in `tbits` tile bits together with the low bits.  With
+// `reorder` (FUSED runs) a pass is list-scheduled instead: the scan takes
+// every gate that no skipped earlier gate shares a qubit with (targets or
+// controls), so gates on disjoint qubits may run before gates they commute
+// with; the arithmetic then differs from program order by rounding only.
+// TILED runs keep program order (bit-identical to PLAIN).
+static void plan_passes(const std::vector<LGate>& prog, uint32_t nbits, int tbits_max, std::vector<PassPlan>& out,
+                        bool reorder = false) {
     int tbits = std::min<int>((int)nbits, tbits_max);
+    const uint64_t all = nbits >= 64 ? ~0ull : ((1ull << nbits) - 1);
+    std::vector<char> used(prog.size(), 0);
     size_t i = 0;
     while (i < prog.size()) {
         uint64_t hi = 0;  // moving bits of the run
         PassPlan pp;
         std::vector<const LGate*> run;
-        size_t j = i;
         // The tile is bits 0..3 (runs of >= 16 consecutive amplitudes per
         // load), the moving bits and the lowest other bits, tbits in total:
         // at most tbits - 4 moving bits outside bits 0..3.
         const bool whole = (int)nbits <= tbits;
-        for (; j < prog.size(); j++) {
+        uint64_t blocked = 0;
+        for (size_t j = i; j < prog.size(); j++) {
+            if (used[j]) continue;
+            uint64_t qm = moving_mask(prog[j]);
+            for (int q = 0; q < prog[j].k; q++) qm |= (uint64_t)1 << prog[j].tb[q];
+            for (int c = 0; c < prog[j].nc; c++) qm |= (uint64_t)1 << prog[j].cb[c];
+            if (qm & blocked) {
+                blocked |= qm;
+                if ((blocked & all) == all) break;
+                continue;
+            }
             const uint64_t mb = moving_mask(prog[j]);
             const uint64_t nh = hi | mb;
-            const int used = whole ? __builtin_popcountll(nh) : __builtin_popcountll(nh & ~(uint64_t)0xF);
-            if (used > (whole ? (int)nbits : tbits - 4) || __builtin_popcountll(mb) > kMaxTargets) break;
+            const int nused = whole ? __builtin_popcountll(nh) : __builtin_popcountll(nh & ~(uint64_t)0xF);
+            if (nused > (whole ? (int)nbits : tbits - 4) || __builtin_popcountll(mb) > kMaxTargets) {
+                if (!reorder) break;
+                blocked |= qm;
+                if ((blocked & all) == all) break;
+                continue;
+            }
             hi = nh;
             run.push_back(&prog[j]);
+            used[j] = 1;
         }
         if (run.empty()) {
             PassPlan sp;
             sp.single = true;
             sp.gate = prog[i];
             out.push_back(sp);
-            i++;
+            used[i] = 1;
+            while (i < prog.size() && used[i]) i++;
             continue;
         }
+        while (i < prog.size() && used[i]) i++;
         uint64_t tile = whole ? hi : (hi | (uint64_t)0xF);
         for (int b = 0; __builtin_popcountll(tile) < tbits && b < (int)nbits; b++) tile |= (uint64_t)1 << b;
         std::vector<int> TB;
@@ -1521,7 +1557,6 @@ static void plan_passes(const std::vector<LGate>& prog, uint32_t nbits, int tbit
         }
         pp.hdr.nops = (int32_t)pp.ops.size();
         out.push_back(pp);
-        i = j;
     }
 }
 
@@ -2072,6 +2107,7 @@ struct TileConfig {
     int k = 0;
     int tbits = 0;
     int rb = 0;
+    int tc = 1;  // complex64 FUSED: dense 3..5-qubit blocks may go to the tensor cores
 };
 
 // FP32 -> TF32, round to nearest even (low 13 mantissa bits cleared)
@@ -2143,17 +2179,18 @@ static void tc_prepare(PassPlan& pp) {
     }
 }
 
+// The host plan of a TILED / FUSED run: passes (fused blocks, tile shapes,
+// register segments, tensor-core operands).
 template <typename V>
-static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, const std::vector<LGate>& prog,
-                           int32_t mode, const TileConfig& cfg, bool check_err = true) {
+static void plan_run(uint32_t nbits, const std::vector<LGate>& prog, int32_t mode, const TileConfig& cfg,
+                     std::vector<PassPlan>& passes, bool* any_tc) {
     std::vector<LGate> work;
-    const bool exact = (mode == YAO_MODE_TILED) && sizeof(V) == 16;
     if (mode == YAO_MODE_FUSED)
         fuse_blocks(prog, nbits, std::min(cfg.k, kMaxTargets), work);
     else
         work = prog;
-    std::vector<PassPlan> passes;
-    plan_passes(work, nbits, cfg.tbits, passes);
+    passes.clear();
+    plan_passes(work, nbits, cfg.tbits, passes, mode == YAO_MODE_FUSED && pass_reorder());
     for (PassPlan& pp : passes)
         if (!pp.single) {
             // at most kTileThreads threads per tile
@@ -2161,19 +2198,27 @@ static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, c
             const int rb = std::max(tb - 9, std::min(cfg.rb, tb));
             plan_segments(pp, std::min(rb, max_reg_bits<V>()), sizeof(V) == 8);
         }
-    // dense 5-qubit blocks of complex64 FUSED runs go to the tensor cores
-    // (YAO_TC=0 keeps them on the CUDA cores)
-    bool any_tc = false;
-    if (sizeof(V) == 8 && mode == YAO_MODE_FUSED) {
+    // dense 3..5-qubit blocks of complex64 FUSED runs go to the tensor cores
+    // (cfg.tc; YAO_TC=0 keeps them on the CUDA cores)
+    *any_tc = false;
+    if (sizeof(V) == 8 && mode == YAO_MODE_FUSED && cfg.tc) {
         const char* e = getenv("YAO_TC");
         if (!(e && e[0] == '0'))
             for (PassPlan& pp : passes)
                 if (!pp.single) {
                     tc_prepare(pp);
-                    any_tc |= pp.hdr.mma != 0;
+                    *any_tc |= pp.hdr.mma != 0;
                 }
     }
-    for (const PassPlan& pp : passes) {
+}
+
+// Launches passes[first], passes[first + step], ... of a plan.
+template <typename V>
+static int launch_passes(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, int32_t mode,
+                         const std::vector<PassPlan>& passes, size_t first = 0, size_t step = 1) {
+    const bool exact = (mode == YAO_MODE_TILED) && sizeof(V) == 16;
+    for (size_t i = first; i < passes.size(); i += step) {
+        const PassPlan& pp = passes[i];
         int s;
         if (pp.single)
             s = launch_gate(ctx, st, precision, nbits, pp.gate);
@@ -2183,6 +2228,17 @@ static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, c
             s = run_pass<V, false>(ctx, st, nbits, pp);
         if (s) return s;
     }
+    return YAO_OK;
+}
+
+template <typename V>
+static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, const std::vector<LGate>& prog,
+                           int32_t mode, const TileConfig& cfg, bool check_err = true) {
+    std::vector<PassPlan> passes;
+    bool any_tc = false;
+    plan_run<V>(nbits, prog, mode, cfg, passes, &any_tc);
+    int s = launch_passes<V>(ctx, st, nbits, precision, mode, passes);
+    if (s) return s;
     ctx->tc_used = any_tc;
     // a bounded wait of some pass (a tile's TMA copies, a tensor-core
     // operand copy or MMA completion) gave up: the run's result is void
@@ -2203,12 +2259,15 @@ static int run_program_cfg(Ctx* ctx, V* st, uint32_t nbits, int32_t precision, c
 // ------------------------------------------------------------ autotuner
 //
 // The tile shape (tile bits, register bits) and, for FUSED with k = 0, the
-// fusion width are picked by timing candidates on the device: a prefix of
-// the program (at most 2^39 amplitude-gate updates, at least 64 gates) runs
-// on a scratch copy of the register for every candidate, and the fastest is
+// fusion width (and, for complex64, whether dense blocks go to the tensor
+// cores) are picked by timing candidates on the device.  Every candidate's
+// whole program is planned on the host; an evenly spread sample of its
+// passes (at most kTuneSample, from the start, middle and end of the
+// program alike) runs on a scratch copy of the register, and the sample's
+// time scaled by passes / sampled passes estimates the run.  The fastest is
 // kept per (device, qubits, precision, mode, requested k).  Choices live in
 // memory and, when YAO_TUNE_CACHE names a file, in that file (one
-// "key k tbits rb" line per entry).  YAO_TILE_BITS / YAO_REG_BITS pin the
+// "key k tbits rb tc" line per entry).  YAO_TILE_BITS / YAO_REG_BITS pin the
 // shape and YAO_AUTOTUNE=0 turns tuning off (defaults below).
 
 static std::mutex g_tune_mu;
@@ -2228,9 +2287,11 @@ static void tune_load_locked() {
     if (!path || !*path) return;
     FILE* f = fopen(path, "r");
     if (!f) return;
-    char key[128];
-    TileConfig c;
-    while (fscanf(f, "%127s %d %d %d", key, &c.k, &c.tbits, &c.rb) == 4) g_tune[key] = c;
+    char line[256], key[128];
+    while (fgets(line, sizeof(line), f)) {
+        TileConfig c;
+        if (sscanf(line, "%127s %d %d %d %d", key, &c.k, &c.tbits, &c.rb, &c.tc) == 5) g_tune[key] = c;
+    }
     fclose(f);
 }
 
@@ -2239,7 +2300,8 @@ static void tune_store_locked() {
     if (!path || !*path) return;
     FILE* f = fopen(path, "w");
     if (!f) return;
-    for (const auto& kv : g_tune) fprintf(f, "%s %d %d %d\n", kv.first.c_str(), kv.second.k, kv.second.tbits, kv.second.rb);
+    for (const auto& kv : g_tune)
+        fprintf(f, "%s %d %d %d %d\n", kv.first.c_str(), kv.second.k, kv.second.tbits, kv.second.rb, kv.second.tc);
     fclose(f);
 }
 
@@ -2281,15 +2343,15 @@ static void tile_candidates(uint32_t nbits, std::vector<TileConfig>& out) {
 
 // Time every candidate on a scratch copy of the state; *best receives the
 // fastest (left at the default when no scratch memory is available).
+constexpr size_t kTuneSample = 12;
+
 template <typename V>
 static int tune_program(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t kreq,
                         TileConfig* best, double* best_ms) {
     *best = default_config<V>(mode, kreq);
     *best_ms = -1.0;
     const uint32_t n = r->nbits;
-    const size_t cap = std::max<size_t>(64, (size_t)1 << std::max(0, 39 - (int)n));
-    std::vector<LGate> sample(prog.begin(), prog.begin() + std::min(prog.size(), cap));
-    if (sample.empty()) return YAO_OK;
+    if (prog.empty()) return YAO_OK;
     const size_t bytes = ((size_t)1 << n) * sizeof(V);
     V* scratch = nullptr;
     if (cudaMallocAsync((void**)&scratch, bytes, ctx->stream) != cudaSuccess) {
@@ -2303,13 +2365,33 @@ static int tune_program(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog, 
     YAO_CUDA(cudaEventCreate(&a));
     YAO_CUDA(cudaEventCreate(&b));
     int st = YAO_OK;
-    auto timed = [&](const TileConfig& c, float* ms) -> int {
+    // one plan per candidate (host), then timed samples of its passes
+    struct Cand {
+        TileConfig c;
+        std::vector<PassPlan> passes;
+        size_t first = 0, step = 1, nsample = 0;
+        float best = 0.f;  // estimated ms of the whole run
+    };
+    auto make = [&](const TileConfig& c) {
+        Cand x;
+        x.c = c;
+        bool any_tc = false;
+        plan_run<V>(n, prog, mode, c, x.passes, &any_tc);
+        const size_t P = x.passes.size();
+        x.step = P > kTuneSample ? P / kTuneSample : 1;
+        x.first = P > kTuneSample ? (P - x.step * (kTuneSample - 1)) / 2 : 0;
+        x.nsample = 0;
+        for (size_t i = x.first; i < P; i += x.step) x.nsample++;
+        return x;
+    };
+    auto timed = [&](Cand& x, float* ms) -> int {
         YAO_CUDA(cudaEventRecord(a, ctx->stream));
-        int s = run_program_cfg<V>(ctx, scratch, n, r->precision, sample, mode, c);
+        int s = launch_passes<V>(ctx, scratch, n, r->precision, mode, x.passes, x.first, x.step);
         if (s) return s;
         YAO_CUDA(cudaEventRecord(b, ctx->stream));
         YAO_CUDA(cudaEventSynchronize(b));
         YAO_CUDA(cudaEventElapsedTime(ms, a, b));
+        *ms *= (float)x.passes.size() / (float)std::max<size_t>(1, x.nsample);
         return YAO_OK;
     };
     // Candidates are timed in interleaved rounds (every candidate once per
@@ -2318,60 +2400,77 @@ static int tune_program(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog, 
     // cap the SM clock drifts over seconds; interleaving gives every
     // candidate the same clocks, so a drift does not pick a slower one.
     constexpr int kRounds = 3;
-    // YAO_TUNE_LOG=1: every candidate's best time on stderr
+    // YAO_TUNE_LOG=1: every candidate's estimate on stderr
     const char* tl = getenv("YAO_TUNE_LOG");
     const bool log = tl && tl[0] == '1';
-    auto best_of = [&](const std::vector<TileConfig>& cand, size_t* pick, float* pick_ms) -> int {
-        std::vector<float> bestv(cand.size(), 0.f);
+    auto best_of = [&](std::vector<Cand>& cand, size_t* pick, float* pick_ms) -> int {
         float ms = 0.f;
         for (int round = 0; round <= kRounds; round++)
             for (size_t i = 0; i < cand.size(); i++) {
                 int s = timed(cand[i], &ms);
                 if (s) return s;
-                if (round == 1 || (round > 1 && ms < bestv[i])) bestv[i] = ms;
+                if (round == 1 || (round > 1 && ms < cand[i].best)) cand[i].best = ms;
             }
         *pick = 0;
         for (size_t i = 1; i < cand.size(); i++)
-            if (bestv[i] < bestv[*pick]) *pick = i;
-        *pick_ms = bestv[*pick];
+            if (cand[i].best < cand[*pick].best) *pick = i;
+        *pick_ms = cand[*pick].best;
         if (log)
             for (size_t i = 0; i < cand.size(); i++)
-                fprintf(stderr, "[yao tune] n=%u %s mode=%d k=%d tbits=%d rb=%d: %.3f ms over %zu gates%s\n", n,
-                        sizeof(V) == 8 ? "c64" : "c128", mode, cand[i].k, cand[i].tbits, cand[i].rb, bestv[i],
-                        sample.size(), i == *pick ? "  <- chosen" : "");
+                fprintf(stderr,
+                        "[yao tune] n=%u %s mode=%d k=%d tbits=%d rb=%d tc=%d: %.3f ms (%zu of %zu passes timed)%s\n",
+                        n, sizeof(V) == 8 ? "c64" : "c128", mode, cand[i].c.k, cand[i].c.tbits, cand[i].c.rb,
+                        cand[i].c.tc, cand[i].best, cand[i].nsample, cand[i].passes.size(),
+                        i == *pick ? "  <- chosen" : "");
         return YAO_OK;
     };
     std::vector<TileConfig> shapes;
     tile_candidates<V>(n, shapes);
-    std::vector<TileConfig> cand;
+    std::vector<Cand> cand;
     for (const TileConfig& sc : shapes) {
         TileConfig c = *best;
         c.tbits = sc.tbits;
         c.rb = sc.rb;
-        cand.push_back(c);
+        cand.push_back(make(c));
     }
     size_t pick = 0;
     float bms = 0.f;
     st = best_of(cand, &pick, &bms);
-    if (!st) *best = cand[pick];
+    if (!st) *best = cand[pick].c;
     if (!st && mode == YAO_MODE_FUSED && kreq <= 0) {
-        // widths 2..6 with the chosen shape (tensor-core widths with the 2^12
-        // tile they need), the chosen configuration among them
+        // widths 2..6 with the chosen shape; complex64 widths 3..5 also
+        // with the tensor cores' 2^12 tile, on and off the tensor cores
         const TileConfig shape = *best;
-        cand.clear();
-        cand.push_back(shape);
+        std::vector<TileConfig> cs;
         for (int k = 2; k <= kMaxTargets; k++) {
-            if (k == shape.k) continue;
             TileConfig c = shape;
             c.k = k;
+            c.tc = 0;
+            cs.push_back(c);
             if (sizeof(V) == 8 && k >= 3 && k <= kTcK) {
                 c.tbits = kTcTileBits;
                 c.rb = 3;
+                c.tc = 1;
+                cs.push_back(c);
             }
-            cand.push_back(c);
         }
+        cand.clear();
+        for (const TileConfig& c : cs) cand.push_back(make(c));
         st = best_of(cand, &pick, &bms);
-        if (!st) *best = cand[pick];
+        if (!st) *best = cand[pick].c;
+    } else if (!st && mode == YAO_MODE_FUSED && sizeof(V) == 8 && kreq >= 3 && kreq <= kTcK) {
+        // a requested complex64 width: the tensor cores' 2^12 tile against the
+        // chosen shape on the CUDA cores
+        TileConfig on = *best, off = *best;
+        on.tbits = kTcTileBits;
+        on.rb = 3;
+        on.tc = 1;
+        off.tc = 0;
+        cand.clear();
+        cand.push_back(make(on));
+        cand.push_back(make(off));
+        st = best_of(cand, &pick, &bms);
+        if (!st) *best = cand[pick].c;
     }
     ctx->prof = prof;
     cudaEventDestroy(a);
@@ -2456,7 +2555,7 @@ int plan_info(const std::vector<LGate>& prog, uint32_t nbits, int32_t precision,
         work = prog;
     info[6] = (int64_t)work.size();
     std::vector<PassPlan> passes;
-    plan_passes(work, nbits, tbits, passes);
+    plan_passes(work, nbits, tbits, passes, mode == YAO_MODE_FUSED && pass_reorder());
     const int maxrb = precision == YAO_C128 ? max_reg_bits<double2>() : max_reg_bits<float2>();
     for (PassPlan& pp : passes) {
         info[0]++;
@@ -2479,7 +2578,7 @@ int plan_info(const std::vector<LGate>& prog, uint32_t nbits, int32_t precision,
     return YAO_OK;
 }
 
-int autotune_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k, int32_t out[3]) {
+int autotune_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k, int32_t out[4]) {
     TileConfig c;
     int s = r->precision == YAO_C128 ? choose_config<double2>(ctx, r, prog, mode, k, true, &c)
                                      : choose_config<float2>(ctx, r, prog, mode, k, true, &c);
@@ -2487,6 +2586,7 @@ int autotune_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t m
     out[0] = c.k;
     out[1] = c.tbits;
     out[2] = c.rb;
+    out[3] = c.tc;
     return YAO_OK;
 }
 
@@ -2522,7 +2622,8 @@ static int batch_t(Ctx* ctx, const std::vector<const std::vector<LGate>*>& progs
         std::vector<LGate> work;
         if (mode == YAO_MODE_FUSED)
             fuse_blocks(*progs[c], regs[c]->nbits, std::max(1, std::min(k, kMaxTargets)), work);
-        plan_passes(mode == YAO_MODE_FUSED ? work : *progs[c], regs[c]->nbits, tbits_cap, plans[c]);
+        plan_passes(mode == YAO_MODE_FUSED ? work : *progs[c], regs[c]->nbits, tbits_cap, plans[c],
+                    mode == YAO_MODE_FUSED && pass_reorder());
         for (PassPlan& pp : plans[c]) {
             if (pp.single) bad[c] = 1;
             else if (pp.hdr.tbits - pp.hdr.m > kMaxScatterBits) bad[c] = 2;

@@ -197,7 +197,7 @@ int launch_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mod
 int read_device_err(Ctx* ctx, const char* what);
 // Time TILED / FUSED candidates for this program and register (always
 // re-tunes); out = {k, tile bits, register bits}.
-int autotune_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k, int32_t out[3]);
+int autotune_program(Ctx* ctx, Reg* r, const std::vector<LGate>& prog, int32_t mode, int32_t k, int32_t out[4]);
 // Host-only plan of a TILED / FUSED run (see yao_plan_info).
 int plan_info(const std::vector<LGate>& prog, uint32_t nbits, int32_t precision, int32_t mode, int32_t k,
               int32_t tbits, int32_t rb, int64_t info[7]);

@@ -30,9 +30,9 @@ def apply(circuit, reg: ArrayReg, mode: int = A.MODE_PLAIN, k: int = 0) -> Array
 def autotune(circuit, reg: ArrayReg, mode: int = A.MODE_FUSED, k: int = 0) -> dict:
     """Time the TILED / FUSED execution choices for this circuit on a scratch
     copy of `reg` and keep the fastest for later calls; returns the choice."""
-    out = (C.c_int32 * 3)()
+    out = (C.c_int32 * 4)()
     A.check(A.lib().yao_autotune(circuit.handle, reg.handle, mode, k, out))
-    return {"k": out[0], "tile_bits": out[1], "reg_bits": out[2]}
+    return {"k": out[0], "tile_bits": out[1], "reg_bits": out[2], "tensor_cores": out[3]}
 
 
 def plan_info(circuit, precision=A.C128, mode=A.MODE_FUSED, k=5, tile_bits=12, reg_bits=3) -> dict:
