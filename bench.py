@@ -772,7 +772,7 @@ def summary(x, plain_s, first_gates):
     kern = {k["kernel"]: k["GBps"] for k in d["kernels"]}
     s["dm14"] = {"plain_s": d["s_per_circuit"], "fused_s": d["fused_superop"]["s_per_circuit"],
                  "purity": d["purity"], "fused_max_z_diff": d["fused_superop"]["max_z_diff"],
-                 "kernel_GBps": kern,
+                 "kernel_GBps": kern, "channel_passes_GBps": d["channel_passes_GBps"],
                  "fused_kernel_GBps": {k["kernel"]: k["GBps"] for k in d["fused_superop"]["kernels"]},
                  "n12_layer_vs_oracle": d["n12_layer_vs_oracle"]["max_abs_diff"]}
     q = x["qft20"]
@@ -966,10 +966,14 @@ def dm_extra(Y, A, torch, stream, dev, timed):
     prof = A.profile_report(dev)
     A.profile(False, dev)
     zs = [Y.expect_dm(d, Y.OperatorPolynomial.single(i, Y.Op.Z, 1.0)).real for i in range(n)]
+    chans = [p for p in prof if p["kernel"].startswith("dm_channel")]
     res = {"qubits": n, "layers": layers, "elements": len(c.elements), "s_per_circuit": t,
            "purity": d.purity(), "trace_re": d.trace().real, "z": zs,
            "kernels": [{"kernel": p["kernel"], "launches": p["launches"], "ms": round(p["ms"], 2),
-                        "GBps": round(p["bytes"] / (p["ms"] / 1e3) / 1e9, 1)} for p in prof]}
+                        "GBps": round(p["bytes"] / (p["ms"] / 1e3) / 1e9, 1)} for p in prof],
+           # every channel pass together (Pauli-type, row-monomial and general kernels)
+           "channel_passes_GBps": round(sum(p["bytes"] for p in chans) / (sum(p["ms"] for p in chans) / 1e3) / 1e9, 1)
+           if chans else None}
     # FUSED form: rho as a 28-qubit vector through the fused tile passes,
     # channels as superoperators
     f = Y.DensityMatrix.zero_state(n, device=dev)

@@ -528,11 +528,13 @@ def test_density_matrix_bit_exact(n):
     assert maxdiff(Y.probs(d, [n - 1, 0] if n > 1 else [0]), O.dm_probs(ref, n, [n - 1, 0] if n > 1 else [0])) == 0.0
 
 
-@pytest.mark.parametrize("paths", [{"YAO_DM_MONO": "0"}, {"YAO_DM_MONO": "0", "YAO_DM_XOR": "0"}])
+@pytest.mark.parametrize("paths", [{}, {"YAO_DM_XOR2H": "0"}, {"YAO_DM_MONO": "0"},
+                                   {"YAO_DM_MONO": "0", "YAO_DM_XOR": "0"}])
 def test_density_matrix_channel_kernels_agree(monkeypatch, paths):
     """Every channel kernel is bit-exact against the oracle: the register
-    forms (1-qubit row-monomial channels, Pauli-type XOR channels) and, with
-    them switched off, the shared-memory Kraus-sum kernel."""
+    forms (1-qubit row-monomial channels, Pauli-type XOR channels, 2-qubit
+    ones with one or two threads per group) and, with them switched off, the
+    shared-memory Kraus-sum kernel."""
     for k, v in paths.items():
         monkeypatch.setenv(k, v)
     n = 6

@@ -46,7 +46,9 @@ constexpr int kAdjMaxSlots = 48;    // generator dots per pass
 constexpr int32_t kAdjFused = 16;
 constexpr int kAdjFusedGens = 3;
 
-struct AdjTileOp {
+// The control fields of an op: 64 bytes, 16-byte aligned, so the register
+// segments copy them into registers with four 16-byte loads per op.
+struct __align__(16) AdjOpCtl {
     int32_t gen;     // 1: accumulate Re <lambda | G psi> into `slot`; 0: U^dagger on psi and lambda
     int32_t cls;     // GC_X / GC_SWAP / GC_DIAG / GC_DENSE (generators: GC_DENSE), or kAdjFused
     int32_t k;       // 1 or 2 targets
@@ -60,10 +62,14 @@ struct AdjTileOp {
     int32_t a_id;    // kAdjFused: A is the identity (no U^dagger in the run)
     uint32_t lcmask, lcval;  // in-tile controls (local positions)
     uint64_t gcmask, gcval;  // out-of-tile controls (global bits)
+};
+static_assert(sizeof(AdjOpCtl) == 64, "the control fields are four 16-byte words");
+
+struct AdjTileOp : AdjOpCtl {
     uint64_t active;         // DIAG: entries different from 1
     double2 m[16];           // dense 2^k x 2^k row-major, or the 2^k diagonal entries
 };
-static_assert(sizeof(AdjTileOp) % 8 == 0, "AdjTileOp is staged as 64-bit words");
+static_assert(sizeof(AdjTileOp) % 16 == 0, "AdjTileOp is staged as 64-bit words, 16-byte aligned");
 
 struct AdjTileHdr {
     int32_t tbits, nops, nslots, nouts;
@@ -296,35 +302,36 @@ __device__ __forceinline__ void seg_pair_idx(int q, int& a, int& b) {
 }
 
 template <int S>
-__device__ __forceinline__ void seg_op(const AdjTileOp& op, double2 (&x)[4], double2 (&l)[4], const uint32_t (&li)[4],
-                                       double* __restrict__ acc, uint32_t nw, bool valid) {
+__device__ __forceinline__ void seg_op(const AdjOpCtl& c, const AdjTileOp& op, double2 (&x)[4], double2 (&l)[4],
+                                       const uint32_t (&li)[4], double* __restrict__ acc, uint32_t nw, bool valid) {
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (op.cls == kAdjFused) {
-        const int ng = op.ngen;
+    if (c.cls == kAdjFused) {
+        // G'_j = A^dagger G_j A is anti-Hermitian like the generators
+        // (G = -i times a Hermitian matrix; the host folds only such runs):
+        // Re sum_rc G'[r][c] P[r][c] = -Im G'00 Im P00 - Im G'11 Im P11
+        //                              + Re(G'01 (P01 - conj(P10))),
+        // P[r][c] = conj(l_r) x_c
+        const int ng = c.ngen;
         double dot[kAdjFusedGens] = {0.0, 0.0, 0.0};
+        const bool apply = !c.a_id;
 #pragma unroll
         for (int q = 0; q < 2; q++) {
             int ia, ib;
             seg_pair_idx<S>(q, ia, ib);
             const double2 x0 = x[ia], x1 = x[ib], l0 = l[ia], l1 = l[ib];
             if (valid && ng > 0) {
-                // P[r][c] = conj(l_r) x_c; Re sum G'[r][c] P[r][c]
-                const double2 p00 = make_double2(fma(l0.x, x0.x, l0.y * x0.y), fma(l0.x, x0.y, -l0.y * x0.x));
-                const double2 p01 = make_double2(fma(l0.x, x1.x, l0.y * x1.y), fma(l0.x, x1.y, -l0.y * x1.x));
-                const double2 p10 = make_double2(fma(l1.x, x0.x, l1.y * x0.y), fma(l1.x, x0.y, -l1.y * x0.x));
-                const double2 p11 = make_double2(fma(l1.x, x1.x, l1.y * x1.y), fma(l1.x, x1.y, -l1.y * x1.x));
+                const double i00 = fma(l0.x, x0.y, -l0.y * x0.x);  // Im P00
+                const double i11 = fma(l1.x, x1.y, -l1.y * x1.x);  // Im P11
+                const double qx = fma(l0.x, x1.x, fma(l0.y, x1.y, fma(-l1.x, x0.x, -l1.y * x0.y)));
+                const double qy = fma(l0.x, x1.y, fma(-l0.y, x1.x, fma(-l1.y, x0.x, l1.x * x0.y)));
 #pragma unroll
                 for (int j = 0; j < kAdjFusedGens; j++)
                     if (j < ng) {
-                        const double2* G = op.m + 4 + 4 * j;
-                        double d = fma(G[0].x, p00.x, -G[0].y * p00.y);
-                        d = fma(G[1].x, p01.x, fma(-G[1].y, p01.y, d));
-                        d = fma(G[2].x, p10.x, fma(-G[2].y, p10.y, d));
-                        d = fma(G[3].x, p11.x, fma(-G[3].y, p11.y, d));
-                        dot[j] += d;
+                        const double2 g01 = op.m[5 + 4 * j];
+                        dot[j] += fma(-op.m[4 + 4 * j].y, i00, fma(-op.m[7 + 4 * j].y, i11, fma(g01.x, qx, -g01.y * qy)));
                     }
             }
-            if (!op.a_id) {
+            if (apply) {
                 const double2 a0 = op.m[0], a1 = op.m[1], a2 = op.m[2], a3 = op.m[3];
                 x[ia] = cfma2(cmul2(a0, x0), a1, x1);
                 x[ib] = cfma2(cmul2(a2, x0), a3, x1);
@@ -336,7 +343,7 @@ __device__ __forceinline__ void seg_op(const AdjTileOp& op, double2 (&x)[4], dou
         for (int j = 0; j < kAdjFusedGens; j++)
             if (j < ng) {
                 const double d = warp_sum(dot[j]);
-                if (lane == 0) acc[op.gslot[j] * nw + warp] += d;
+                if (lane == 0) acc[c.gslot[j] * nw + warp] += d;
             }
         return;
     }
@@ -345,20 +352,20 @@ __device__ __forceinline__ void seg_op(const AdjTileOp& op, double2 (&x)[4], dou
     for (int q = 0; q < 2; q++) {
         int ia, ib;
         seg_pair_idx<S>(q, ia, ib);
-        if ((li[ia] & op.lcmask) != op.lcval) continue;
-        if (op.gen) {
+        if ((li[ia] & c.lcmask) != c.lcval) continue;
+        if (c.gen) {
             if (!valid) continue;
             const double2 y0 = cfma2(cmul2(op.m[0], x[ia]), op.m[1], x[ib]);
             const double2 y1 = cfma2(cmul2(op.m[2], x[ia]), op.m[3], x[ib]);
             dot += redot(l[ia], y0) + redot(l[ib], y1);
-        } else if (op.cls == GC_X) {
+        } else if (c.cls == GC_X) {
             double2 t = x[ia];
             x[ia] = x[ib];
             x[ib] = t;
             t = l[ia];
             l[ia] = l[ib];
             l[ib] = t;
-        } else if (op.cls == GC_DIAG) {
+        } else if (c.cls == GC_DIAG) {
             if (op.active & 1) {
                 x[ia] = cmul2(op.m[0], x[ia]);
                 l[ia] = cmul2(op.m[0], l[ia]);
@@ -375,9 +382,9 @@ __device__ __forceinline__ void seg_op(const AdjTileOp& op, double2 (&x)[4], dou
             l[ib] = cfma2(cmul2(op.m[2], l0), op.m[3], l1);
         }
     }
-    if (op.gen) {
+    if (c.gen) {
         const double d = warp_sum(dot);
-        if (lane == 0) acc[op.slot * nw + warp] += d;
+        if (lane == 0) acc[c.slot * nw + warp] += d;
     }
 }
 
@@ -402,11 +409,12 @@ __device__ __forceinline__ void adj_seg(const AdjTileOp* __restrict__ sops, int 
     }
     for (int j = 0; j < nr; j++) {
         const AdjTileOp& op = sops[j];
-        if ((base & op.gcmask) != op.gcval) continue;  // uniform over the tile
-        if (op.tl[0] == p0)
-            seg_op<0>(op, x, l, li, acc, nw, valid);
+        const AdjOpCtl c = static_cast<const AdjOpCtl&>(op);  // four 16-byte loads
+        if ((base & c.gcmask) != c.gcval) continue;  // uniform over the tile
+        if (c.tl[0] == p0)
+            seg_op<0>(c, op, x, l, li, acc, nw, valid);
         else
-            seg_op<1>(op, x, l, li, acc, nw, valid);
+            seg_op<1>(c, op, x, l, li, acc, nw, valid);
     }
     if (valid)
 #pragma unroll
@@ -697,6 +705,17 @@ static bool m2_of(const AdjTileOp& op, M2& m) {
     return true;
 }
 
+// G' anti-Hermitian to 1e-12 of its largest entry (the generators of
+// parametric gates are -i times a Hermitian matrix, src/gate.rs, and so is
+// A^dagger G A): real parts of the diagonal zero, G'10 = -conj(G'01)
+static bool m2_antihermitian(const M2& g) {
+    double mx = 0.0;
+    for (int q = 0; q < 4; q++) mx = std::max(mx, std::hypot(g.e[q].x, g.e[q].y));
+    const double tol = 1e-12 * std::max(mx, 1e-300);
+    return std::fabs(g.e[0].x) <= tol && std::fabs(g.e[3].x) <= tol && std::fabs(g.e[1].x + g.e[2].x) <= tol &&
+           std::fabs(g.e[1].y - g.e[2].y) <= tol;
+}
+
 // Fold runs of uncontrolled 1-qubit steps on one target into kAdjFused ops
 // (at most kAdjFusedGens generator dots each).
 static void fuse_runs(std::vector<AdjTileOp>& ops) {
@@ -726,6 +745,7 @@ static void fuse_runs(std::vector<AdjTileOp>& ops) {
             if (o.gen) {
                 if (f.ngen == kAdjFusedGens) break;
                 const M2 g = m2_mul(m2_adj(A), m2_mul(m, A));
+                if (!m2_antihermitian(g)) break;  // the register segments' dot formula needs G'^dagger = -G'
                 for (int q = 0; q < 4; q++) f.m[4 + 4 * f.ngen + q] = g.e[q];
                 f.gslot[f.ngen++] = o.slot;
             } else {

@@ -412,6 +412,82 @@ __global__ void __launch_bounds__(kDCT, 2) k_dm_channel_xor(double2* __restrict_
     }
 }
 
+// 2-qubit XOR channels with two threads per 4 x 4 group: thread h of a
+// pair owns output rows 2h and 2h + 1.  It loads the group with its rows
+// relabelled by a ^ 2h, y[r][b] = rho[row r ^ 2h][b], so that the source
+// y[a' ^ xr][b ^ xc] of its local row a' (output row a = a' ^ 2h) has a
+// compile-time register index; coefficients are read at the output row.
+// Every output entry gets the operations of k_dm_channel_xor in the same
+// order, and a thread needs 16 + 8 entries instead of 16 + 16 registers.
+template <int XR, int XC>
+__device__ __forceinline__ void xor_half(int h2, const double2 (&y)[4][4], double2 (&acc)[2][4], const double2* mr,
+                                         const double2* mc) {
+#pragma unroll
+    for (int ap = 0; ap < 2; ap++) {
+        const int a = ap ^ h2;
+        const double2 cr = mr[a * 4 + (a ^ XR)];
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const double2 v = cmul_sparse(mc[b * 4 + (b ^ XC)], cmul_sparse(cr, y[ap ^ XR][b ^ XC]));
+            acc[ap][b] = cadd_x(acc[ap][b], v);
+        }
+    }
+}
+
+template <int XR>
+__device__ __forceinline__ void xor_half_c(int xc, int h2, const double2 (&y)[4][4], double2 (&acc)[2][4],
+                                           const double2* mr, const double2* mc) {
+    switch (xc) {
+    case 0: xor_half<XR, 0>(h2, y, acc, mr, mc); break;
+    case 1: xor_half<XR, 1>(h2, y, acc, mr, mc); break;
+    case 2: xor_half<XR, 2>(h2, y, acc, mr, mc); break;
+    default: xor_half<XR, 3>(h2, y, acc, mr, mc); break;
+    }
+}
+
+__global__ void __launch_bounds__(kDCT, 3) k_dm_channel_xor2h(double2* __restrict__ rho, uint64_t ngroups,
+                                                              const __grid_constant__ DMChan op) {
+    __shared__ double2 smr[kMaxKraus * 16], smc[kMaxKraus * 16];
+    __shared__ int sx[kMaxKraus][2];
+    for (int i = threadIdx.x; i < op.nk * 16; i += blockDim.x) {
+        smr[i] = op.kr[i];
+        smc[i] = op.kc[i];
+    }
+    for (int i = threadIdx.x; i < op.nk * 2; i += blockDim.x) (&sx[0][0])[i] = (&op.xmask[0][0])[i];
+    __syncthreads();
+    GRID_STRIDE(t, 2 * ngroups) {
+        const uint64_t base = insert_zeros(t >> 1, op.locked, op.nlocked);
+        const int h2 = (int)(t & 1) << 1;
+        double2 y[4][4], acc[2][4];
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) y[r][b] = rho[base + op.roff[r ^ h2] + op.coff[b]];
+#pragma unroll
+        for (int ap = 0; ap < 2; ap++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) acc[ap][b] = make_double2(0.0, 0.0);
+        for (int q = 0; q < op.nk; q++) {
+            const double2* mr = smr + q * 16;
+            const double2* mc = smc + q * 16;
+            const int xr = sx[q][0], xc = sx[q][1];
+            switch (xr) {
+            case 0: xor_half_c<0>(xc, h2, y, acc, mr, mc); break;
+            case 1: xor_half_c<1>(xc, h2, y, acc, mr, mc); break;
+            case 2: xor_half_c<2>(xc, h2, y, acc, mr, mc); break;
+            default: xor_half_c<3>(xc, h2, y, acc, mr, mc); break;
+            }
+        }
+        // both threads of the pair (adjacent lanes, always both in the loop:
+        // 2 ngroups is even) read the whole group before either writes
+        __syncwarp(3u << (threadIdx.x & 30));
+#pragma unroll
+        for (int ap = 0; ap < 2; ap++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) rho[base + op.roff[ap ^ h2] + op.coff[b]] = acc[ap][b];
+    }
+}
+
 // 1-qubit channels whose every Kraus operator has at most one non-zero
 // entry per row (and so its conjugate: amplitude and phase damping, resets,
 // and the Pauli channels): the 2 x 2 group stays in registers and each
@@ -552,32 +628,39 @@ int launch_dm_channel(Ctx* ctx, DM* d, const std::vector<LGate>& rows, const std
     }
     uint64_t ngroups = (uint64_t)1 << (2 * d->nbits - op.nlocked);
     unsigned grid = grid_for(ngroups, kDT, ctx->num_sms);
-    ProfScope prof(ctx, "dm_channel", (double)ngroups * (double)(1 << (2 * k)) * 32.0);
-    if (xr_ok && !(getenv("YAO_DM_XOR") && getenv("YAO_DM_XOR")[0] == '0')) {
-        if (k == 1)
-            k_dm_channel_xor<1><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);
-        else
-            k_dm_channel_xor<2><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);
-        ctx->launches++;
-        YAO_CUDA(cudaGetLastError());
-        return YAO_OK;
-    }
+    const double bytes = (double)ngroups * (double)(1 << (2 * k)) * 32.0;
+    auto off = [](const char* name) {
+        const char* e = getenv(name);
+        return e && e[0] == '0';
+    };
     bool dense = false;
     for (int q = 0; q < nk; q++) dense |= op.cls[q] != GC_DIAG && !op.mono[q];
-    // 1-qubit channels of diagonal and row-monomial operators: registers
-    // (YAO_DM_MONO=0: the shared-memory form)
-    if (k == 1 && !dense && !(getenv("YAO_DM_MONO") && getenv("YAO_DM_MONO")[0] == '0')) {
+    if (xr_ok && !off("YAO_DM_XOR")) {
+        // Pauli-type channels: the group in registers
+        if (k == 1) {
+            ProfScope prof(ctx, "dm_channel_xor1", bytes);
+            k_dm_channel_xor<1><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);
+        } else if (off("YAO_DM_XOR2H")) {
+            ProfScope prof(ctx, "dm_channel_xor2", bytes);
+            k_dm_channel_xor<2><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);
+        } else {  // two threads per group
+            ProfScope prof(ctx, "dm_channel_xor2", bytes);
+            k_dm_channel_xor2h<<<grid_for(2 * ngroups, kDT, ctx->num_sms), kDCT, 0, ctx->stream>>>((double2*)d->d,
+                                                                                                ngroups, op);
+        }
+    } else if (k == 1 && !dense && !off("YAO_DM_MONO")) {
+        // 1-qubit channels of diagonal and row-monomial operators: registers
+        ProfScope prof(ctx, "dm_channel_mono1", bytes);
         k_dm_channel_mono1<<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);
-        ctx->launches++;
-        YAO_CUDA(cudaGetLastError());
-        return YAO_OK;
+    } else {
+        ProfScope prof(ctx, "dm_channel", bytes);
+        if (k == 1)
+            dense ? k_dm_channel<1, true><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op)
+                  : k_dm_channel<1, false><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);
+        else
+            dense ? k_dm_channel<2, true><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op)
+                  : k_dm_channel<2, false><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);
     }
-    if (k == 1)
-        dense ? k_dm_channel<1, true><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op)
-              : k_dm_channel<1, false><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);
-    else
-        dense ? k_dm_channel<2, true><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op)
-              : k_dm_channel<2, false><<<grid, kDCT, 0, ctx->stream>>>((double2*)d->d, ngroups, op);
     ctx->launches++;
     YAO_CUDA(cudaGetLastError());
     (void)row_bits;

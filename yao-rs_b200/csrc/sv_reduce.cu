@@ -619,8 +619,12 @@ int build_lambda_sets(Ctx* ctx, const void* psi_d, void* lam_d, uint32_t nbits, 
     size_t bytes = std::max<size_t>(1, h.size()) * sizeof(MonoFull);
     YAO_CUDA(cudaMallocAsync(&d, bytes, ctx->stream));
     if (!h.empty()) YAO_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(MonoFull), cudaMemcpyHostToDevice, ctx->stream));
-    k_lambda<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>((const double2*)psi_d, (double2*)lam_d, n,
-                                                                       (const MonoFull*)d, (int)h.size());
+    {
+        // reads psi once per distinct X mask (the low ones hit L2), writes lambda
+        ProfScope prof(ctx, "lambda", (double)n * 32.0);
+        k_lambda<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>((const double2*)psi_d, (double2*)lam_d, n,
+                                                                           (const MonoFull*)d, (int)h.size());
+    }
     ctx->launches++;
     YAO_CUDA(cudaGetLastError());
     YAO_CUDA(cudaFreeAsync(d, ctx->stream));
