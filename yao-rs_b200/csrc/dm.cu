@@ -225,6 +225,7 @@ struct DMChan {
     int32_t mono[kMaxKraus];
     int8_t perm[kMaxKraus][2][4];
     int32_t xmask[kMaxKraus][2];  // XOR channels: row / column permutation a -> a ^ xmask
+    int8_t ckind[kMaxKraus][2];   // XOR channels: 0 every non-zero row / column coefficient real, 1 imaginary, 2 neither
     double2 kr[kMaxKraus * 16], kc[kMaxKraus * 16];  // row / column matrices, 2^k x 2^k each
 };
 
@@ -338,6 +339,31 @@ __global__ void __launch_bounds__(kDCT, DENSE ? 1 : 4) k_dm_channel(double2* __r
 // NL^2 code paths with compile-time source indices (no shared-memory reads
 // of the group).  Operation per entry and operator as in k_dm_channel's
 // monomial path: acc += cmul(kc[b], cmul(kr[a], orig[a ^ xr][b ^ xc])).
+// cmul_sparse for a coefficient known to be real (KIND 0) or imaginary
+// (KIND 1): the same two products, without the tests
+template <int KIND>
+__device__ __forceinline__ double2 cmul_kind(double2 c, double2 x) {
+    if (KIND == 0) return make_double2(__dmul_rn(c.x, x.x), __dmul_rn(c.x, x.y));
+    return make_double2(-__dmul_rn(c.y, x.y), __dmul_rn(c.y, x.x));
+}
+
+// xor_op for an operator whose row and column permutations are both
+// a -> a ^ X and whose coefficients are all real / all imaginary per axis
+template <int K, int X, int RK, int CK>
+__device__ __forceinline__ void xor_op_kind(const double2 (&x)[1 << K][1 << K], double2 (&acc)[1 << K][1 << K],
+                                            const double2* mr, const double2* mc) {
+    constexpr int NL = 1 << K;
+#pragma unroll
+    for (int a = 0; a < NL; a++) {
+        const double2 cr = mr[a * NL + (a ^ X)];
+#pragma unroll
+        for (int b = 0; b < NL; b++) {
+            const double2 y = cmul_kind<CK>(mc[b * NL + (b ^ X)], cmul_kind<RK>(cr, x[a ^ X][b ^ X]));
+            acc[a][b] = cadd_x(acc[a][b], y);
+        }
+    }
+}
+
 template <int K, int XR, int XC>
 __device__ __forceinline__ void xor_op(const double2 (&x)[1 << K][1 << K], double2 (&acc)[1 << K][1 << K],
                                        const double2* mr, const double2* mc) {
@@ -374,11 +400,16 @@ __global__ void __launch_bounds__(kDCT, 2) k_dm_channel_xor(double2* __restrict_
     constexpr int NL = 1 << K, MS = NL * NL;
     __shared__ double2 smr[kMaxKraus * MS], smc[kMaxKraus * MS];
     __shared__ int sx[kMaxKraus][2];
+    __shared__ int sk[kMaxKraus];  // 1-qubit: x * 4 + row kind * 2 + column kind, or -1
     for (int i = threadIdx.x; i < op.nk * MS; i += blockDim.x) {
         smr[i] = op.kr[i];
         smc[i] = op.kc[i];
     }
     for (int i = threadIdx.x; i < op.nk * 2; i += blockDim.x) (&sx[0][0])[i] = (&op.xmask[0][0])[i];
+    for (int q = threadIdx.x; q < op.nk; q += blockDim.x)
+        sk[q] = K == 1 && op.xmask[q][0] == op.xmask[q][1] && op.ckind[q][0] < 2 && op.ckind[q][1] < 2
+                    ? op.xmask[q][0] * 4 + op.ckind[q][0] * 2 + op.ckind[q][1]
+                    : -1;
     __syncthreads();
     GRID_STRIDE(g, ngroups) {
         const uint64_t base = insert_zeros(g, op.locked, op.nlocked);
@@ -395,7 +426,18 @@ __global__ void __launch_bounds__(kDCT, 2) k_dm_channel_xor(double2* __restrict_
             const double2* mc = smc + q * MS;
             const int xr = sx[q][0], xc = sx[q][1];
             if constexpr (K == 1) {
-                if (xr == 0) xor_op_c<K, 0>(xc, x, acc, mr, mc); else xor_op_c<K, 1>(xc, x, acc, mr, mc);
+                switch (sk[q]) {
+                case 0: xor_op_kind<1, 0, 0, 0>(x, acc, mr, mc); break;
+                case 1: xor_op_kind<1, 0, 0, 1>(x, acc, mr, mc); break;
+                case 2: xor_op_kind<1, 0, 1, 0>(x, acc, mr, mc); break;
+                case 3: xor_op_kind<1, 0, 1, 1>(x, acc, mr, mc); break;
+                case 4: xor_op_kind<1, 1, 0, 0>(x, acc, mr, mc); break;
+                case 5: xor_op_kind<1, 1, 0, 1>(x, acc, mr, mc); break;
+                case 6: xor_op_kind<1, 1, 1, 0>(x, acc, mr, mc); break;
+                case 7: xor_op_kind<1, 1, 1, 1>(x, acc, mr, mc); break;
+                default:
+                    if (xr == 0) xor_op_c<K, 0>(xc, x, acc, mr, mc); else xor_op_c<K, 1>(xc, x, acc, mr, mc);
+                }
             } else {
                 switch (xr) {
                 case 0: xor_op_c<K, 0>(xc, x, acc, mr, mc); break;
@@ -445,15 +487,35 @@ __device__ __forceinline__ void xor_half_c(int xc, int h2, const double2 (&y)[4]
     }
 }
 
+template <int XR, int RK, int CK>
+__device__ __forceinline__ void xor_half_kind(int h2, const double2 (&y)[4][4], double2 (&acc)[2][4],
+                                              const double2* mr, const double2* mc) {
+#pragma unroll
+    for (int ap = 0; ap < 2; ap++) {
+        const int a = ap ^ h2;
+        const double2 cr = mr[a * 4 + (a ^ XR)];
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const double2 v = cmul_kind<CK>(mc[b * 4 + (b ^ XR)], cmul_kind<RK>(cr, y[ap ^ XR][b ^ XR]));
+            acc[ap][b] = cadd_x(acc[ap][b], v);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kDCT, 3) k_dm_channel_xor2h(double2* __restrict__ rho, uint64_t ngroups,
                                                               const __grid_constant__ DMChan op) {
     __shared__ double2 smr[kMaxKraus * 16], smc[kMaxKraus * 16];
     __shared__ int sx[kMaxKraus][2];
+    __shared__ int sk[kMaxKraus];  // xr * 4 + row kind * 2 + column kind, or -1
     for (int i = threadIdx.x; i < op.nk * 16; i += blockDim.x) {
         smr[i] = op.kr[i];
         smc[i] = op.kc[i];
     }
     for (int i = threadIdx.x; i < op.nk * 2; i += blockDim.x) (&sx[0][0])[i] = (&op.xmask[0][0])[i];
+    for (int q = threadIdx.x; q < op.nk; q += blockDim.x)
+        sk[q] = op.xmask[q][0] == op.xmask[q][1] && op.ckind[q][0] < 2 && op.ckind[q][1] < 2
+                    ? op.xmask[q][0] * 4 + op.ckind[q][0] * 2 + op.ckind[q][1]
+                    : -1;
     __syncthreads();
     GRID_STRIDE(t, 2 * ngroups) {
         const uint64_t base = insert_zeros(t >> 1, op.locked, op.nlocked);
@@ -471,6 +533,22 @@ __global__ void __launch_bounds__(kDCT, 3) k_dm_channel_xor2h(double2* __restric
             const double2* mr = smr + q * 16;
             const double2* mc = smc + q * 16;
             const int xr = sx[q][0], xc = sx[q][1];
+            // same permutation on rows and columns (K and conj(K)) and
+            // coefficients of one kind per axis: a branch-free variant
+            const int code = sk[q];
+            if (code >= 0) {
+                switch (code) {
+#define XOR_KIND_CASE(X, R, C) \
+    case X * 4 + R * 2 + C: xor_half_kind<X, R, C>(h2, y, acc, mr, mc); break;
+                XOR_KIND_CASE(0, 0, 0) XOR_KIND_CASE(0, 0, 1) XOR_KIND_CASE(0, 1, 0) XOR_KIND_CASE(0, 1, 1)
+                XOR_KIND_CASE(1, 0, 0) XOR_KIND_CASE(1, 0, 1) XOR_KIND_CASE(1, 1, 0) XOR_KIND_CASE(1, 1, 1)
+                XOR_KIND_CASE(2, 0, 0) XOR_KIND_CASE(2, 0, 1) XOR_KIND_CASE(2, 1, 0) XOR_KIND_CASE(2, 1, 1)
+                XOR_KIND_CASE(3, 0, 0) XOR_KIND_CASE(3, 0, 1) XOR_KIND_CASE(3, 1, 0) XOR_KIND_CASE(3, 1, 1)
+#undef XOR_KIND_CASE
+                default: break;
+                }
+                continue;
+            }
             switch (xr) {
             case 0: xor_half_c<0>(xc, h2, y, acc, mr, mc); break;
             case 1: xor_half_c<1>(xc, h2, y, acc, mr, mc); break;
@@ -626,6 +704,19 @@ int launch_dm_channel(Ctx* ctx, DM* d, const std::vector<LGate>& rows, const std
             op.xmask[q][ax] = x0;
         }
     }
+    // coefficient kinds of each operator's non-zero entries (rows: K, columns:
+    // conj(K)): all real, all imaginary, or mixed
+    for (int q = 0; q < nk; q++)
+        for (int ax = 0; ax < 2; ax++) {
+            const double2* m = ax == 0 ? op.kr + q * MS : op.kc + q * MS;
+            bool re = true, im = true;
+            for (int i = 0; i < MS; i++) {
+                if (m[i].x == 0.0 && m[i].y == 0.0) continue;
+                re &= m[i].y == 0.0;
+                im &= m[i].x == 0.0;
+            }
+            op.ckind[q][ax] = (int8_t)(re ? 0 : (im ? 1 : 2));
+        }
     uint64_t ngroups = (uint64_t)1 << (2 * d->nbits - op.nlocked);
     unsigned grid = grid_for(ngroups, kDT, ctx->num_sms);
     const double bytes = (double)ngroups * (double)(1 << (2 * k)) * 32.0;

@@ -761,7 +761,7 @@ template <typename V, bool EXACT, int RB, bool TC = false, bool DM = false>
 __device__ __forceinline__ void tile_compute(const TileHdr& hdr, uint64_t base, const TOp* __restrict__ ops,
                                              const TSeg* __restrict__ segs,
                                              const typename CoefT<V>::C* __restrict__ coef, V* s,
-                                             TcCtx* tcx = nullptr) {
+                                             TcCtx* tcx = nullptr, bool last_sync = true) {
     typedef typename CoefT<V>::C C;
     constexpr int NA = 1 << RB;
     V* tag = nullptr;  // selects the swizzle overload
@@ -857,7 +857,7 @@ __device__ __forceinline__ void tile_compute(const TileHdr& hdr, uint64_t base, 
                         wide_tc8<V>(op, s, *tcx);
                     else
                         wide_tc<V>(op, s, *tcx);
-                    __syncthreads();
+                    if (si + 1 < hdr.nsegs || last_sync) __syncthreads();
                     continue;
                 }
             }
@@ -940,7 +940,9 @@ __device__ __forceinline__ void tile_compute(const TileHdr& hdr, uint64_t base, 
             for (int i = 0; i < NA; i++)
                 if (outi[i] != 0xffffffffu) s[swz(outi[i], tag)] = outv[i];
         }
-        __syncthreads();
+        // the next segment moves amplitudes along other bits; after the last
+        // one the caller synchronises itself when last_sync is false
+        if (si + 1 < hdr.nsegs || last_sync) __syncthreads();
     }
 }
 
@@ -1188,10 +1190,11 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         } else {
             tile_load<V, false>(st, hdr, hoff, base, cur);  // ends with __syncthreads
         }
+        // TMA form: the tile's last barrier is the one before its store below
         if constexpr (use_tc)
-            tile_compute<V, EXACT, RB, true>(hdr, base, ops, segs, coef, cur, &tcx);
+            tile_compute<V, EXACT, RB, true>(hdr, base, ops, segs, coef, cur, &tcx, !use_tma);
         else
-            tile_compute<V, EXACT, RB, false, DM>(hdr, base, ops, segs, coef, cur);
+            tile_compute<V, EXACT, RB, false, DM>(hdr, base, ops, segs, coef, cur, nullptr, !use_tma);
         if (use_tma) {
             tc::fence_proxy_async();  // this thread's tile writes are visible to the bulk store
             __syncthreads();
