@@ -2,22 +2,24 @@
 // (yao-rs src/ad.rs:75-156) over shared-memory tiles.
 //
 // The per-gate form reads and writes psi and lambda once per gate of the
-// reverse sweep.  Here a pass takes a run of consecutive reverse-sweep steps
-// whose targets all lie in one tile (the low 4 bits plus up to 7 scattered
-// bits), loads psi's and lambda's tile into shared memory, and for every step
-// in order
+// reverse sweep.  Here a pass takes reverse-sweep steps whose targets all lie
+// in one tile (the low 4 bits plus up to 7 scattered bits), loads psi's and
+// lambda's tile into shared memory, and for every step
 //   - accumulates Re <lambda | G psi> over the tile's groups for each
 //     generator G of a parametric gate (only the control-matching branch,
 //     ad.rs:56-64), and
 //   - applies U^dagger to both tiles,
-// then writes both tiles back.  Consecutive steps on the same target bits
-// (a gate's generator dots and its U^dagger step, and the next gate's on the
-// same qubit) enumerate the same groups on the same threads, so no barrier
-// separates them.  Dots are reduced over the warp, added per warp in shared memory
-// (tiles of a CTA in a fixed order), summed over warps per CTA and over CTAs
-// in block order: deterministic for a given launch shape.  Arithmetic is
-// FP64 with FMA; the result is the reverse sweep of the per-gate form up to
-// rounding (~1e-15 relative).
+// then writes both tiles back.  A pass is list-scheduled over the sweep: it
+// takes every step that no skipped earlier step shares a qubit with (steps
+// on disjoint qubits commute, and a generator dot does not change under
+// steps on other qubits), and within the pass consecutive 1-qubit steps on
+// at most two target bits form a register segment: each thread keeps its
+// 4-amplitude group of both tiles in registers across the segment.  Dots are
+// reduced over the warp, added per warp in shared memory (tiles of a CTA in a
+// fixed order), summed over warps per CTA and over CTAs in block order:
+// deterministic for a given launch shape.  Arithmetic is FP64 with FMA; the
+// result is the reverse sweep of the per-gate form up to rounding (~1e-15
+// relative).
 #include <algorithm>
 #include <cmath>
 #include <cstring>

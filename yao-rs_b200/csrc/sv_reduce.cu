@@ -423,6 +423,17 @@ __device__ __forceinline__ double2 qturn(double2 v, int q) {
     }
 }
 
+// qturn without branches (the same numbers, signs of zero included): swap
+// the parts for odd q, then flip the sign bits of the real part (q = 1, 2)
+// and of the imaginary part (q = 2, 3)
+__device__ __forceinline__ double2 qturn_bf(double2 v, int q) {
+    const double re = (q & 1) ? v.y : v.x, im = (q & 1) ? v.x : v.y;
+    const unsigned long long sr = (unsigned long long)((q ^ (q >> 1)) & 1) << 63;
+    const unsigned long long si = (unsigned long long)((q >> 1) & 1) << 63;
+    return make_double2(__longlong_as_double(__double_as_longlong(re) ^ (long long)sr),
+                        __longlong_as_double(__double_as_longlong(im) ^ (long long)si));
+}
+
 constexpr int kMaxGroupTerms = 8;
 struct MonoGroup {
     uint64_t xmask;
@@ -557,28 +568,40 @@ __global__ void __launch_bounds__(kTTThreads, 1)
                 for (int k = 0; k < hdr.nterms; k++) {
                     const TermTile& m = terms[k];
                     const int q = mono_phase(m.t, g);
-                    const double2 v = q >= 0 ? qturn(sp[l ^ m.lx], q) : make_double2(0.0, 0.0);
+                    const double2 v = q >= 0 ? qturn_bf(sp[l ^ m.lx], q) : make_double2(0.0, 0.0);
                     a = cadd_x(a, cmul_x(m.c, v));
                 }
                 lam[g] = a;
             }
         } else {
-            for (int k = 0; k < hdr.nterms; k++) {
-                const TermTile& m = terms[k];
-                double re = 0.0, im = 0.0;
+            // chunks of 8 terms: each amplitude and its index read once per chunk
+            constexpr int kChunk = 8;
+            for (int k0 = 0; k0 < hdr.nterms; k0 += kChunk) {
+                double re[kChunk], im[kChunk];
+#pragma unroll
+                for (int j = 0; j < kChunk; j++) re[j] = im[j] = 0.0;
                 for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) {
                     const uint64_t g = base | (l & lmask) | hoff[l >> nlow];
-                    const int q = mono_phase(m.t, g);
-                    if (q < 0) continue;
-                    const double2 x = sp[l], y = qturn(sp[l ^ m.lx], q);
-                    re += x.x * y.x + x.y * y.y;  // conj(x) y
-                    im += x.x * y.y - x.y * y.x;
+                    const double2 x = sp[l];
+#pragma unroll
+                    for (int j = 0; j < kChunk; j++) {
+                        if (k0 + j >= hdr.nterms) break;
+                        const TermTile& m = terms[k0 + j];
+                        const int q = mono_phase(m.t, g);
+                        if (q < 0) continue;
+                        const double2 y = qturn_bf(sp[l ^ m.lx], q);
+                        re[j] = fma(x.x, y.x, fma(x.y, y.y, re[j]));  // conj(x) y
+                        im[j] = fma(x.x, y.y, fma(-x.y, y.x, im[j]));
+                    }
                 }
-                re = warp_sum(re);
-                im = warp_sum(im);
-                if (lane == 0) {
-                    acc[(2 * k) * nw + warp] += re;
-                    acc[(2 * k + 1) * nw + warp] += im;
+#pragma unroll
+                for (int j = 0; j < kChunk; j++) {
+                    if (k0 + j >= hdr.nterms) break;
+                    const double r = warp_sum(re[j]), i = warp_sum(im[j]);
+                    if (lane == 0) {
+                        acc[(2 * (k0 + j)) * nw + warp] += r;
+                        acc[(2 * (k0 + j) + 1) * nw + warp] += i;
+                    }
                 }
             }
         }
@@ -684,12 +707,13 @@ int expect_terms_launch(Ctx* ctx, const Reg* r, const std::vector<MonoTerm>& ter
         size_t npart = 0, nres = 2 * terms.size();
         for (auto& p : tp) npart += (size_t)grid * 2 * p.second.size();
         const size_t tbytes = terms.size() * sizeof(TermTile);
-        const size_t tdoubles = (tbytes + sizeof(double) - 1) / sizeof(double);
-        if (ctx->ensure_scratch(sizeof(double) * (npart + nres + tdoubles))) return YAO_ERR_OUT_OF_MEMORY;
+        // the term table after partials and results, on a 16-byte boundary
+        const size_t toff = (sizeof(double) * (npart + nres) + 15) / 16 * 16;
+        if (ctx->ensure_scratch(toff + tbytes)) return YAO_ERR_OUT_OF_MEMORY;
         if (ctx->ensure_host_pinned(sizeof(double) * nres)) return YAO_ERR_OUT_OF_MEMORY;
         double* part = (double*)ctx->scratch;
         double* res = part + npart;
-        TermTile* dterms = (TermTile*)(res + nres);
+        TermTile* dterms = (TermTile*)((char*)ctx->scratch + toff);
         std::vector<TermTile> all;
         for (auto& p : tp) all.insert(all.end(), p.second.begin(), p.second.end());
         YAO_CUDA(cudaMemcpyAsync(dterms, all.data(), tbytes, cudaMemcpyHostToDevice, ctx->stream));

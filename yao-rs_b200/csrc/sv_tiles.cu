@@ -14,7 +14,8 @@
 //    any bit: a diagonal entry and a control test only read the amplitude's
 //    global index.
 //  - FUSED form: gates are first multiplied into dense blocks of at most k
-//    qubits (host, FP64); each block is one op of a pass.  On complex64
+//    qubits (host, FP64); each block is one op of a pass, and a pass may take
+//    blocks out of order past blocks on disjoint qubits.  On complex64
 //    registers the block coefficients are split into an FP32 high part and
 //    an FP32 low part (c = hi + lo), and both products are accumulated in
 //    FP32 (a two-term compensated product).
