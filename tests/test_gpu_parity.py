@@ -299,39 +299,6 @@ def random_polynomial(rng, n, nterms):
     return Y.OperatorPolynomial(coeffs, strs)
 
 
-@pytest.mark.parametrize("n", [3, 11, 14, 16])
-def test_expect_terms_over_tiles(monkeypatch, n):
-    """Pauli sums with many terms of scattered X masks (and one whose X mask
-    has more scattered bits than a tile holds, which takes the whole-state
-    kernels): the tiled expectation agrees with the whole-state one and the
-    oracle to 1e-12, and expect_grad's gradient is the same numbers with and
-    without the tiled lambda."""
-    rng = np.random.default_rng(700 + n)
-    psi = random_state(rng, n)
-    r = Y.ArrayReg.from_vec(n, psi)
-    ops = [random_polynomial(rng, n, 40), tfim(n)]
-    if n >= 12:
-        ops.append(Y.OperatorPolynomial([0.5], [Y.OperatorString([(q, Y.Op.X) for q in range(n)])]) + tfim(n))
-    for op in ops:
-        ref = O.expect_arrayreg(psi, n, op)
-        monkeypatch.setenv("YAO_TERM_TILES", "1")
-        got = Y.expect_arrayreg(r, op)
-        monkeypatch.setenv("YAO_TERM_TILES", "0")
-        whole = Y.expect_arrayreg(r, op)
-        assert abs(got - ref) <= 1e-12 * max(1.0, abs(ref)), (got, ref)
-        assert abs(got - whole) <= 1e-12 * max(1.0, abs(ref)), (got, whole)
-    c = vqe_ansatz(n, 2, rng.uniform(-math.pi, math.pi, size=2 * n * 2))
-    op = tfim(n, 0.7) + random_polynomial(rng, n, 10)
-    monkeypatch.setenv("YAO_TERM_TILES", "1")
-    v1, g1 = Y.expect_grad(op, c, r)
-    monkeypatch.setenv("YAO_TERM_TILES", "0")
-    v0, g0 = Y.expect_grad(op, c, r)
-    assert abs(v1 - v0) < 1e-12
-    assert np.max(np.abs(np.array(g1) - np.array(g0))) == 0.0
-    vo, go = O.expect_grad(op, c, psi)
-    assert np.max(np.abs(np.array(g1) - np.array(go))) < 1e-11
-
-
 @pytest.mark.parametrize("n", [1, 3, 7, 12])
 def test_expect_arrayreg(n):
     rng = np.random.default_rng(40 + n)

@@ -500,9 +500,13 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
     const uint32_t lmask = (1u << nlow) - 1;
     bool dead = false;
     uint32_t it = 0;
-    for (uint64_t t = blockIdx.x; t < hdr.ntiles; t += gridDim.x, it++) {
+    // buffer of this tile (it % nbuf) and the parity of its use (it / nbuf),
+    // carried from tile to tile instead of divided out
+    uint32_t bcur = 0, bpar = 0;
+    for (uint64_t t = blockIdx.x; t < hdr.ntiles;
+         t += gridDim.x, it++, bcur = bcur + 1 == (uint32_t)nbuf ? 0u : bcur + 1, bpar ^= bcur == 0 ? 1u : 0u) {
         const uint64_t base = tile_base(t);
-        const int b = use_tma ? (int)(it % (uint32_t)nbuf) : 0;
+        const int b = use_tma ? (int)bcur : 0;
         double2* sp = (double2*)(smem + (size_t)b * 2 * tile_bytes);
         double2* sl = sp + T;
         if (use_tma) {
@@ -513,7 +517,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
                 pending |= 1u << bn;
             }
             if (!dead) {
-                const uint32_t parity = (it / (uint32_t)nbuf) & 1u;
+                const uint32_t parity = bpar;
                 const uint64_t t0 = adj_ns();
                 while (!tc::mbar_try_wait(&full_bar[b], parity)) {
                     if (adj_ns() - t0 > kAdjWaitNs) {
@@ -574,7 +578,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
                 // compute to read it
                 const uint64_t tn = t + (uint64_t)(nbuf - 1) * gridDim.x;
                 if (nbuf > 2 && tn < hdr.ntiles) {
-                    const int bn = (int)((it + (uint32_t)nbuf - 1) % (uint32_t)nbuf);
+                    const int bn = (int)(bcur == 0 ? (uint32_t)nbuf - 1 : bcur - 1);
                     tma::wait_group_read<1>();
                     issue(tn, bn);
                     pending |= 1u << bn;

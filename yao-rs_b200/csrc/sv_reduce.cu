@@ -423,17 +423,6 @@ __device__ __forceinline__ double2 qturn(double2 v, int q) {
     }
 }
 
-// qturn without branches (the same numbers, signs of zero included): swap
-// the parts for odd q, then flip the sign bits of the real part (q = 1, 2)
-// and of the imaginary part (q = 2, 3)
-__device__ __forceinline__ double2 qturn_bf(double2 v, int q) {
-    const double re = (q & 1) ? v.y : v.x, im = (q & 1) ? v.x : v.y;
-    const unsigned long long sr = (unsigned long long)((q ^ (q >> 1)) & 1) << 63;
-    const unsigned long long si = (unsigned long long)((q >> 1) & 1) << 63;
-    return make_double2(__longlong_as_double(__double_as_longlong(re) ^ (long long)sr),
-                        __longlong_as_double(__double_as_longlong(im) ^ (long long)si));
-}
-
 constexpr int kMaxGroupTerms = 8;
 struct MonoGroup {
     uint64_t xmask;
@@ -504,190 +493,6 @@ static MonoDev to_dev(const MonoTerm& m) {
     return d;
 }
 
-// ---------------------------------------------- Pauli sums over tiles
-//
-// lambda = H psi and the terms' expectation values over shared-memory tiles
-// of psi: 2^tbits amplitudes, the 4 lowest bits plus up to 7 scattered bits.
-// A pass takes consecutive terms (term order) whose X masks lie in the
-// tile, so every (P_t psi)[i] of the pass reads psi from the tile.  lambda:
-// each amplitude accumulates its terms in order onto the previous passes'
-// value (the first pass starts from zero): the operations of k_lambda in
-// the same order, so lambda is the same numbers.  Expectation: per tile and
-// term sum_i conj(psi_i) (P_t psi)_i, reduced per warp, per CTA in warp
-// order, then over CTAs in block order.
-constexpr int kTTLow = 4, kTTScatter = 7, kTTThreads = 512, kTTMaxTerms = 48;
-
-struct TermTileHdr {
-    int32_t tbits, nterms, nouts, first;
-    int8_t hb[kTTScatter];  // global bits at local positions kTTLow ..
-    int8_t pad;
-    int8_t outb[64];        // global bits outside the tile, ascending
-    uint64_t ntiles;
-};
-
-struct TermTile {
-    MonoDev t;
-    uint32_t lx;  // X mask at local positions
-    int32_t pad;
-    double2 c;    // coefficient (lambda)
-};
-
-template <bool LAMBDA>
-__global__ void __launch_bounds__(kTTThreads, 1)
-    k_terms_tiles(const double2* __restrict__ psi, double2* __restrict__ lam, const TermTileHdr phdr,
-                  const TermTile* __restrict__ gterms, double* __restrict__ partial) {
-    extern __shared__ __align__(16) unsigned char tt_smem[];
-    __shared__ uint64_t hoff[1 << kTTScatter];
-    __shared__ TermTileHdr hdr;  // indexed with run-time subscripts: keep it out of the parameter space
-    if (threadIdx.x == 0) hdr = phdr;
-    __syncthreads();
-    const uint32_t T = 1u << hdr.tbits, nw = blockDim.x >> 5;
-    const int nlow = min(kTTLow, hdr.tbits), nh = hdr.tbits - nlow;
-    double2* sp = (double2*)tt_smem;
-    TermTile* terms = (TermTile*)(sp + T);
-    double* acc = (double*)(terms + hdr.nterms);  // [term][re / im][warp]
-    for (int i = threadIdx.x; i < hdr.nterms; i += blockDim.x) terms[i] = gterms[i];
-    for (int i = threadIdx.x; i < 2 * hdr.nterms * (int)nw; i += blockDim.x) acc[i] = 0.0;
-    for (uint32_t h = threadIdx.x; h < (1u << nh); h += blockDim.x) {
-        uint64_t o = 0;
-        for (int j = 0; j < nh; j++) o |= (uint64_t)((h >> j) & 1) << hdr.hb[j];
-        hoff[h] = o;
-    }
-    __syncthreads();
-    const uint32_t lmask = (1u << nlow) - 1;
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (uint64_t t = blockIdx.x; t < hdr.ntiles; t += gridDim.x) {
-        uint64_t base = 0;
-        for (int i = 0; i < hdr.nouts; i++) base |= ((t >> i) & 1) << hdr.outb[i];
-        for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) sp[l] = psi[base | (l & lmask) | hoff[l >> nlow]];
-        __syncthreads();
-        if (LAMBDA) {
-            for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) {
-                const uint64_t g = base | (l & lmask) | hoff[l >> nlow];
-                double2 a = hdr.first ? make_double2(0.0, 0.0) : lam[g];
-                for (int k = 0; k < hdr.nterms; k++) {
-                    const TermTile& m = terms[k];
-                    const int q = mono_phase(m.t, g);
-                    const double2 v = q >= 0 ? qturn_bf(sp[l ^ m.lx], q) : make_double2(0.0, 0.0);
-                    a = cadd_x(a, cmul_x(m.c, v));
-                }
-                lam[g] = a;
-            }
-        } else {
-            // chunks of 8 terms: each amplitude and its index read once per chunk
-            constexpr int kChunk = 8;
-            for (int k0 = 0; k0 < hdr.nterms; k0 += kChunk) {
-                double re[kChunk], im[kChunk];
-#pragma unroll
-                for (int j = 0; j < kChunk; j++) re[j] = im[j] = 0.0;
-                for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) {
-                    const uint64_t g = base | (l & lmask) | hoff[l >> nlow];
-                    const double2 x = sp[l];
-#pragma unroll
-                    for (int j = 0; j < kChunk; j++) {
-                        if (k0 + j >= hdr.nterms) break;
-                        const TermTile& m = terms[k0 + j];
-                        const int q = mono_phase(m.t, g);
-                        if (q < 0) continue;
-                        const double2 y = qturn_bf(sp[l ^ m.lx], q);
-                        re[j] = fma(x.x, y.x, fma(x.y, y.y, re[j]));  // conj(x) y
-                        im[j] = fma(x.x, y.y, fma(-x.y, y.x, im[j]));
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < kChunk; j++) {
-                    if (k0 + j >= hdr.nterms) break;
-                    const double r = warp_sum(re[j]), i = warp_sum(im[j]);
-                    if (lane == 0) {
-                        acc[(2 * (k0 + j)) * nw + warp] += r;
-                        acc[(2 * (k0 + j) + 1) * nw + warp] += i;
-                    }
-                }
-            }
-        }
-        __syncthreads();
-    }
-    if (!LAMBDA)
-        for (int v = threadIdx.x; v < 2 * hdr.nterms; v += blockDim.x) {
-            double sum = 0.0;
-            for (uint32_t w = 0; w < nw; w++) sum += acc[v * nw + w];
-            partial[(size_t)blockIdx.x * 2 * hdr.nterms + v] = sum;
-        }
-}
-
-// YAO_TERM_TILES=0: expectation groups and lambda by the whole-state kernels
-static bool term_tiles_on() {
-    const char* e = getenv("YAO_TERM_TILES");
-    return !(e && e[0] == '0');
-}
-
-// Passes of consecutive terms whose X masks fit a tile; false when some
-// term's mask has more scattered bits than a tile holds (the caller then
-// uses the whole-state kernels).
-static bool plan_term_tiles(const std::vector<MonoTerm>& terms, uint32_t nbits,
-                            std::vector<std::pair<TermTileHdr, std::vector<TermTile>>>& out) {
-    const int tbits = (int)std::min<uint32_t>(nbits, kTTLow + kTTScatter);
-    const int nlow = std::min(kTTLow, tbits), S = tbits - nlow;
-    size_t i = 0;
-    while (i < terms.size()) {
-        uint64_t H = 0;
-        size_t j = i;
-        for (; j < terms.size() && (int)(j - i) < kTTMaxTerms; j++) {
-            const uint64_t hi = terms[j].xmask >> nlow << nlow;
-            if (__builtin_popcountll(H | hi) > S) break;
-            H |= hi;
-        }
-        if (j == i) return false;
-        for (int b = nlow; __builtin_popcountll(H) < S && b < (int)nbits; b++) H |= 1ull << b;
-        TermTileHdr h;
-        memset(&h, 0, sizeof(h));
-        h.tbits = tbits;
-        h.first = out.empty() ? 1 : 0;
-        int local[64];
-        for (int b = 0; b < 64; b++) local[b] = b < nlow ? b : -1;
-        int pos = nlow;
-        for (int b = nlow; b < (int)nbits; b++)
-            if ((H >> b) & 1) {
-                h.hb[pos - nlow] = (int8_t)b;
-                local[b] = pos++;
-            }
-        for (int b = 0; b < (int)nbits; b++)
-            if (local[b] < 0) h.outb[h.nouts++] = (int8_t)b;
-        h.ntiles = (uint64_t)1 << (nbits - tbits);
-        std::vector<TermTile> tt;
-        for (size_t k = i; k < j; k++) {
-            TermTile x;
-            memset(&x, 0, sizeof(x));
-            x.t = to_dev(terms[k]);
-            for (int b = 0; b < (int)nbits; b++)
-                if ((terms[k].xmask >> b) & 1) x.lx |= 1u << local[b];
-            x.c = make_double2(terms[k].coeff.re, terms[k].coeff.im);
-            tt.push_back(x);
-        }
-        h.nterms = (int32_t)tt.size();
-        out.emplace_back(h, std::move(tt));
-        i = j;
-    }
-    return true;
-}
-
-// Launches one pass of k_terms_tiles; `terms_dev` holds the pass's terms.
-template <bool LAMBDA>
-static int launch_term_tiles(Ctx* ctx, const double2* psi, double2* lam, const TermTileHdr& h,
-                             const TermTile* terms_dev, double* partial, int grid) {
-    const size_t smem = ((size_t)1 << h.tbits) * sizeof(double2) + (size_t)h.nterms * sizeof(TermTile) +
-                        (size_t)2 * h.nterms * (kTTThreads / 32) * sizeof(double);
-    static bool attr[2] = {false, false};
-    if (!attr[LAMBDA]) {
-        YAO_CUDA(cudaFuncSetAttribute(k_terms_tiles<LAMBDA>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-        attr[LAMBDA] = true;
-    }
-    k_terms_tiles<LAMBDA><<<grid, kTTThreads, smem, ctx->stream>>>(psi, lam, h, terms_dev, partial);
-    ctx->launches++;
-    YAO_CUDA(cudaGetLastError());
-    return YAO_OK;
-}
-
 // values[t] = <psi|O_t|psi> (without the coefficient), in two halves: the
 // launch half groups the terms by X mask, runs one reduction per group into
 // its own part of the scratch (partials, then the group's sums) and queues
@@ -699,45 +504,6 @@ int expect_terms_launch(Ctx* ctx, const Reg* r, const std::vector<MonoTerm>& ter
     pend.nv.clear();
     pend.nterms = terms.size();
     const uint64_t n = (uint64_t)1 << r->nbits;
-    // complex128 registers: every term over tiles, consecutive terms per pass
-    std::vector<std::pair<TermTileHdr, std::vector<TermTile>>> tp;
-    if (term_tiles_on() && r->precision == YAO_C128 && r->nbits >= 3 && !terms.empty() &&
-        plan_term_tiles(terms, r->nbits, tp)) {
-        const int grid = (int)std::min<uint64_t>(tp[0].first.ntiles, (uint64_t)2 * ctx->num_sms);
-        size_t npart = 0, nres = 2 * terms.size();
-        for (auto& p : tp) npart += (size_t)grid * 2 * p.second.size();
-        const size_t tbytes = terms.size() * sizeof(TermTile);
-        // the term table after partials and results, on a 16-byte boundary
-        const size_t toff = (sizeof(double) * (npart + nres) + 15) / 16 * 16;
-        if (ctx->ensure_scratch(toff + tbytes)) return YAO_ERR_OUT_OF_MEMORY;
-        if (ctx->ensure_host_pinned(sizeof(double) * nres)) return YAO_ERR_OUT_OF_MEMORY;
-        double* part = (double*)ctx->scratch;
-        double* res = part + npart;
-        TermTile* dterms = (TermTile*)((char*)ctx->scratch + toff);
-        std::vector<TermTile> all;
-        for (auto& p : tp) all.insert(all.end(), p.second.begin(), p.second.end());
-        YAO_CUDA(cudaMemcpyAsync(dterms, all.data(), tbytes, cudaMemcpyHostToDevice, ctx->stream));
-        size_t po = 0, ro = 0, to = 0, k = 0;
-        for (auto& p : tp) {
-            const int nt = (int)p.second.size();
-            {
-                ProfScope prof(ctx, "expect_tiles", (double)n * 16.0);
-                int st = launch_term_tiles<false>(ctx, (const double2*)r->d, nullptr, p.first, dterms + to, part + po,
-                                                  grid);
-                if (st) return st;
-            }
-            k_final_sum<<<1, kRT, 0, ctx->stream>>>(part + po, grid, 2 * nt, res + ro);
-            ctx->launches++;
-            YAO_CUDA(cudaGetLastError());
-            for (int q = 0; q < nt; q++) pend.idx.push_back(k++);
-            pend.nv.push_back(2 * nt);
-            po += (size_t)grid * 2 * nt;
-            ro += 2 * (size_t)nt;
-            to += (size_t)nt;
-        }
-        YAO_CUDA(cudaMemcpyAsync(ctx->host_pinned, res, sizeof(double) * nres, cudaMemcpyDeviceToHost, ctx->stream));
-        return YAO_OK;
-    }
     std::vector<bool> done(terms.size(), false);
     std::vector<MonoGroup> groups;
     for (size_t t0 = 0; t0 < terms.size(); t0++) {
@@ -835,25 +601,7 @@ __global__ void __launch_bounds__(256) k_lambda(const double2* __restrict__ psi,
 }
 
 int build_lambda(Ctx* ctx, const Reg* psi, const std::vector<MonoTerm>& terms, Reg* lambda) {
-    std::vector<std::pair<TermTileHdr, std::vector<TermTile>>> passes;
-    if (!term_tiles_on() || terms.empty() || psi->nbits < 3 || !plan_term_tiles(terms, psi->nbits, passes))
-        return build_lambda_sets(ctx, psi->d, lambda->d, psi->nbits, 1, terms);
-    std::vector<TermTile> all;
-    for (auto& p : passes) all.insert(all.end(), p.second.begin(), p.second.end());
-    void* d = nullptr;
-    YAO_CUDA(cudaMallocAsync(&d, all.size() * sizeof(TermTile), ctx->stream));
-    YAO_CUDA(cudaMemcpyAsync(d, all.data(), all.size() * sizeof(TermTile), cudaMemcpyHostToDevice, ctx->stream));
-    const int grid = (int)std::min<uint64_t>(passes[0].first.ntiles, (uint64_t)2 * ctx->num_sms);
-    size_t off = 0;
-    for (auto& p : passes) {
-        ProfScope prof(ctx, "lambda", (double)((uint64_t)1 << psi->nbits) * (p.first.first ? 32.0 : 48.0));
-        int s = launch_term_tiles<true>(ctx, (const double2*)psi->d, (double2*)lambda->d, p.first,
-                                         (const TermTile*)d + off, nullptr, grid);
-        if (s) return s;
-        off += p.second.size();
-    }
-    YAO_CUDA(cudaFreeAsync(d, ctx->stream));
-    return YAO_OK;
+    return build_lambda_sets(ctx, psi->d, lambda->d, psi->nbits, 1, terms);
 }
 
 // nsets registers back to back: every mask lies below the register-index

@@ -1160,8 +1160,12 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
         __syncthreads();
     }
     bool dead = false;  // a wait gave up: skip the remaining waits
-    for (uint32_t it = 0; t < hdr.ntiles; t += grid, it++) {
-        const uint32_t b = use_tma ? it % (uint32_t)nbuf : 0;
+    // buffer of this tile (it % nbuf) and the parity of its use (it / nbuf),
+    // carried from tile to tile instead of divided out
+    uint32_t bcur = 0, bpar = 0;
+    for (uint32_t it = 0; t < hdr.ntiles;
+         t += grid, it++, bcur = bcur + 1 == (uint32_t)nbuf ? 0u : bcur + 1, bpar ^= bcur == 0 ? 1u : 0u) {
+        const uint32_t b = use_tma ? bcur : 0;
         V* cur = (V*)(smem + (size_t)b * tile_bytes);
         const uint64_t base = tile_base(t, bt);
         if (use_tma) {
@@ -1177,7 +1181,7 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
                 }
             }
             if (!dead) {
-                const uint32_t parity = (it / (uint32_t)nbuf) & 1u;
+                const uint32_t parity = bpar;
                 const uint64_t t0 = global_ns_tc();
                 while (!tc::mbar_try_wait(&full_bar[b], parity)) {
                     if (global_ns_tc() - t0 > kTileWaitNs) {
@@ -1207,7 +1211,7 @@ __global__ void __launch_bounds__(kTileThreads, RB <= 2 ? 2 : 1)
                 // may still be reading), so no thread waits before computing
                 const uint64_t tn = t + (uint64_t)(nbuf - 1) * grid;
                 if (nbuf > 2 && tn < hdr.ntiles) {
-                    const uint32_t bn = (it + (uint32_t)nbuf - 1) % (uint32_t)nbuf;
+                    const uint32_t bn = bcur == 0 ? (uint32_t)nbuf - 1 : bcur - 1;
                     tma::wait_group_read<1>();
                     tma_load_tile(&tmap, hdr, tile_base(tn, bt), sbase + bn * tile_bytes, &full_bar[bn], tile_bytes);
                     pending |= 1u << bn;
@@ -2075,7 +2079,21 @@ static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
     const int slots = hdr.tc_resident ? ntc : 1;
     hdr.staged = 2 * tile_bytes + tcb(slots) + stg <= budget ? 1 : 0;
     hdr.nstage = 2;
-    for (int ns = 4; ns > 2 && hdr.use_tma; ns--)
+    // CTAs of at most 256 threads fit twice per SM by registers (128 a
+    // thread): take the most tile buffers with which two CTAs fit the SM's
+    // shared memory (16 warps instead of 8), else the most one CTA holds
+    static int sm_total = 0;
+    if (!sm_total)
+        YAO_CUDA(cudaDeviceGetAttribute(&sm_total, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
+    const size_t half = (size_t)sm_total / 2 - 16 * 1024 - 2048;  // static shared memory, reserve, alignment
+    bool two = false;
+    if (hdr.use_tma && !hdr.mma && threads <= 256)
+        for (int ns = 3; ns >= 2 && !two; ns--)
+            if ((size_t)ns * tile_bytes + (hdr.staged ? stg : 0) <= half) {
+                hdr.nstage = ns;
+                two = true;
+            }
+    for (int ns = 4; ns > 2 && hdr.use_tma && !two; ns--)
         if ((size_t)ns * tile_bytes + tcb(slots) + (hdr.staged ? stg : 0) <= budget) {
             hdr.nstage = ns;
             break;
