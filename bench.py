@@ -917,10 +917,11 @@ def qft_extra(Y, A, torch, stream, dev, timed):
     for name, mode in (("plain", Y.MODE_PLAIN), ("tiled", Y.MODE_TILED)):
         r = Y.ArrayReg.from_vec(n, psi, device=dev)
         Y.apply_inplace(c, r, mode)
-        reps = 5
         r.set_state(psi)
-        t = timed(lambda: [Y.apply_inplace(c, r, mode) for _ in range(reps)])
-        res[f"s_per_circuit_{name}"] = t / reps
+        # one circuit per timing, median of 11: a call of about a millisecond
+        # is exposed to the shared host's scheduling, which a mean would carry
+        ts = sorted(timed(lambda: Y.apply_inplace(c, r, mode)) for _ in range(11))
+        res[f"s_per_circuit_{name}"] = ts[5]
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
     t0 = time.perf_counter()

@@ -2087,7 +2087,8 @@ static int run_pass(Ctx* ctx, V* st, uint32_t nbits, const PassPlan& pp) {
         YAO_CUDA(cudaDeviceGetAttribute(&sm_total, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
     const size_t half = (size_t)sm_total / 2 - 16 * 1024 - 2048;  // static shared memory, reserve, alignment
     bool two = false;
-    if (hdr.use_tma && !hdr.mma && threads <= 256)
+    const char* te = getenv("YAO_TILE_TWO");  // YAO_TILE_TWO=0: the most buffers one CTA holds
+    if (hdr.use_tma && !hdr.mma && threads <= 256 && !(te && te[0] == '0'))
         for (int ns = 3; ns >= 2 && !two; ns--)
             if ((size_t)ns * tile_bytes + (hdr.staged ? stg : 0) <= half) {
                 hdr.nstage = ns;
