@@ -2470,12 +2470,13 @@ static int tune_program(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog, 
             c.k = k;
             c.tc = 0;
             cs.push_back(c);
-            if (sizeof(V) == 8 && k >= 3 && k <= kTcK) {
-                c.tbits = kTcTileBits;
-                c.rb = 3;
-                c.tc = 1;
-                cs.push_back(c);
-            }
+            if (sizeof(V) == 8 && k >= 3 && k <= kTcK)
+                for (int rb = 3; rb <= 4; rb++) {  // 512 or 256 threads a tile
+                    c.tbits = kTcTileBits;
+                    c.rb = rb;
+                    c.tc = 1;
+                    cs.push_back(c);
+                }
         }
         cand.clear();
         for (const TileConfig& c : cs) cand.push_back(make(c));
@@ -2484,13 +2485,15 @@ static int tune_program(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog, 
     } else if (!st && mode == YAO_MODE_FUSED && sizeof(V) == 8 && kreq >= 3 && kreq <= kTcK) {
         // a requested complex64 width: the tensor cores' 2^12 tile against the
         // chosen shape on the CUDA cores
-        TileConfig on = *best, off = *best;
-        on.tbits = kTcTileBits;
+        TileConfig on = *best, on4 = *best, off = *best;
+        on.tbits = on4.tbits = kTcTileBits;
         on.rb = 3;
-        on.tc = 1;
+        on4.rb = 4;
+        on.tc = on4.tc = 1;
         off.tc = 0;
         cand.clear();
         cand.push_back(make(on));
+        cand.push_back(make(on4));
         cand.push_back(make(off));
         st = best_of(cand, &pick, &bms);
         if (!st) *best = cand[pick].c;
