@@ -842,13 +842,17 @@ def test_expect_grad_tiled_sweep_matches_per_gate(monkeypatch, n, form):
     controls inside and outside the tiles, 2-qubit parametric gates, SWAP,
     ISWAP, X, diagonal and controlled dense 1-qubit steps; in every form of
     the tiled sweep: register segments (steps re-sequenced within a pass) or
-    one op at a time, steps moved across commuting ones or kept in order."""
+    one op at a time, steps moved across commuting ones or kept in order.
+    Every third qubit carries a run of three parametric steps (three
+    generator dots of one folded run)."""
     rng = np.random.default_rng(40 + n)
     els = []
     for _ in range(2):
         for q in range(n):
             els.append(Y.put([q], Gate.Ry(float(rng.uniform(-3, 3)))))
             els.append(Y.put([q], Gate.Rz(float(rng.uniform(-3, 3)))))
+            if q % 3 == 0:
+                els.append(Y.put([q], Gate.Rx(float(rng.uniform(-3, 3)))))
         els.append(Y.put([n - 4], Gate.T))
         els.append(Y.control([n - 3], [2], Gate.H))
         els.append(Y.PositionedGate(Gate.Rz(float(rng.uniform(-3, 3))), [n - 1], [1], [False]))

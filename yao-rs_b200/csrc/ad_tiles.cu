@@ -303,9 +303,25 @@ __device__ __forceinline__ void seg_pair_idx(int q, int& a, int& b) {
     }
 }
 
+// Two warp sums in five shuffle rounds: after the exchange across the half
+// warps, lanes 0..15 carry partial sums of a and lanes 16..31 of b; the
+// returned value is the sum of a in lanes 0..15 and of b in lanes 16..31.
+__device__ __forceinline__ double warp_sum_pair(double a, double b) {
+    const bool hi = (threadIdx.x & 16) != 0;
+    double v = hi ? b : a;
+    v += __shfl_xor_sync(0xffffffffu, hi ? a : b, 16);
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One op of a segment on the thread's group (base gb, segment bit masks m0,
+// m1).  Dots are summed over the group's two pairs, then over the warp, and
+// added to the warp's slot.
 template <int S>
 __device__ __forceinline__ void seg_op(const AdjOpCtl& c, const AdjTileOp& op, double2 (&x)[4], double2 (&l)[4],
-                                       const uint32_t (&li)[4], double* __restrict__ acc, uint32_t nw, bool valid) {
+                                       uint32_t gb, uint32_t m0, uint32_t m1, bool valid, double* __restrict__ acc,
+                                       uint32_t nw) {
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (c.cls == kAdjFused) {
         // G'_j = A^dagger G_j A is anti-Hermitian like the generators
@@ -330,7 +346,8 @@ __device__ __forceinline__ void seg_op(const AdjOpCtl& c, const AdjTileOp& op, d
                 for (int j = 0; j < kAdjFusedGens; j++)
                     if (j < ng) {
                         const double2 g01 = op.m[5 + 4 * j];
-                        dot[j] += fma(-op.m[4 + 4 * j].y, i00, fma(-op.m[7 + 4 * j].y, i11, fma(g01.x, qx, -g01.y * qy)));
+                        dot[j] += fma(-op.m[4 + 4 * j].y, i00,
+                                      fma(-op.m[7 + 4 * j].y, i11, fma(g01.x, qx, -g01.y * qy)));
                     }
             }
             if (apply) {
@@ -341,12 +358,19 @@ __device__ __forceinline__ void seg_op(const AdjOpCtl& c, const AdjTileOp& op, d
                 l[ib] = cfma2(cmul2(a2, l0), a3, l1);
             }
         }
-#pragma unroll
-        for (int j = 0; j < kAdjFusedGens; j++)
-            if (j < ng) {
-                const double d = warp_sum(dot[j]);
-                if (lane == 0) acc[c.gslot[j] * nw + warp] += d;
+        if (ng >= 2) {
+            const double d = warp_sum_pair(dot[0], dot[1]);
+            if (lane == 0) acc[c.gslot[0] * nw + warp] += d;
+            __syncwarp();  // (the two slots may coincide)
+            if (lane == 16) acc[c.gslot[1] * nw + warp] += d;
+            if (ng == 3) {
+                const double d2 = warp_sum(dot[2]);
+                if (lane == 0) acc[c.gslot[2] * nw + warp] += d2;
             }
+        } else if (ng == 1) {
+            const double d = warp_sum(dot[0]);
+            if (lane == 0) acc[c.gslot[0] * nw + warp] += d;
+        }
         return;
     }
     double dot = 0.0;
@@ -354,7 +378,10 @@ __device__ __forceinline__ void seg_op(const AdjOpCtl& c, const AdjTileOp& op, d
     for (int q = 0; q < 2; q++) {
         int ia, ib;
         seg_pair_idx<S>(q, ia, ib);
-        if ((li[ia] & c.lcmask) != c.lcval) continue;
+        // local index of the pair's first amplitude: the group base with
+        // the other segment bit q
+        const uint32_t la = gb | (q ? (S == 0 ? m1 : m0) : 0u);
+        if ((la & c.lcmask) != c.lcval) continue;
         if (c.gen) {
             if (!valid) continue;
             const double2 y0 = cfma2(cmul2(op.m[0], x[ia]), op.m[1], x[ib]);
@@ -394,17 +421,17 @@ __device__ __forceinline__ void adj_seg(const AdjTileOp* __restrict__ sops, int 
                                         double2* __restrict__ sp, double2* __restrict__ sl, uint32_t T,
                                         double* __restrict__ acc, uint32_t nw) {
     const int p0 = sops[0].seg[0], p1 = sops[0].seg[1];
+    const uint32_t m0 = 1u << p0, m1 = 1u << p1;
     const uint32_t g = threadIdx.x;
     const bool valid = g < (T >> 2);
-    const uint32_t b = valid ? adj_ins0(adj_ins0(g, p0), p1) : 0u;
-    uint32_t li[4];
+    const uint32_t gb = valid ? adj_ins0(adj_ins0(g, p0), p1) : 0u;
     double2 x[4], l[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        li[q] = b | ((uint32_t)(q & 1) << p0) | ((uint32_t)(q >> 1) << p1);
+        const uint32_t li = gb | ((q & 1) ? m0 : 0u) | ((q & 2) ? m1 : 0u);
         if (valid) {
-            x[q] = sp[adj_swz(li[q])];
-            l[q] = sl[adj_swz(li[q])];
+            x[q] = sp[adj_swz(li)];
+            l[q] = sl[adj_swz(li)];
         } else {
             x[q] = l[q] = make_double2(0.0, 0.0);
         }
@@ -414,15 +441,16 @@ __device__ __forceinline__ void adj_seg(const AdjTileOp* __restrict__ sops, int 
         const AdjOpCtl c = static_cast<const AdjOpCtl&>(op);  // four 16-byte loads
         if ((base & c.gcmask) != c.gcval) continue;  // uniform over the tile
         if (c.tl[0] == p0)
-            seg_op<0>(c, op, x, l, li, acc, nw, valid);
+            seg_op<0>(c, op, x, l, gb, m0, m1, valid, acc, nw);
         else
-            seg_op<1>(c, op, x, l, li, acc, nw, valid);
+            seg_op<1>(c, op, x, l, gb, m0, m1, valid, acc, nw);
     }
     if (valid)
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            sp[adj_swz(li[q])] = x[q];
-            sl[adj_swz(li[q])] = l[q];
+            const uint32_t li = gb | ((q & 1) ? m0 : 0u) | ((q & 2) ? m1 : 0u);
+            sp[adj_swz(li)] = x[q];
+            sl[adj_swz(li)] = l[q];
         }
 }
 

@@ -1240,12 +1240,12 @@ int yao_expect_grad(const yao_term* terms, size_t nterms, const yao_circuit* cc,
         plan.p = adjoint_plan_new(c, psi0->nbits, YAO_C128, np, &pst);
         if (!plan.p && pst != YAO_ERR_UNSUPPORTED) return pst;
     }
-    ExpectPending pend;
-    s = expect_terms_launch(ctx, &psi_r, mt, pend);
-    if (s) return s;
-    std::vector<Cx> vals;
-    auto energy = [&]() {
-        expect_terms_collect(ctx, pend, vals);
+    if (np == 0) {
+        std::vector<Cx> vals;
+        s = read_device_err(ctx, "expect_grad");
+        if (s) return s;
+        s = expect_terms(ctx, &psi_r, mt, vals);
+        if (s) return s;
         Cx acc{0, 0};
         for (size_t t = 0; t < mt.size(); t++) {
             Cx p = cxmul(mt[t].coeff, vals[t]);
@@ -1253,13 +1253,7 @@ int yao_expect_grad(const yao_term* terms, size_t nterms, const yao_circuit* cc,
             acc.im += p.im;
         }
         *value = acc.re;
-    };
-    if (np == 0 || !plan.p) {
-        // the per-gate form reuses the reduction buffers: collect first
-        s = read_device_err(ctx, "expect_grad");
-        if (s) return s;
-        energy();
-        if (np == 0) return YAO_OK;
+        return YAO_OK;
     }
     if (cudaMallocAsync(&pool.b, bytes, ctx->stream) != cudaSuccess) {
         cudaGetLastError();
@@ -1269,15 +1263,21 @@ int yao_expect_grad(const yao_term* terms, size_t nterms, const yao_circuit* cc,
     lam_r.d = pool.b;
     Reg* psi = &psi_r;
     Reg* lam = &lam_r;
-    s = build_lambda(ctx, psi, mt, lam);
+    // lambda = H psi, and the energy Re <psi|lambda> = <psi|H|psi>.re in the
+    // same pass (read back with the gradient)
+    s = build_lambda_energy(ctx, psi, mt, lam);
     if (s) return s;
     // reverse sweep over shared-memory tiles of psi and lambda
     if (plan.p) {
         s = adjoint_run(ctx, psi, lam, plan.p, grad);
         if (s) return s;
-        energy();  // adjoint_run synchronised
+        *value = lambda_energy_collect(ctx);  // adjoint_run synchronised
         return YAO_OK;
     }
+    // the per-gate form reuses the reduction buffers: collect first
+    s = read_device_err(ctx, "expect_grad");
+    if (s) return s;
+    *value = lambda_energy_collect(ctx);
     size_t slot = np;
     for (size_t ei = c->elems.size(); ei-- > 0;) {
         const Element& el = c->elems[ei];

@@ -586,18 +586,63 @@ struct MonoFull {
     double2 c;
 };
 
-__global__ void __launch_bounds__(256) k_lambda(const double2* __restrict__ psi, double2* __restrict__ lam, uint64_t n,
-                                               const MonoFull* __restrict__ terms, int nt) {
-    GRID_STRIDE(i, n) {
-        double2 acc = make_double2(0.0, 0.0);
-        for (int t = 0; t < nt; t++) {
-            const MonoFull& m = terms[t];
-            int q = mono_phase(m.t, i);
-            double2 v = q >= 0 ? qturn(psi[i ^ m.xmask], q) : make_double2(0.0, 0.0);
-            acc = cadd_x(acc, cmul_x(m.c, v));
+// i^q * v for q in 0..3 without branches (the same values as qturn: every
+// step is a swap or a negation, exact)
+__device__ __forceinline__ double2 qturn_sel(double2 v, int q) {
+    const double2 w = (q & 1) ? make_double2(-v.y, v.x) : v;
+    return (q & 2) ? make_double2(-w.x, -w.y) : w;
+}
+
+// Each thread builds kLamR amplitudes of lambda (256 apart, coalesced), so a
+// term's fields are read once per kLamR amplitudes.  PAULI: every term is a
+// Pauli string (factors I, X, Y, Z), whose phase at index i is
+// i^(base + 2 popc(i & d2)) (no projector masks, no quarter-turn mask).
+// ENERGY: also Re <psi | lambda> = <psi|H|psi>.re (ad.rs:87) per block, in
+// the block's fixed order, into partial[blockIdx.x].
+constexpr int kLamR = 4;
+template <bool PAULI, bool ENERGY>
+__global__ void __launch_bounds__(kRT) k_lambda(const double2* __restrict__ psi, double2* __restrict__ lam, uint64_t n,
+                                               const MonoFull* __restrict__ terms, int nt,
+                                               double* __restrict__ partial) {
+    __shared__ double sm[kRT / 32];
+    double e = 0.0;
+    const uint64_t span = (uint64_t)kRT * kLamR;
+    const uint64_t nchunks = (n + span - 1) / span;
+    for (uint64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+        uint64_t idx[kLamR];
+        double2 acc[kLamR];
+#pragma unroll
+        for (int k = 0; k < kLamR; k++) {
+            idx[k] = ch * span + (uint64_t)k * kRT + threadIdx.x;
+            acc[k] = make_double2(0.0, 0.0);
         }
-        lam[i] = acc;
+        for (int t = 0; t < nt; t++) {
+            const MonoFull m = terms[t];
+#pragma unroll
+            for (int k = 0; k < kLamR; k++) {
+                if (idx[k] >= n) continue;
+                const uint64_t i = idx[k];
+                double2 v;
+                if (PAULI) {
+                    v = qturn_sel(psi[i ^ m.xmask], (m.t.base + 2 * __popcll(i & m.t.d2)) & 3);
+                } else {
+                    const int q = mono_phase(m.t, i);
+                    v = q >= 0 ? qturn_sel(psi[i ^ m.xmask], q) : make_double2(0.0, 0.0);
+                }
+                acc[k] = cadd_x(acc[k], cmul_x(m.c, v));
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kLamR; k++) {
+            if (idx[k] >= n) continue;
+            lam[idx[k]] = acc[k];
+            if (ENERGY) {
+                const double2 p = psi[idx[k]];
+                e += p.x * acc[k].x + p.y * acc[k].y;
+            }
+        }
     }
+    if (ENERGY) block_sum_write(&e, 1, sm, partial + blockIdx.x);
 }
 
 int build_lambda(Ctx* ctx, const Reg* psi, const std::vector<MonoTerm>& terms, Reg* lambda) {
@@ -606,30 +651,72 @@ int build_lambda(Ctx* ctx, const Reg* psi, const std::vector<MonoTerm>& terms, R
 
 // nsets registers back to back: every mask lies below the register-index
 // bits, so one pass over all nsets * 2^nbits amplitudes builds every lambda.
-int build_lambda_sets(Ctx* ctx, const void* psi_d, void* lam_d, uint32_t nbits, uint64_t nsets,
-                      const std::vector<MonoTerm>& terms) {
-    uint64_t n = nsets << nbits;
+// With `energy`, one register (nsets == 1): Re <psi|lambda> is reduced in the
+// same pass, its final sum queued for a copy into ctx->host_pinned[0]
+// (read it after the stream has passed the copy: lambda_energy_collect).
+static int lambda_launch(Ctx* ctx, const void* psi_d, void* lam_d, uint32_t nbits, uint64_t nsets,
+                         const std::vector<MonoTerm>& terms, bool energy) {
+    const uint64_t n = nsets << nbits;
     std::vector<MonoFull> h(terms.size());
+    bool pauli = true;
     for (size_t t = 0; t < terms.size(); t++) {
         h[t].t = to_dev(terms[t]);
         h[t].xmask = terms[t].xmask;
         h[t].c = make_double2(terms[t].coeff.re, terms[t].coeff.im);
+        const MonoDev& d = h[t].t;
+        pauli = pauli && d.d1 == 0 && d.need0 == 0 && d.need1 == 0 && d.zero == 0;
     }
     void* d = nullptr;
     size_t bytes = std::max<size_t>(1, h.size()) * sizeof(MonoFull);
     YAO_CUDA(cudaMallocAsync(&d, bytes, ctx->stream));
     if (!h.empty()) YAO_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(MonoFull), cudaMemcpyHostToDevice, ctx->stream));
+    const unsigned grid = grid_for((n + kLamR - 1) / kLamR, kRT, ctx->num_sms);
+    double* part = nullptr;
+    if (energy) {
+        if (ctx->ensure_scratch(sizeof(double) * (grid + 1)) || ctx->ensure_host_pinned(sizeof(double))) {
+            cudaFreeAsync(d, ctx->stream);
+            return YAO_ERR_OUT_OF_MEMORY;
+        }
+        part = (double*)ctx->scratch;
+    }
     {
         // reads psi once per distinct X mask (the low ones hit L2), writes lambda
         ProfScope prof(ctx, "lambda", (double)n * 32.0);
-        k_lambda<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>((const double2*)psi_d, (double2*)lam_d, n,
-                                                                           (const MonoFull*)d, (int)h.size());
+        const double2* ps = (const double2*)psi_d;
+        double2* ls = (double2*)lam_d;
+        const MonoFull* td = (const MonoFull*)d;
+        const int nt = (int)h.size();
+        if (pauli && energy)
+            k_lambda<true, true><<<grid, kRT, 0, ctx->stream>>>(ps, ls, n, td, nt, part);
+        else if (pauli)
+            k_lambda<true, false><<<grid, kRT, 0, ctx->stream>>>(ps, ls, n, td, nt, part);
+        else if (energy)
+            k_lambda<false, true><<<grid, kRT, 0, ctx->stream>>>(ps, ls, n, td, nt, part);
+        else
+            k_lambda<false, false><<<grid, kRT, 0, ctx->stream>>>(ps, ls, n, td, nt, part);
     }
     ctx->launches++;
     YAO_CUDA(cudaGetLastError());
     YAO_CUDA(cudaFreeAsync(d, ctx->stream));
+    if (energy) {
+        k_final_sum<<<1, kRT, 0, ctx->stream>>>(part, (int)grid, 1, part + grid);
+        ctx->launches++;
+        YAO_CUDA(cudaGetLastError());
+        YAO_CUDA(cudaMemcpyAsync(ctx->host_pinned, part + grid, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
     return YAO_OK;
 }
+
+int build_lambda_sets(Ctx* ctx, const void* psi_d, void* lam_d, uint32_t nbits, uint64_t nsets,
+                      const std::vector<MonoTerm>& terms) {
+    return lambda_launch(ctx, psi_d, lam_d, nbits, nsets, terms, false);
+}
+
+int build_lambda_energy(Ctx* ctx, const Reg* psi, const std::vector<MonoTerm>& terms, Reg* lambda) {
+    return lambda_launch(ctx, psi->d, lambda->d, psi->nbits, 1, terms, true);
+}
+
+double lambda_energy_collect(Ctx* ctx) { return ((const double*)ctx->host_pinned)[0]; }
 
 // ------------------------------------------------------------- adjoint
 

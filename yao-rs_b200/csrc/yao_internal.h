@@ -253,6 +253,11 @@ int expect_noalloc(Ctx* ctx, const Reg* r, const yao_term* terms, size_t nterms,
 int build_lambda(Ctx* ctx, const Reg* psi, const std::vector<MonoTerm>& terms, Reg* lambda);
 int build_lambda_sets(Ctx* ctx, const void* psi_d, void* lam_d, uint32_t nbits, uint64_t nsets,
                       const std::vector<MonoTerm>& terms);
+// lambda = H psi and, in the same pass, Re <psi|lambda> = <psi|H|psi>.re,
+// queued for ctx->host_pinned[0]; lambda_energy_collect reads it once the
+// stream has passed that copy (sv_reduce.cu).
+int build_lambda_energy(Ctx* ctx, const Reg* psi, const std::vector<MonoTerm>& terms, Reg* lambda);
+double lambda_energy_collect(Ctx* ctx);
 // A gate on nsets complex128 registers of nbits qubits stored back to back.
 int launch_gate_sets(Ctx* ctx, void* state, uint32_t nbits, const LGate& g, uint64_t nsets);
 // Energies and adjoint gradients of nsets parameter vectors of one circuit.
