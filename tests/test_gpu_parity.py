@@ -831,7 +831,8 @@ def test_fp64_tensor_core_blocks(monkeypatch, n, k, tbits, rb):
 
 
 SWEEP_FORMS = {"segments": {}, "one_op": {"YAO_ADJ_SEGMENTS": "0"}, "in_order": {"YAO_ADJ_REORDER": "0"},
-               "in_order_one_op": {"YAO_ADJ_REORDER": "0", "YAO_ADJ_SEGMENTS": "0"}}
+               "in_order_one_op": {"YAO_ADJ_REORDER": "0", "YAO_ADJ_SEGMENTS": "0"},
+               "segments_per_lane_controls": {"YAO_ADJ_UPAIR": "0"}}
 
 
 @pytest.mark.parametrize("form", list(SWEEP_FORMS))

@@ -15,9 +15,9 @@
 // steps on other qubits), and within the pass consecutive 1-qubit steps on
 // at most two target bits form a register segment: each thread keeps its
 // 4-amplitude group of both tiles in registers across the segment.  Dots are
-// reduced over the warp, added per warp in shared memory (tiles of a CTA in a
-// fixed order), summed over warps per CTA and over CTAs in block order:
-// deterministic for a given launch shape.  Arithmetic is FP64 with FMA; the
+// reduced over the warp down to four partial sums, added per warp in shared
+// memory (tiles of a CTA in a fixed order), summed over warps per CTA and
+// over CTAs in block order: deterministic for a given launch shape.  Arithmetic is FP64 with FMA; the
 // result is the reverse sweep of the per-gate form up to rounding (~1e-15
 // relative).
 #include <algorithm>
@@ -59,7 +59,8 @@ struct __align__(16) AdjOpCtl {
     int8_t sync;     // barrier after this op (the next op moves amplitudes along other bits)
     int8_t ngen;     // kAdjFused: generator dots of the run
     int8_t seg[2];   // 1-qubit ops: the segment's two local positions (seg[0] < seg[1])
-    int8_t pad[2];
+    int8_t upair;    // segment op whose only in-tile control is the other segment bit: 1 + that bit's value
+    int8_t pad[1];
     int32_t gslot[kAdjFusedGens];
     int32_t a_id;    // kAdjFused: A is the identity (no U^dagger in the run)
     uint32_t lcmask, lcval;  // in-tile controls (local positions)
@@ -102,6 +103,37 @@ __device__ __forceinline__ double2 cmul2(double2 a, double2 x) {
 }
 // Re(conj(l) * y)
 __device__ __forceinline__ double redot(double2 l, double2 y) { return fma(l.x, y.x, l.y * y.y); }
+
+// Dot accumulators: kAdjSub per warp and slot, acc[(slot * nw + warp) *
+// kAdjSub + sub].  A dot is summed over the warp only down to kAdjSub
+// partial sums (three shuffle rounds instead of five); the CTA adds them up
+// once, in a fixed order, after its last tile.
+constexpr int kAdjSub = 4;
+
+// Lanes 0..3 return the sums over lanes {i, i + 4, ..., i + 28}.
+__device__ __forceinline__ double warp_part(double v) {
+#pragma unroll
+    for (int o = 16; o >= kAdjSub; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Two values in three rounds: after the exchange across the half warps,
+// lanes 0..15 carry partial sums of a and lanes 16..31 of b; lanes 0..3
+// return the partial sums of a, lanes 16..19 those of b.
+__device__ __forceinline__ double warp_part_pair(double a, double b) {
+    const bool hi = (threadIdx.x & 16) != 0;
+    double v = hi ? b : a;
+    v += __shfl_xor_sync(0xffffffffu, hi ? a : b, 16);
+#pragma unroll
+    for (int o = 8; o >= kAdjSub; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// The warp's partial sums of one dot into its accumulators (lanes 0..3).
+__device__ __forceinline__ void acc_part(double* __restrict__ acc, int slot, uint32_t nw, double d) {
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane < (uint32_t)kAdjSub) acc[((uint32_t)slot * nw + warp) * kAdjSub + lane] += d;
+}
 
 // One reverse-sweep op on the groups of the tile owned by this thread.
 // A run of up to kAdjRun consecutive ops on the same target positions (in
@@ -200,13 +232,9 @@ __device__ __forceinline__ void adj_run(const AdjTileOp* __restrict__ rops, int 
             sl[idx[q]] = l[q];
         }
     }
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
     for (int j = 0; j < kAdjRun; j++)
-        if (on[j] && rops[j].gen) {
-            const double d = warp_sum(dot[j]);
-            if (lane == 0) acc[rops[j].slot * nw + warp] += d;
-        }
+        if (on[j] && rops[j].gen) acc_part(acc, rops[j].slot, nw, warp_part(dot[j]));
 }
 
 // A run of one X step (the CNOTs of the sweep: X on one target under
@@ -274,13 +302,9 @@ __device__ __forceinline__ void adj_fused1(const AdjTileOp& op, double2* __restr
             sl[i1] = cfma2(cmul2(a2, l0), a3, l1);
         }
     }
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
     for (int j = 0; j < kAdjFusedGens; j++)
-        if (j < ng) {
-            const double d = warp_sum(dot[j]);
-            if (lane == 0) acc[op.gslot[j] * nw + warp] += d;
-        }
+        if (j < ng) acc_part(acc, op.gslot[j], nw, warp_part(dot[j]));
 }
 
 // A segment: consecutive 1-qubit ops of a pass whose targets lie on two
@@ -303,16 +327,41 @@ __device__ __forceinline__ void seg_pair_idx(int q, int& a, int& b) {
     }
 }
 
-// Two warp sums in five shuffle rounds: after the exchange across the half
-// warps, lanes 0..15 carry partial sums of a and lanes 16..31 of b; the
-// returned value is the sum of a in lanes 0..15 and of b in lanes 16..31.
-__device__ __forceinline__ double warp_sum_pair(double a, double b) {
-    const bool hi = (threadIdx.x & 16) != 0;
-    double v = hi ? b : a;
-    v += __shfl_xor_sync(0xffffffffu, hi ? a : b, 16);
-#pragma unroll
-    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
+// A non-folded segment op on pair Q of the group (its controls checked by
+// the caller): a generator dot, or U^dagger on psi and lambda.
+template <int S, int Q>
+__device__ __forceinline__ void seg_pair(const AdjOpCtl& c, const AdjTileOp& op, double2 (&x)[4], double2 (&l)[4],
+                                         bool valid, double& dot) {
+    int ia, ib;
+    seg_pair_idx<S>(Q, ia, ib);
+    if (c.gen) {
+        if (!valid) return;
+        const double2 y0 = cfma2(cmul2(op.m[0], x[ia]), op.m[1], x[ib]);
+        const double2 y1 = cfma2(cmul2(op.m[2], x[ia]), op.m[3], x[ib]);
+        dot += redot(l[ia], y0) + redot(l[ib], y1);
+    } else if (c.cls == GC_X) {
+        double2 t = x[ia];
+        x[ia] = x[ib];
+        x[ib] = t;
+        t = l[ia];
+        l[ia] = l[ib];
+        l[ib] = t;
+    } else if (c.cls == GC_DIAG) {
+        if (op.active & 1) {
+            x[ia] = cmul2(op.m[0], x[ia]);
+            l[ia] = cmul2(op.m[0], l[ia]);
+        }
+        if (op.active & 2) {
+            x[ib] = cmul2(op.m[1], x[ib]);
+            l[ib] = cmul2(op.m[1], l[ib]);
+        }
+    } else {
+        const double2 x0 = x[ia], x1 = x[ib], l0 = l[ia], l1 = l[ib];
+        x[ia] = cfma2(cmul2(op.m[0], x0), op.m[1], x1);
+        x[ib] = cfma2(cmul2(op.m[2], x0), op.m[3], x1);
+        l[ia] = cfma2(cmul2(op.m[0], l0), op.m[1], l1);
+        l[ib] = cfma2(cmul2(op.m[2], l0), op.m[3], l1);
+    }
 }
 
 // One op of a segment on the thread's group (base gb, segment bit masks m0,
@@ -359,62 +408,32 @@ __device__ __forceinline__ void seg_op(const AdjOpCtl& c, const AdjTileOp& op, d
             }
         }
         if (ng >= 2) {
-            const double d = warp_sum_pair(dot[0], dot[1]);
-            if (lane == 0) acc[c.gslot[0] * nw + warp] += d;
+            const double d = warp_part_pair(dot[0], dot[1]);
+            acc_part(acc, c.gslot[0], nw, d);
             __syncwarp();  // (the two slots may coincide)
-            if (lane == 16) acc[c.gslot[1] * nw + warp] += d;
-            if (ng == 3) {
-                const double d2 = warp_sum(dot[2]);
-                if (lane == 0) acc[c.gslot[2] * nw + warp] += d2;
-            }
+            if ((lane & 16) && (lane & 15) < (uint32_t)kAdjSub)
+                acc[((uint32_t)c.gslot[1] * nw + warp) * kAdjSub + (lane & 15)] += d;
+            if (ng == 3) acc_part(acc, c.gslot[2], nw, warp_part(dot[2]));
         } else if (ng == 1) {
-            const double d = warp_sum(dot[0]);
-            if (lane == 0) acc[c.gslot[0] * nw + warp] += d;
+            acc_part(acc, c.gslot[0], nw, warp_part(dot[0]));
         }
         return;
     }
     double dot = 0.0;
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-        int ia, ib;
-        seg_pair_idx<S>(q, ia, ib);
-        // local index of the pair's first amplitude: the group base with
-        // the other segment bit q
-        const uint32_t la = gb | (q ? (S == 0 ? m1 : m0) : 0u);
-        if ((la & c.lcmask) != c.lcval) continue;
-        if (c.gen) {
-            if (!valid) continue;
-            const double2 y0 = cfma2(cmul2(op.m[0], x[ia]), op.m[1], x[ib]);
-            const double2 y1 = cfma2(cmul2(op.m[2], x[ia]), op.m[3], x[ib]);
-            dot += redot(l[ia], y0) + redot(l[ib], y1);
-        } else if (c.cls == GC_X) {
-            double2 t = x[ia];
-            x[ia] = x[ib];
-            x[ib] = t;
-            t = l[ia];
-            l[ia] = l[ib];
-            l[ib] = t;
-        } else if (c.cls == GC_DIAG) {
-            if (op.active & 1) {
-                x[ia] = cmul2(op.m[0], x[ia]);
-                l[ia] = cmul2(op.m[0], l[ia]);
-            }
-            if (op.active & 2) {
-                x[ib] = cmul2(op.m[1], x[ib]);
-                l[ib] = cmul2(op.m[1], l[ib]);
-            }
-        } else {
-            const double2 x0 = x[ia], x1 = x[ib], l0 = l[ia], l1 = l[ib];
-            x[ia] = cfma2(cmul2(op.m[0], x0), op.m[1], x1);
-            x[ib] = cfma2(cmul2(op.m[2], x0), op.m[3], x1);
-            l[ia] = cfma2(cmul2(op.m[0], l0), op.m[1], l1);
-            l[ib] = cfma2(cmul2(op.m[2], l0), op.m[3], l1);
-        }
+    if (c.upair) {
+        // the only in-tile control is the other segment bit: one pair, the
+        // same in every lane
+        if (c.upair == 1)
+            seg_pair<S, 0>(c, op, x, l, valid, dot);
+        else
+            seg_pair<S, 1>(c, op, x, l, valid, dot);
+    } else {
+        // local index of a pair's first amplitude: the group base with the
+        // other segment bit q
+        if ((gb & c.lcmask) == c.lcval) seg_pair<S, 0>(c, op, x, l, valid, dot);
+        if (((gb | (S == 0 ? m1 : m0)) & c.lcmask) == c.lcval) seg_pair<S, 1>(c, op, x, l, valid, dot);
     }
-    if (c.gen) {
-        const double d = warp_sum(dot);
-        if (lane == 0) acc[c.slot * nw + warp] += d;
-    }
+    if (c.gen) acc_part(acc, c.slot, nw, warp_part(dot));
 }
 
 __device__ __forceinline__ void adj_seg(const AdjTileOp* __restrict__ sops, int nr, uint64_t base,
@@ -487,13 +506,13 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
     unsigned char* smem = adj_smem + ((1024u - (tc::smem_u32(adj_smem) & 1023u)) & 1023u);
     const uint32_t tile_bytes = T * (uint32_t)sizeof(double2);  // one array's tile
     AdjTileOp* ops = (AdjTileOp*)(smem + (size_t)nbuf * 2 * tile_bytes);
-    double* acc = (double*)(ops + hdr.nops);  // [slot][warp]
+    double* acc = (double*)(ops + hdr.nops);  // [slot][warp][kAdjSub]
     const int nlow = min(kAdjLowBits, hdr.tbits), nh = hdr.tbits - nlow;
     {
         const uint64_t* src = (const uint64_t*)gops;
         uint64_t* dst = (uint64_t*)ops;
         for (int i = threadIdx.x; i < hdr.nops * (int)(sizeof(AdjTileOp) / 8); i += blockDim.x) dst[i] = src[i];
-        for (int i = threadIdx.x; i < hdr.nslots * (int)nw; i += blockDim.x) acc[i] = 0.0;
+        for (int i = threadIdx.x; i < hdr.nslots * (int)nw * kAdjSub; i += blockDim.x) acc[i] = 0.0;
         for (uint32_t h = threadIdx.x; h < (1u << nh); h += blockDim.x) {
             uint64_t o = 0;
             for (int j = 0; j < nh; j++) o |= (uint64_t)((h >> j) & 1) << hdr.hb[j];
@@ -632,10 +651,10 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
                     }
     }
     __syncthreads();
-    // per CTA: slot sums over warps in order
+    // per CTA: slot sums over the warps' partial sums in order
     for (int sidx = threadIdx.x; sidx < hdr.nslots; sidx += blockDim.x) {
         double s = 0.0;
-        for (uint32_t w = 0; w < nw; w++) s += acc[sidx * nw + w];
+        for (uint32_t w = 0; w < nw * kAdjSub; w++) s += acc[sidx * nw * kAdjSub + w];
         partial[(size_t)blockIdx.x * hdr.nslots + sidx] = s;
     }
 }
@@ -870,6 +889,11 @@ static std::vector<size_t> segment_order(const std::vector<HostOp>& hops, const 
 // second one added when the run uses one), a barrier after the last.  Runs
 // of 2-qubit ops (and, segments off, of 1-qubit ops) on the same positions
 // share a barrier up to kAdjRun ops; fused ops stand alone.
+static bool upair_on() {
+    const char* e = getenv("YAO_ADJ_UPAIR");
+    return !(e && e[0] == '0');
+}
+
 static void mark_barriers(std::vector<AdjTileOp>& ops, bool seg) {
     size_t i = 0;
     while (i < ops.size()) {
@@ -888,6 +912,10 @@ static void mark_barriers(std::vector<AdjTileOp>& ops, bool seg) {
                 ops[q].seg[0] = (int8_t)lo;
                 ops[q].seg[1] = (int8_t)hi;
                 ops[q].sync = (int8_t)(q + 1 == j ? 1 : 0);
+                const uint32_t other = 1u << (ops[q].tl[0] == lo ? hi : lo);
+                ops[q].upair = (int8_t)(upair_on() && ops[q].cls != kAdjFused && ops[q].lcmask == other
+                                            ? 1 + (ops[q].lcval != 0)
+                                            : 0);
             }
             i = j;
             continue;
@@ -1078,11 +1106,17 @@ int adjoint_run(Ctx* ctx, Reg* psi, Reg* lam, const AdjPlan* plan, double* grad)
     if (passes.empty()) return read_device_err(ctx, "expect_grad");
     const int tbits = passes[0].hdr.tbits;
     const size_t tile_bytes = (size_t)2 * ((size_t)1 << tbits) * sizeof(double2);  // psi's and lambda's tile
-    // shared memory: the tile buffers (two when they fit), every op and slot
-    // of the largest pass, 1 KiB for aligning the tiles
+    // shared memory: the tile buffers (three when they fit), the ops and
+    // slot accumulators of the largest pass, 1 KiB for aligning the tiles
     static int optin = 0;
     if (!optin) YAO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-    const size_t rest = kAdjMaxOps * sizeof(AdjTileOp) + (size_t)kAdjMaxSlots * (kAdjThreads / 32) * 8 + 1024;
+    size_t max_ops = 0, max_slots = 0;
+    for (const AdjPass& p : passes) {
+        max_ops = std::max(max_ops, p.ops.size());
+        max_slots = std::max(max_slots, p.slot_grad.size());
+    }
+    const size_t slot_bytes = (size_t)(kAdjThreads / 32) * kAdjSub * sizeof(double);
+    const size_t rest = max_ops * sizeof(AdjTileOp) + max_slots * slot_bytes + 1024;
     const size_t budget = (size_t)optin - 4096;  // static shared memory of the kernel
     const int nstage = 3 * tile_bytes + rest <= budget ? 3 : (2 * tile_bytes + rest <= budget ? 2 : 1);
     const size_t smem_max = (size_t)nstage * tile_bytes + rest;
@@ -1130,7 +1164,7 @@ int adjoint_run(Ctx* ctx, Reg* psi, Reg* lam, const AdjPlan* plan, double* grad)
                           : 0;
         hdr.nstage = hdr.use_tma ? nstage : 1;
         const size_t smem = 1024 + (size_t)(hdr.use_tma ? nstage : 1) * tile_bytes + p.ops.size() * sizeof(AdjTileOp) +
-                            (size_t)p.slot_grad.size() * (kAdjThreads / 32) * 8;
+                            p.slot_grad.size() * slot_bytes;
         {
             ProfScope prof(ctx, "adjoint_tiles", (double)((uint64_t)1 << n) * 4.0 * sizeof(double2));
             k_adjoint_tiles<<<grid, kAdjThreads, smem, ctx->stream>>>((double2*)psi->d, (double2*)lam->d, hdr,

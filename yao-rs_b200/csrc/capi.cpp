@@ -31,6 +31,20 @@ int cuda_fail(cudaError_t e, const char* what) {
 }
 
 // ----------------------------------------------------------------- context
+// cudaMalloc; when it fails, the freed memory that the device's default pool
+// keeps is released (after this context's queued frees) and it is tried once
+// more.
+static cudaError_t alloc_device(Ctx* ctx, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaErrorMemoryAllocation) return e;
+    cudaGetLastError();
+    cudaMemPool_t pool;
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess ||
+        cudaDeviceGetDefaultMemPool(&pool, ctx->device) != cudaSuccess || cudaMemPoolTrimTo(pool, 0) != cudaSuccess)
+        return e;
+    return cudaMalloc(p, bytes);
+}
+
 int Ctx::ensure_scratch(size_t bytes) {
     if (bytes <= scratch_bytes) return 0;
     size_t nb = std::max<size_t>(bytes, 1 << 20);
@@ -40,7 +54,8 @@ int Ctx::ensure_scratch(size_t bytes) {
         scratch = nullptr;
         scratch_bytes = 0;
     }
-    if (cudaMalloc(&scratch, nb) != cudaSuccess) {
+    if (alloc_device(this, &scratch, nb) != cudaSuccess) {
+        cudaGetLastError();
         scratch = nullptr;
         fail(YAO_ERR_OUT_OF_MEMORY, "cannot allocate reduction scratch");
         return -1;
@@ -264,7 +279,7 @@ static int alloc_reg(Ctx* ctx, uint32_t nbits, int32_t prec, Reg** out) {
     r->ctx = ctx;
     r->nbits = nbits;
     r->precision = prec;
-    cudaError_t e = cudaMalloc(&r->d, r->bytes());
+    cudaError_t e = alloc_device(ctx, &r->d, r->bytes());
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(YAO_ERR_OUT_OF_MEMORY, "cannot allocate a " + std::to_string(nbits) + "-qubit register (" +
@@ -281,7 +296,7 @@ static int alloc_dm(Ctx* ctx, uint32_t nbits, DM** out) {
     std::unique_ptr<yao_dm> d(new yao_dm());
     d->ctx = ctx;
     d->nbits = nbits;
-    if (cudaMalloc(&d->d, d->bytes()) != cudaSuccess) {
+    if (alloc_device(ctx, &d->d, d->bytes()) != cudaSuccess) {
         cudaGetLastError();
         return fail(YAO_ERR_OUT_OF_MEMORY, "cannot allocate the density matrix");
     }
@@ -332,6 +347,14 @@ int yao_ctx_create(int device, yao_ctx** out) {
     std::unique_ptr<yao_ctx> c(new yao_ctx());
     c->device = device;
     YAO_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    // the stream-ordered work buffers (expect_grad's psi and lambda, tile
+    // tables) come from the device's default pool: let it keep up to 4 GiB
+    // of freed memory across calls instead of unmapping it at every
+    // synchronisation (alloc_device trims it when an allocation fails)
+    cudaMemPool_t pool;
+    YAO_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = (uint64_t)4 << 30;
+    YAO_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     int sms = 0;
     YAO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     c->num_sms = sms;

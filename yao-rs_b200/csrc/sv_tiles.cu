@@ -2303,6 +2303,27 @@ static std::string tune_key(int device, uint32_t nbits, int32_t prec, int32_t mo
     return b;
 }
 
+// FNV-1a over a program's structure (gate classes, target and control bits;
+// not the matrix entries): circuits that differ only in their parameters
+// share a tuned configuration, other circuits of the same size do not.
+static uint64_t program_shape_hash(const std::vector<LGate>& prog) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&h](uint64_t v) {
+        for (int i = 0; i < 8; i++) {
+            h ^= (v >> (8 * i)) & 0xff;
+            h *= 1099511628211ull;
+        }
+    };
+    mix(prog.size());
+    for (const LGate& g : prog) {
+        mix((uint64_t)(uint32_t)g.cls | (uint64_t)(uint32_t)g.k << 32);
+        for (int i = 0; i < g.k; i++) mix((uint64_t)(uint32_t)g.tb[i]);
+        mix(g.cmask());
+        mix(g.cval());
+    }
+    return h;
+}
+
 static void tune_load_locked() {
     if (g_tune_loaded) return;
     g_tune_loaded = true;
@@ -2519,7 +2540,9 @@ static int choose_config(Ctx* ctx, const Reg* r, const std::vector<LGate>& prog,
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     YAO_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
     if (cs != cudaStreamCaptureStatusNone) return YAO_OK;  // no synchronising while a graph is captured
-    const std::string key = tune_key(ctx->device, r->nbits, r->precision, mode, kreq, "prog");
+    char what[32];
+    snprintf(what, sizeof(what), "prog-%016llx", (unsigned long long)program_shape_hash(prog));
+    const std::string key = tune_key(ctx->device, r->nbits, r->precision, mode, kreq, what);
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
         tune_load_locked();
