@@ -483,8 +483,11 @@ def profile_case(args):
         Y.expect_grad_batch(tfim(Y, 16), c, sets, Y.ArrayReg.zero_state(16))
     elif args.profile_case == "pass1q":
         # one complex64 tile pass holding a single 1-qubit block (the bare
-        # load / store pipeline of a pass), run 4 times
-        os.environ.update(YAO_TILE_BITS="12", YAO_REG_BITS="3", YAO_AUTOTUNE="0")
+        # load / store pipeline of a pass), run 4 times; 2^12 tiles unless
+        # YAO_TILE_BITS / YAO_REG_BITS say otherwise
+        os.environ.setdefault("YAO_TILE_BITS", "12")
+        os.environ.setdefault("YAO_REG_BITS", "3")
+        os.environ["YAO_AUTOTUNE"] = "0"
         c = Y.Circuit.qubits(n, [Y.put([0], Y.Gate.Ry(0.3))])
         r = Y.ArrayReg.zero_state(n, Y.C64)
         for _ in range(4):
