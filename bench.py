@@ -981,7 +981,7 @@ def dm_extra(Y, A, torch, stream, dev, timed):
     # FUSED form: rho as a 28-qubit vector through the fused tile passes,
     # channels as superoperators
     f = Y.DensityMatrix.zero_state(n, device=dev)
-    f.apply(noisy_dm_circuit(Y, n, 1, seed=99), Y.MODE_FUSED)  # warm-up
+    f.apply(c, Y.MODE_FUSED)  # warm-up: the autotuner's choice is kept per circuit structure
     del f
     f = Y.DensityMatrix.zero_state(n, device=dev)
     A.profile(True, dev)
