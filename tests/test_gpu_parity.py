@@ -832,7 +832,7 @@ def test_fp64_tensor_core_blocks(monkeypatch, n, k, tbits, rb):
 
 SWEEP_FORMS = {"segments": {}, "one_op": {"YAO_ADJ_SEGMENTS": "0"}, "in_order": {"YAO_ADJ_REORDER": "0"},
                "in_order_one_op": {"YAO_ADJ_REORDER": "0", "YAO_ADJ_SEGMENTS": "0"},
-               "segments_per_lane_controls": {"YAO_ADJ_UPAIR": "0"}}
+               "segments_per_lane_controls": {"YAO_ADJ_UPAIR": "0"}, "segments_no_x_fold": {"YAO_ADJ_XFOLD": "0"}}
 
 
 @pytest.mark.parametrize("form", list(SWEEP_FORMS))
@@ -881,6 +881,49 @@ def test_expect_grad_tiled_sweep_matches_per_gate(monkeypatch, n, form):
     assert np.max(np.abs(np.array(g1) - np.array(g0))) < 1e-11
     assert np.max(np.abs(np.array(g1) - np.array(go))) < 1e-11
     assert maxdiff(r0.state_vec(), psi0) == 0.0
+
+
+def test_expect_grad_cnot_folds_into_segment_runs(monkeypatch):
+    """CNOTs between the two qubits of a register segment merge into the
+    folded Ry.Rz run on their target, before it (the CNOT follows the run in
+    the circuit) and after it (the CNOT precedes the run): the plan has fewer
+    ops and energy and gradient still match the per-gate sweep, the unmerged
+    sweep and the oracle to 1e-11."""
+    rng = np.random.default_rng(123)
+    n = 14
+    els = []
+    for layer in range(3):
+        for q in range(0, n - 1, 2):
+            els.append(Y.control([q + 1], [q], Gate.X))  # before the run on q
+        for q in range(n):
+            els.append(Y.put([q], Gate.Ry(float(rng.uniform(-3, 3)))))
+            els.append(Y.put([q], Gate.Rz(float(rng.uniform(-3, 3)))))
+        for q in range(layer % 2, n - 1, 2):
+            els.append(Y.control([q], [q + 1], Gate.X))  # after the run on q + 1
+    for layer in range(4):  # brickwork: rotations, then CNOTs on alternating pairs
+        for q in range(n):
+            els.append(Y.put([q], Gate.Ry(float(rng.uniform(-3, 3)))))
+            els.append(Y.put([q], Gate.Rz(float(rng.uniform(-3, 3)))))
+        for q in range(layer % 2, n - 1, 2):
+            els.append(Y.control([q], [q + 1], Gate.X))
+    c = Y.Circuit.qubits(n, els)
+    merged = Y.grad_plan_info(c)
+    monkeypatch.setenv("YAO_ADJ_XFOLD", "0")
+    plain = Y.grad_plan_info(c)
+    monkeypatch.delenv("YAO_ADJ_XFOLD")
+    assert merged["ops"] <= plain["ops"] - 5 and merged["dots"] == plain["dots"]
+    op = tfim(n, 0.9) + Y.OperatorPolynomial.single(3, Y.Op.Y, 0.25)
+    psi0 = random_state(rng, n)
+    r0 = Y.ArrayReg.from_vec(n, psi0)
+    v1, g1 = Y.expect_grad(op, c, r0)
+    monkeypatch.setenv("YAO_ADJ_XFOLD", "0")
+    v2, g2 = Y.expect_grad(op, c, r0)
+    monkeypatch.setenv("YAO_ADJ_TILES", "0")
+    v0, g0 = Y.expect_grad(op, c, r0)
+    vo, go = O.expect_grad(op, c, psi0)
+    for v, g in ((v1, g1), (v2, g2), (v0, g0)):
+        assert abs(v - vo) < 1e-12
+        assert np.max(np.abs(np.array(g) - np.array(go))) < 1e-11
 
 
 def test_expect_grad_wide_gate_takes_per_gate_sweep():

@@ -48,6 +48,16 @@ constexpr int kAdjMaxSlots = 48;    // generator dots per pass
 constexpr int32_t kAdjFused = 16;
 constexpr int kAdjFusedGens = 3;
 
+// A folded run (at most 2 dots) merged inside a register segment with an X
+// step whose only control is the segment's other bit (a CNOT between the
+// segment's two qubits): the X acts on one of the group's two pairs, so the
+// op carries one coefficient set per pair q (the value of the other bit):
+// m[8 q .. 8 q + 3] = A_q, m[8 q + 4 + 2 j] = (-Im G'_q,j[0][0],
+// -Im G'_q,j[1][1]), m[8 q + 5 + 2 j] = G'_q,j[0][1].  X before the run:
+// A_q = A X, G'_q = X G' X on the X's pair; X after it: A_q = X A.
+constexpr int32_t kAdjFusedPair = 17;
+constexpr int kAdjPairGens = 2;
+
 // The control fields of an op: 64 bytes, 16-byte aligned, so the register
 // segments copy them into registers with four 16-byte loads per op.
 struct __align__(16) AdjOpCtl {
@@ -372,6 +382,44 @@ __device__ __forceinline__ void seg_op(const AdjOpCtl& c, const AdjTileOp& op, d
                                        uint32_t gb, uint32_t m0, uint32_t m1, bool valid, double* __restrict__ acc,
                                        uint32_t nw) {
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (c.cls == kAdjFusedPair) {
+        const int ng = c.ngen;
+        double dot[kAdjPairGens] = {0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            int ia, ib;
+            seg_pair_idx<S>(q, ia, ib);
+            const double2* mq = op.m + 8 * q;
+            const double2 x0 = x[ia], x1 = x[ib], l0 = l[ia], l1 = l[ib];
+            if (valid && ng > 0) {
+                const double i00 = fma(l0.x, x0.y, -l0.y * x0.x);  // Im P00
+                const double i11 = fma(l1.x, x1.y, -l1.y * x1.x);  // Im P11
+                const double qx = fma(l0.x, x1.x, fma(l0.y, x1.y, fma(-l1.x, x0.x, -l1.y * x0.y)));
+                const double qy = fma(l0.x, x1.y, fma(-l0.y, x1.x, fma(-l1.y, x0.x, l1.x * x0.y)));
+#pragma unroll
+                for (int j = 0; j < kAdjPairGens; j++)
+                    if (j < ng) {
+                        const double2 gd = mq[4 + 2 * j], g01 = mq[5 + 2 * j];
+                        dot[j] += fma(gd.x, i00, fma(gd.y, i11, fma(g01.x, qx, -g01.y * qy)));
+                    }
+            }
+            const double2 a0 = mq[0], a1 = mq[1], a2 = mq[2], a3 = mq[3];
+            x[ia] = cfma2(cmul2(a0, x0), a1, x1);
+            x[ib] = cfma2(cmul2(a2, x0), a3, x1);
+            l[ia] = cfma2(cmul2(a0, l0), a1, l1);
+            l[ib] = cfma2(cmul2(a2, l0), a3, l1);
+        }
+        if (ng == 2) {
+            const double d = warp_part_pair(dot[0], dot[1]);
+            acc_part(acc, c.gslot[0], nw, d);
+            __syncwarp();  // (the two slots may coincide)
+            if ((lane & 16) && (lane & 15) < (uint32_t)kAdjSub)
+                acc[((uint32_t)c.gslot[1] * nw + warp) * kAdjSub + (lane & 15)] += d;
+        } else if (ng == 1) {
+            acc_part(acc, c.gslot[0], nw, warp_part(dot[0]));
+        }
+        return;
+    }
     if (c.cls == kAdjFused) {
         // G'_j = A^dagger G_j A is anti-Hermitian like the generators
         // (G = -i times a Hermitian matrix; the host folds only such runs):
@@ -824,9 +872,17 @@ static bool segments_on() {
     return !(e && e[0] == '0');
 }
 
+// YAO_ADJ_XFOLD=0: keep segment X steps as ops of their own
+static bool xfold_on() {
+    const char* e = getenv("YAO_ADJ_XFOLD");
+    return !(e && e[0] == '0');
+}
+
 // The steps of a pass re-sequenced for register segments: a scan in sweep
 // order emits every ready 1-qubit step whose target is one of the current
-// segment's two bits (or becomes its second); when a scan emits nothing the
+// segment's two bits (or becomes its second; a step with one control that
+// opens a segment brings its control as the second bit, when steps of the
+// pass act on that qubit); when a scan emits nothing the
 // segment closes and the next one starts at the first remaining step (a
 // 2-qubit step is emitted alone).  A step is ready when no earlier
 // remaining step of the pass shares a qubit with it, so the dependencies of
@@ -838,6 +894,10 @@ static std::vector<size_t> segment_order(const std::vector<HostOp>& hops, const 
     std::vector<char> done(take.size(), 0);
     size_t left = take.size();
     int sb[2] = {-1, -1}, nsb = 0;
+    // remaining 1-qubit steps per target qubit
+    std::vector<int> on_target(64, 0);
+    for (size_t i = 0; i < take.size(); i++)
+        if (hops[take[i]].op.k == 1) on_target[hops[take[i]].tb[0]]++;
     while (left) {
         bool emitted = false;
         uint64_t blocked = 0;
@@ -857,6 +917,11 @@ static std::vector<size_t> segment_order(const std::vector<HostOp>& hops, const 
                 } else if (nsb < 2) {
                     sb[nsb++] = t;
                     fit = true;
+                    // a step with one control (a CNOT) opens the segment: its
+                    // control becomes the second bit when steps of the pass act
+                    // on it, so the step can merge into a folded run
+                    if (nsb == 1 && xfold_on() && h.cb.size() == 1 && h.cb[0] != t && on_target[h.cb[0]] > 0)
+                        sb[nsb++] = h.cb[0];
                 }
             }
             if (!fit) {
@@ -864,6 +929,7 @@ static std::vector<size_t> segment_order(const std::vector<HostOp>& hops, const 
                 continue;
             }
             order.push_back(take[i]);
+            if (h.op.k == 1) on_target[h.tb[0]]--;
             done[i] = 1;
             left--;
             emitted = true;
@@ -894,6 +960,87 @@ static bool upair_on() {
     return !(e && e[0] == '0');
 }
 
+// One segment's ops [i, j) (seg[], upair set) with every X step that acts on
+// one pair of every group (upair, no out-of-tile controls) merged into an
+// adjacent folded run on its target (kAdjFusedPair); returns the new ops.
+static std::vector<AdjTileOp> fold_segment_x(const std::vector<AdjTileOp>& ops, size_t i, size_t j) {
+    struct Pair {
+        M2 a[2], g[2][kAdjPairGens];
+    };
+    std::vector<AdjTileOp> out;
+    std::vector<Pair> pp;        // per-pair coefficients of out[k] (when its cls is kAdjFusedPair)
+    auto foldable_x = [](const AdjTileOp& o) {
+        return o.cls == GC_X && !o.gen && o.k == 1 && o.upair && o.gcmask == 0;
+    };
+    auto to_pair = [&](size_t k) -> bool {  // out[k] becomes kAdjFusedPair when it can
+        AdjTileOp& f = out[k];
+        if (f.cls == kAdjFusedPair) return true;
+        if (f.cls != kAdjFused || f.ngen > kAdjPairGens) return false;
+        Pair p;
+        for (int q = 0; q < 2; q++) {
+            for (int e = 0; e < 4; e++) p.a[q].e[e] = f.m[e];
+            for (int g = 0; g < f.ngen; g++)
+                for (int e = 0; e < 4; e++) p.g[q][g].e[e] = f.m[4 + 4 * g + e];
+        }
+        pp[k] = p;
+        f.cls = kAdjFusedPair;
+        f.a_id = 0;
+        return true;
+    };
+    std::vector<bool> used(j, false);  // runs already moved back and merged
+    for (size_t q = i; q < j; q++) {
+        if (used[q]) continue;
+        const AdjTileOp& o = ops[q];
+        if (foldable_x(o)) {
+            const int cv = o.upair - 1;
+            // after the previous run on the same target: A_cv = X A
+            if (!out.empty() && out.back().tl[0] == o.tl[0] && to_pair(out.size() - 1)) {
+                M2& a = pp.back().a[cv];
+                a = M2{{a.e[2], a.e[3], a.e[0], a.e[1]}};
+                continue;
+            }
+            // before the next run on the same target, which moves back to the
+            // X past the steps in between (they neither act on nor are
+            // controlled by its bit, so they commute with it and their dots
+            // do not change): A_cv = A X, G'_cv = X G' X
+            const uint32_t tbit = 1u << o.tl[0];
+            size_t k = q + 1;
+            while (k < j && !used[k] && ops[k].tl[0] != o.tl[0] && !(ops[k].lcmask & tbit)) k++;
+            if (k < j && !used[k] && ops[k].tl[0] == o.tl[0] && ops[k].cls == kAdjFused &&
+                ops[k].ngen <= kAdjPairGens) {
+                out.push_back(ops[k]);
+                pp.emplace_back();
+                to_pair(out.size() - 1);
+                Pair& p = pp.back();
+                M2& a = p.a[cv];
+                a = M2{{a.e[1], a.e[0], a.e[3], a.e[2]}};
+                for (int g = 0; g < out.back().ngen; g++) {
+                    M2& m = p.g[cv][g];
+                    m = M2{{m.e[3], m.e[2], m.e[1], m.e[0]}};
+                }
+                used[k] = true;
+                continue;
+            }
+        }
+        out.push_back(o);
+        pp.emplace_back();
+    }
+    for (size_t k = 0; k < out.size(); k++) {
+        AdjTileOp& f = out[k];
+        if (f.cls != kAdjFusedPair) continue;
+        const Pair& p = pp[k];
+        for (int q = 0; q < 2; q++) {
+            for (int e = 0; e < 4; e++) f.m[8 * q + e] = p.a[q].e[e];
+            for (int g = 0; g < kAdjPairGens; g++) {
+                const M2& m = p.g[q][g];
+                f.m[8 * q + 4 + 2 * g] = g < f.ngen ? make_double2(-m.e[0].y, -m.e[3].y) : make_double2(0, 0);
+                f.m[8 * q + 5 + 2 * g] = g < f.ngen ? m.e[1] : make_double2(0, 0);
+            }
+        }
+    }
+    return out;
+}
+
 static void mark_barriers(std::vector<AdjTileOp>& ops, bool seg) {
     size_t i = 0;
     while (i < ops.size()) {
@@ -916,6 +1063,16 @@ static void mark_barriers(std::vector<AdjTileOp>& ops, bool seg) {
                 ops[q].upair = (int8_t)(upair_on() && ops[q].cls != kAdjFused && ops[q].lcmask == other
                                             ? 1 + (ops[q].lcval != 0)
                                             : 0);
+            }
+            if (xfold_on()) {
+                std::vector<AdjTileOp> f = fold_segment_x(ops, i, j);
+                if (f.size() < j - i) {
+                    for (AdjTileOp& o : f) o.sync = 0;
+                    f.back().sync = 1;
+                    ops.erase(ops.begin() + (std::ptrdiff_t)i, ops.begin() + (std::ptrdiff_t)j);
+                    ops.insert(ops.begin() + (std::ptrdiff_t)i, f.begin(), f.end());
+                    j = i + f.size();
+                }
             }
             i = j;
             continue;
