@@ -57,6 +57,10 @@ constexpr int kAdjFusedGens = 3;
 // A_q = A X, G'_q = X G' X on the X's pair; X after it: A_q = X A.
 constexpr int32_t kAdjFusedPair = 17;
 constexpr int kAdjPairGens = 2;
+// The same with an X step whose controls are in-tile bits outside the
+// segment (xmask, xval): the X acts on both pairs of a group or on neither,
+// so set 1 (m[8 ..]) serves the groups whose bits match and set 0 the others.
+constexpr int32_t kAdjFusedCtl = 18;
 
 // The control fields of an op: 64 bytes, 16-byte aligned, so the register
 // segments copy them into registers with four 16-byte loads per op.
@@ -80,6 +84,7 @@ static_assert(sizeof(AdjOpCtl) == 64, "the control fields are four 16-byte words
 
 struct AdjTileOp : AdjOpCtl {
     uint64_t active;         // DIAG: entries different from 1
+    uint32_t xmask, xval;    // kAdjFusedCtl: in-tile controls of the merged X step
     double2 m[16];           // dense 2^k x 2^k row-major, or the 2^k diagonal entries
 };
 static_assert(sizeof(AdjTileOp) % 16 == 0, "AdjTileOp is staged as 64-bit words, 16-byte aligned");
@@ -382,14 +387,17 @@ __device__ __forceinline__ void seg_op(const AdjOpCtl& c, const AdjTileOp& op, d
                                        uint32_t gb, uint32_t m0, uint32_t m1, bool valid, double* __restrict__ acc,
                                        uint32_t nw) {
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (c.cls == kAdjFusedPair) {
+    if (c.cls == kAdjFusedPair || c.cls == kAdjFusedCtl) {
         const int ng = c.ngen;
         double dot[kAdjPairGens] = {0.0, 0.0};
+        // coefficient set of each pair: by pair, or by the group's bits
+        const int sel = (gb & op.xmask) == op.xval ? 1 : 0;
+        const int s0 = c.cls == kAdjFusedPair ? 0 : sel, s1 = c.cls == kAdjFusedPair ? 1 : sel;
 #pragma unroll
         for (int q = 0; q < 2; q++) {
             int ia, ib;
             seg_pair_idx<S>(q, ia, ib);
-            const double2* mq = op.m + 8 * q;
+            const double2* mq = op.m + 8 * (q ? s1 : s0);
             const double2 x0 = x[ia], x1 = x[ib], l0 = l[ia], l1 = l[ib];
             if (valid && ng > 0) {
                 const double i00 = fma(l0.x, x0.y, -l0.y * x0.x);  // Im P00
@@ -969,12 +977,20 @@ static std::vector<AdjTileOp> fold_segment_x(const std::vector<AdjTileOp>& ops, 
     };
     std::vector<AdjTileOp> out;
     std::vector<Pair> pp;        // per-pair coefficients of out[k] (when its cls is kAdjFusedPair)
-    auto foldable_x = [](const AdjTileOp& o) {
-        return o.cls == GC_X && !o.gen && o.k == 1 && o.upair && o.gcmask == 0;
+    const uint32_t segbits = (1u << ops[i].seg[0]) | (1u << ops[i].seg[1]);
+    // the merged kind of an X step: per pair (its only control is the other
+    // segment bit), per group (in-tile controls off the segment), or none
+    auto x_kind = [&](const AdjTileOp& o) -> int32_t {
+        if (o.cls != GC_X || o.gen || o.k != 1 || o.gcmask != 0) return 0;
+        if (o.upair) return kAdjFusedPair;
+        if (o.lcmask && !(o.lcmask & segbits)) return kAdjFusedCtl;
+        return 0;
     };
-    auto to_pair = [&](size_t k) -> bool {  // out[k] becomes kAdjFusedPair when it can
+    // out[k] becomes a merged run of `kind` (with the X's controls) when it can
+    auto to_pair = [&](size_t k, int32_t kind, const AdjTileOp& x) -> bool {
         AdjTileOp& f = out[k];
-        if (f.cls == kAdjFusedPair) return true;
+        if (f.cls == kind)
+            return kind == kAdjFusedPair || (f.xmask == x.lcmask && f.xval == x.lcval);
         if (f.cls != kAdjFused || f.ngen > kAdjPairGens) return false;
         Pair p;
         for (int q = 0; q < 2; q++) {
@@ -983,18 +999,24 @@ static std::vector<AdjTileOp> fold_segment_x(const std::vector<AdjTileOp>& ops, 
                 for (int e = 0; e < 4; e++) p.g[q][g].e[e] = f.m[4 + 4 * g + e];
         }
         pp[k] = p;
-        f.cls = kAdjFusedPair;
+        f.cls = kind;
         f.a_id = 0;
+        if (kind == kAdjFusedCtl) {
+            f.xmask = x.lcmask;
+            f.xval = x.lcval;
+        }
         return true;
     };
     std::vector<bool> used(j, false);  // runs already moved back and merged
     for (size_t q = i; q < j; q++) {
         if (used[q]) continue;
         const AdjTileOp& o = ops[q];
-        if (foldable_x(o)) {
-            const int cv = o.upair - 1;
+        const int32_t kind = x_kind(o);
+        if (kind) {
+            // coefficient set the X acts on: its pair, or set 1
+            const int cv = kind == kAdjFusedPair ? o.upair - 1 : 1;
             // after the previous run on the same target: A_cv = X A
-            if (!out.empty() && out.back().tl[0] == o.tl[0] && to_pair(out.size() - 1)) {
+            if (!out.empty() && out.back().tl[0] == o.tl[0] && to_pair(out.size() - 1, kind, o)) {
                 M2& a = pp.back().a[cv];
                 a = M2{{a.e[2], a.e[3], a.e[0], a.e[1]}};
                 continue;
@@ -1005,12 +1027,13 @@ static std::vector<AdjTileOp> fold_segment_x(const std::vector<AdjTileOp>& ops, 
             // do not change): A_cv = A X, G'_cv = X G' X
             const uint32_t tbit = 1u << o.tl[0];
             size_t k = q + 1;
-            while (k < j && !used[k] && ops[k].tl[0] != o.tl[0] && !(ops[k].lcmask & tbit)) k++;
+            // (runs already moved back sit before this X: passed over)
+            while (k < j && (used[k] || (ops[k].tl[0] != o.tl[0] && !(ops[k].lcmask & tbit)))) k++;
             if (k < j && !used[k] && ops[k].tl[0] == o.tl[0] && ops[k].cls == kAdjFused &&
                 ops[k].ngen <= kAdjPairGens) {
                 out.push_back(ops[k]);
                 pp.emplace_back();
-                to_pair(out.size() - 1);
+                to_pair(out.size() - 1, kind, o);
                 Pair& p = pp.back();
                 M2& a = p.a[cv];
                 a = M2{{a.e[1], a.e[0], a.e[3], a.e[2]}};
@@ -1027,7 +1050,7 @@ static std::vector<AdjTileOp> fold_segment_x(const std::vector<AdjTileOp>& ops, 
     }
     for (size_t k = 0; k < out.size(); k++) {
         AdjTileOp& f = out[k];
-        if (f.cls != kAdjFusedPair) continue;
+        if (f.cls != kAdjFusedPair && f.cls != kAdjFusedCtl) continue;
         const Pair& p = pp[k];
         for (int q = 0; q < 2; q++) {
             for (int e = 0; e < 4; e++) f.m[8 * q + e] = p.a[q].e[e];
