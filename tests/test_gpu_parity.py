@@ -887,8 +887,9 @@ def test_expect_grad_cnot_folds_into_segment_runs(monkeypatch):
     """CNOTs merge into the folded Ry.Rz run on their target inside a
     register segment, before it (the CNOT follows the run in the circuit) and
     after it (the CNOT precedes the run), controlled by the segment's other
-    qubit (one coefficient set per pair) or by another qubit of the tile (one
-    set per group): the plan has fewer ops and energy and gradient still
+    qubit (one coefficient set per pair) or by another qubit, in the tile or
+    out of it (one set per group): the plan has fewer ops and energy and
+    gradient still
     match the per-gate sweep, the unmerged sweep and the oracle to 1e-11."""
     rng = np.random.default_rng(123)
     n = 14

@@ -202,14 +202,14 @@ def test_grad_plan_reorders_commuting_steps(monkeypatch):
     scheduling over the steps' qubits lets a pass take steps on disjoint
     qubits out of sweep order, halving the passes of the in-order plan; every
     parameter keeps one generator dot, and every Ry.Rz pair folds into one
-    op next to its CNOT.  Within register segments, a CNOT whose control is
-    in the tile merges into the folded run on its target (169 of the 192
-    CNOTs in the list-scheduled plan, 7 in sweep order)."""
+    op next to its CNOT.  Within register segments, a CNOT merges into the
+    folded run on its target (191 of the 192 CNOTs in the list-scheduled
+    plan, 7 in sweep order)."""
     from helpers import vqe_ansatz
     rng = np.random.default_rng(2024)
     c = vqe_ansatz(24, 8, rng.uniform(-3, 3, size=2 * 24 * 8))
     got = Y.grad_plan_info(c)
-    assert got == {"passes": 23, "ops": 215, "dots": 384}
+    assert got == {"passes": 23, "ops": 193, "dots": 384}
     monkeypatch.setenv("YAO_ADJ_XFOLD", "0")
     assert Y.grad_plan_info(c) == {"passes": 23, "ops": 384, "dots": 384}
     monkeypatch.delenv("YAO_ADJ_XFOLD")

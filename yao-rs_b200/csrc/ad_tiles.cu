@@ -57,9 +57,10 @@ constexpr int kAdjFusedGens = 3;
 // A_q = A X, G'_q = X G' X on the X's pair; X after it: A_q = X A.
 constexpr int32_t kAdjFusedPair = 17;
 constexpr int kAdjPairGens = 2;
-// The same with an X step whose controls are in-tile bits outside the
-// segment (xmask, xval): the X acts on both pairs of a group or on neither,
-// so set 1 (m[8 ..]) serves the groups whose bits match and set 0 the others.
+// The same with an X step whose controls are off the segment (in-tile bits
+// xmask / xval, out-of-tile bits xgmask / xgval): the X acts on both pairs of
+// a group or on neither, so set 1 (m[8 ..]) serves the groups whose bits
+// match and set 0 the others.
 constexpr int32_t kAdjFusedCtl = 18;
 
 // The control fields of an op: 64 bytes, 16-byte aligned, so the register
@@ -85,6 +86,7 @@ static_assert(sizeof(AdjOpCtl) == 64, "the control fields are four 16-byte words
 struct AdjTileOp : AdjOpCtl {
     uint64_t active;         // DIAG: entries different from 1
     uint32_t xmask, xval;    // kAdjFusedCtl: in-tile controls of the merged X step
+    uint64_t xgmask, xgval;  // kAdjFusedCtl: its out-of-tile controls
     double2 m[16];           // dense 2^k x 2^k row-major, or the 2^k diagonal entries
 };
 static_assert(sizeof(AdjTileOp) % 16 == 0, "AdjTileOp is staged as 64-bit words, 16-byte aligned");
@@ -384,14 +386,14 @@ __device__ __forceinline__ void seg_pair(const AdjOpCtl& c, const AdjTileOp& op,
 // added to the warp's slot.
 template <int S>
 __device__ __forceinline__ void seg_op(const AdjOpCtl& c, const AdjTileOp& op, double2 (&x)[4], double2 (&l)[4],
-                                       uint32_t gb, uint32_t m0, uint32_t m1, bool valid, double* __restrict__ acc,
-                                       uint32_t nw) {
+                                       uint32_t gb, uint32_t m0, uint32_t m1, bool valid, uint64_t base,
+                                       double* __restrict__ acc, uint32_t nw) {
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (c.cls == kAdjFusedPair || c.cls == kAdjFusedCtl) {
         const int ng = c.ngen;
         double dot[kAdjPairGens] = {0.0, 0.0};
         // coefficient set of each pair: by pair, or by the group's bits
-        const int sel = (gb & op.xmask) == op.xval ? 1 : 0;
+        const int sel = (gb & op.xmask) == op.xval && (base & op.xgmask) == op.xgval ? 1 : 0;
         const int s0 = c.cls == kAdjFusedPair ? 0 : sel, s1 = c.cls == kAdjFusedPair ? 1 : sel;
 #pragma unroll
         for (int q = 0; q < 2; q++) {
@@ -516,9 +518,9 @@ __device__ __forceinline__ void adj_seg(const AdjTileOp* __restrict__ sops, int 
         const AdjOpCtl c = static_cast<const AdjOpCtl&>(op);  // four 16-byte loads
         if ((base & c.gcmask) != c.gcval) continue;  // uniform over the tile
         if (c.tl[0] == p0)
-            seg_op<0>(c, op, x, l, gb, m0, m1, valid, acc, nw);
+            seg_op<0>(c, op, x, l, gb, m0, m1, valid, base, acc, nw);
         else
-            seg_op<1>(c, op, x, l, gb, m0, m1, valid, acc, nw);
+            seg_op<1>(c, op, x, l, gb, m0, m1, valid, base, acc, nw);
     }
     if (valid)
 #pragma unroll
@@ -981,16 +983,17 @@ static std::vector<AdjTileOp> fold_segment_x(const std::vector<AdjTileOp>& ops, 
     // the merged kind of an X step: per pair (its only control is the other
     // segment bit), per group (in-tile controls off the segment), or none
     auto x_kind = [&](const AdjTileOp& o) -> int32_t {
-        if (o.cls != GC_X || o.gen || o.k != 1 || o.gcmask != 0) return 0;
-        if (o.upair) return kAdjFusedPair;
-        if (o.lcmask && !(o.lcmask & segbits)) return kAdjFusedCtl;
+        if (o.cls != GC_X || o.gen || o.k != 1) return 0;
+        if (o.upair && o.gcmask == 0) return kAdjFusedPair;
+        if ((o.lcmask || o.gcmask) && !(o.lcmask & segbits)) return kAdjFusedCtl;
         return 0;
     };
     // out[k] becomes a merged run of `kind` (with the X's controls) when it can
     auto to_pair = [&](size_t k, int32_t kind, const AdjTileOp& x) -> bool {
         AdjTileOp& f = out[k];
         if (f.cls == kind)
-            return kind == kAdjFusedPair || (f.xmask == x.lcmask && f.xval == x.lcval);
+            return kind == kAdjFusedPair || (f.xmask == x.lcmask && f.xval == x.lcval && f.xgmask == x.gcmask &&
+                                             f.xgval == x.gcval);
         if (f.cls != kAdjFused || f.ngen > kAdjPairGens) return false;
         Pair p;
         for (int q = 0; q < 2; q++) {
@@ -1004,6 +1007,8 @@ static std::vector<AdjTileOp> fold_segment_x(const std::vector<AdjTileOp>& ops, 
         if (kind == kAdjFusedCtl) {
             f.xmask = x.lcmask;
             f.xval = x.lcval;
+            f.xgmask = x.gcmask;
+            f.xgval = x.gcval;
         }
         return true;
     };
