@@ -16,6 +16,7 @@
 #include <map>
 #include <memory>
 #include <set>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -504,24 +505,32 @@ std::map<int64_t, int64_t> strides_of(const std::vector<int64_t>& legs, const st
 
 // Offset table of a label group: entry v (row-major over `grp`) holds, per
 // tensor in `who`, sum_i digit_i * stride_i (0 where the tensor lacks it).
+// Built as an odometer: each step adds the strides of the digits it moves.
 std::vector<int64_t> group_table(const std::vector<int64_t>& grp, const std::map<int64_t, uint32_t>& size,
                                  const std::vector<const std::map<int64_t, int64_t>*>& who) {
+    const size_t ng = grp.size(), w = who.size();
     size_t cnt = 1;
-    for (int64_t l : grp) cnt *= size.at(l);
-    const size_t w = who.size();
-    std::vector<int64_t> t(cnt * w, 0);
-    std::vector<uint32_t> dig(grp.size(), 0);
-    for (size_t v = 0; v < cnt; v++) {
+    std::vector<uint32_t> dim(ng);
+    std::vector<int64_t> st(ng * w, 0);  // stride of leg i in tensor j
+    for (size_t i = 0; i < ng; i++) {
+        dim[i] = size.at(grp[i]);
+        cnt *= dim[i];
         for (size_t j = 0; j < w; j++) {
-            int64_t o = 0;
-            for (size_t i = 0; i < grp.size(); i++) {
-                auto it = who[j]->find(grp[i]);
-                if (it != who[j]->end()) o += (int64_t)dig[i] * it->second;
-            }
-            t[v * w + j] = o;
+            auto it = who[j]->find(grp[i]);
+            if (it != who[j]->end()) st[i * w + j] = it->second;
         }
-        for (size_t i = grp.size(); i-- > 0;) {  // row-major increment
-            if (++dig[i] < size.at(grp[i])) break;
+    }
+    std::vector<int64_t> t(cnt * w, 0);
+    std::vector<uint32_t> dig(ng, 0);
+    std::vector<int64_t> cur(w, 0);
+    for (size_t v = 0; v < cnt; v++) {
+        for (size_t j = 0; j < w; j++) t[v * w + j] = cur[j];
+        for (size_t i = ng; i-- > 0;) {  // row-major increment
+            if (++dig[i] < dim[i]) {
+                for (size_t j = 0; j < w; j++) cur[j] += st[i * w + j];
+                break;
+            }
+            for (size_t j = 0; j < w; j++) cur[j] -= (int64_t)(dim[i] - 1) * st[i * w + j];
             dig[i] = 0;
         }
     }
@@ -663,34 +672,52 @@ int tn_contract(Ctx* ctx, const TNet& tn, double* out) {
         out[1] = 0.0;
         return YAO_OK;
     }
-    while (nlive > 1) {
-        double best = 0.0;
-        size_t ba = 0, bb = 0;
-        bool have = false;
-        std::set<std::pair<size_t, size_t>> tried;
-        for (const auto& kv : holders) {
-            const std::set<size_t>& hs = kv.second;
-            for (auto i = hs.begin(); i != hs.end(); ++i)
-                for (auto j = std::next(i); j != hs.end(); ++j) {
-                    if (!tried.insert({*i, *j}).second) continue;
-                    const std::set<int64_t> keep = keep_for(*i, *j);
-                    std::vector<int64_t> res(keep.begin(), keep.end());
-                    std::vector<int64_t> ra;
-                    for (int64_t l : res)
-                        if (std::find(live[*i].legs.begin(), live[*i].legs.end(), l) != live[*i].legs.end() ||
-                            std::find(live[*j].legs.begin(), live[*j].legs.end(), l) != live[*j].legs.end())
-                            ra.push_back(l);
-                    const double c = std::exp2(log2_size(ra, size)) - std::exp2(log2_size(live[*i].legs, size)) -
-                                     std::exp2(log2_size(live[*j].legs, size));
-                    if (!have || c < best || (c == best && std::make_pair(*i, *j) < std::make_pair(ba, bb))) {
-                        best = c;
-                        ba = *i;
-                        bb = *j;
-                        have = true;
-                    }
-                }
+    // Candidate pairs (tensors sharing a label) ordered by (growth, a, b):
+    // the first is the pair the rule picks.  A pair's growth depends only on
+    // which tensors hold its labels, and contracting a and b into c keeps
+    // every label another tensor holds (now held by c), so after a step only
+    // the pairs with c are new; those with a or b are dropped.
+    auto growth = [&](size_t i, size_t j) {
+        const std::set<int64_t> keep = keep_for(i, j);
+        std::vector<int64_t> ra;
+        for (int64_t l : keep)
+            if (std::find(live[i].legs.begin(), live[i].legs.end(), l) != live[i].legs.end() ||
+                std::find(live[j].legs.begin(), live[j].legs.end(), l) != live[j].legs.end())
+                ra.push_back(l);
+        return std::exp2(log2_size(ra, size)) - std::exp2(log2_size(live[i].legs, size)) -
+               std::exp2(log2_size(live[j].legs, size));
+    };
+    std::set<std::tuple<double, size_t, size_t>> cand;
+    std::map<size_t, std::map<size_t, double>> partner;  // t -> (other, growth of the pair)
+    auto add_pairs_of = [&](size_t t) {
+        std::set<size_t> nb;
+        for (int64_t l : live[t].legs)
+            for (size_t h : holders[l])
+                if (h != t) nb.insert(h);
+        for (size_t h : nb) {
+            const size_t i = std::min(t, h), j = std::max(t, h);
+            if (partner[i].count(j)) continue;
+            const double c = growth(i, j);
+            partner[i][j] = c;
+            partner[j][i] = c;
+            cand.insert(std::make_tuple(c, i, j));
         }
-        if (!have) {  // no shared label: the two smallest (an outer product)
+    };
+    auto drop_pairs_of = [&](size_t t) {
+        for (const auto& kv : partner[t]) {
+            const size_t i = std::min(t, kv.first), j = std::max(t, kv.first);
+            cand.erase(std::make_tuple(kv.second, i, j));
+            partner[kv.first].erase(t);
+        }
+        partner.erase(t);
+    };
+    for (size_t t = 0; t < live.size(); t++) add_pairs_of(t);
+    while (nlive > 1) {
+        size_t ba = 0, bb = 0;
+        if (!cand.empty()) {
+            ba = std::get<1>(*cand.begin());
+            bb = std::get<2>(*cand.begin());
+        } else {  // no shared label: the two smallest (an outer product)
             std::vector<std::pair<double, size_t>> bysize;
             for (size_t t = 0; t < live.size(); t++)
                 if (alive[t]) bysize.push_back({log2_size(live[t].legs, size), t});
@@ -705,6 +732,7 @@ int tn_contract(Ctx* ctx, const TNet& tn, double* out) {
             return s;
         }
         for (size_t x : {ba, bb}) {
+            drop_pairs_of(x);
             for (int64_t l : live[x].legs) {
                 holders[l].erase(x);
                 if (holders[l].empty()) holders.erase(l);
@@ -716,6 +744,7 @@ int tn_contract(Ctx* ctx, const TNet& tn, double* out) {
         live.push_back(c);
         alive.push_back(true);
         for (int64_t l : c.legs) holders[l].insert(live.size() - 1);
+        add_pairs_of(live.size() - 1);
         nlive--;
     }
     size_t last = 0;
