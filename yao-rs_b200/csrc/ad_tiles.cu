@@ -14,12 +14,15 @@
 // on disjoint qubits commute, and a generator dot does not change under
 // steps on other qubits), and within the pass consecutive 1-qubit steps on
 // at most two target bits form a register segment: each thread keeps its
-// 4-amplitude group of both tiles in registers across the segment.  Dots are
+// 4-amplitude group of both tiles in registers across the segment.  On the
+// host, runs of uncontrolled 1-qubit steps on one target fold into one op,
+// and an X step (a CNOT) in a segment merges into the run on its target,
+// which then carries a coefficient set per pair or per group.  Dots are
 // reduced over the warp down to four partial sums, added per warp in shared
 // memory (tiles of a CTA in a fixed order), summed over warps per CTA and
-// over CTAs in block order: deterministic for a given launch shape.  Arithmetic is FP64 with FMA; the
-// result is the reverse sweep of the per-gate form up to rounding (~1e-15
-// relative).
+// over CTAs in block order: deterministic for a given launch shape.
+// Arithmetic is FP64 with FMA; the result is the reverse sweep of the
+// per-gate form up to rounding (~1e-15 relative).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
