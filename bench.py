@@ -243,6 +243,16 @@ def sig(x, d=4):
     return x
 
 
+def bench_config(n, world):
+    """The workload both arms measure: per-gate algorithmic GB/s of the PLAIN
+    FP64 path on the layered circuit (one layer a step on the GPU; the CPU arm
+    samples it one gate a step)."""
+    return {"workload": f"layered random circuit n={n}, 40 layers (Rx,Ry,Rz + CNOT brickwork), PLAIN FP64 "
+                        "gate by gate",
+            "qubits": n, "state_bytes": 16 * (1 << n), "l2": "state larger than L2, no flush",
+            "parallelism": f"replicas x{world}"}
+
+
 # -------------------------------------------------------------- reference
 def run_reference(args, rank, world):
     """yao-rs cannot run here (Rust; no toolchain): its CPU path is timed
@@ -281,11 +291,11 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * T / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": f"layered random circuit n={n}, one gate per step (layer order)", "qubits": n,
-                   "l2": "state larger than L2"},
+        "config": bench_config(n, world),
         "cpu_baseline": {"value": v, "unit": "GB/s", "cores": 1, "kind": "port",
-                         "sample": f"{args.steps} gates of the layered circuit at n={n}, oracle (C restatement of "
-                                   "yao-rs instruct loops, -O3, 1 thread: yao-rs is single-threaded)"},
+                         "sample": f"one gate of the layered circuit per step (layer order), {args.steps} gates at "
+                                   f"n={n}, oracle (C restatement of yao-rs instruct loops, -O3, 1 thread: yao-rs "
+                                   "is single-threaded)"},
         "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -429,10 +439,7 @@ def main():
             "metric": METRIC, "value": sig(value, 6), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sig(ms / args.steps, 6), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": f"layered random circuit n={n}, 40 layers (Rx,Ry,Rz + CNOT brickwork), "
-                                   "one layer per step, PLAIN FP64",
-                       "qubits": n, "state_bytes": state_bytes, "l2": "state (16 GiB) larger than L2, no flush",
-                       "parallelism": f"replicas x{world}"},
+            "config": bench_config(n, world),
             "roofline": sig(roofline), "e2e": sig(e2e), "gpu_launches": int(launches), "clocks": clk,
             "cpu_baseline": sig(cpu),
         }
