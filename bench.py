@@ -752,7 +752,7 @@ def summary(x, plain_s, first_gates):
     # [s/circuit, 1 - F (normalised), |norm^2 - 1|]
     L["fused"] = {k.replace("fused_", ""): [sig(v["s_per_circuit"], 3), sig(v["one_minus_fidelity_normalised"], 2),
                                             sig(abs(v["norm2_minus_1"]), 2)]
-                  for k, v in x["fused"].items()}
+                  for k, v in x["fused"].items() if k not in ("fused_c64_k3", "fused_c64_k4")}
     # the tuned choices of the auto forms (and of c64 k = 5): [k, tile bits,
     # register bits(, tensor cores for complex64)]
     L["autotuned"] = {k.replace("fused_", ""): [c["k"], c["tile_bits"], c["reg_bits"]] +
@@ -777,7 +777,7 @@ def summary(x, plain_s, first_gates):
     c = x["batched_circuits"]
     s["batch2048"] = {"plain_s": c["s_plain"],
                       "forms": {k: [f["s"], f["speedup_vs_plain"], f["max_one_minus_fidelity"]]
-                                for k, f in c["forms"].items()}}
+                                for k, f in c["forms"].items() if k != "fused_c64_k2"}}
     d = x["noisy_dm14"]
     kern = {k["kernel"]: k["GBps"] for k in d["kernels"]}
     s["dm14"] = {"plain_s": d["s_per_circuit"], "fused_s": d["fused_superop"]["s_per_circuit"],
