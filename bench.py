@@ -519,6 +519,14 @@ def profile_case(args):
         # 2-qubit depolarizing channels through the register kernel
         d = Y.DensityMatrix.zero_state(12)
         d.apply(noisy_dm_circuit(Y, 12, 1))
+    elif args.profile_case == "dm_fused":
+        # three noisy layers of the benchmark's density-matrix circuit at
+        # --qubits (12: a 24-bit vector of 268 MB, larger than L2) in the FUSED
+        # superoperator form, with the shape the autotuner picks at n = 14
+        # (k = 4 blocks on 2^11 tiles)
+        os.environ.update(YAO_TILE_BITS="11", YAO_REG_BITS="3", YAO_AUTOTUNE="0")
+        d = Y.DensityMatrix.zero_state(n)
+        d.apply(noisy_dm_circuit(Y, n, 3), Y.MODE_FUSED)
     elif args.profile_case == "dm":
         nd = 12
         els = []
