@@ -313,7 +313,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--profile-case", default=None,
                     choices=["plain", "tiled", "fused64", "fused32", "fused32_tc", "pass1q", "fused64_dmma",
-                             "fused64_cuda", "vqe", "grad24", "dm", "dm_channel", "batch", "vqe_batch", "tc_drift"],
+                             "fused64_cuda", "vqe", "grad24", "dm", "dm_fused", "dm_channel", "batch", "vqe_batch",
+                             "tc_drift"],
                     help="run one small case of a kernel family (for ncu captures) and exit")
     args = ap.parse_args()
     if args.profile_case:
