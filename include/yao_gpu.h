@@ -367,6 +367,15 @@ int yao_tn_output_len(const yao_tn* tn, size_t* out);
  * order, complex128; `out` receives the result, legs in the order of the
  * output labels, row-major (2 * out_len doubles). */
 int yao_tn_contract(yao_ctx* ctx, const yao_tn* tn, double* out, size_t out_len);
+/* The same in a given order (src/contractor.rs:20-32 contract_with_tree and
+ * contract_dm_with_tree: the contraction tree as its post-order list of
+ * pairs).  A network of T tensors takes exactly T - 1 pairs; pair s
+ * contracts path[2s] and path[2s + 1], where 0..T-1 are the network's
+ * tensors and T + r is the result of pair r < s; every tensor is used once.
+ * Paths that break these rules fail with YAO_ERR_INVALID_ARGUMENT before
+ * anything reaches the GPU. */
+int yao_tn_contract_path(yao_ctx* ctx, const yao_tn* tn, const uint32_t* path, size_t npairs, double* out,
+                         size_t out_len);
 
 #ifdef __cplusplus
 }

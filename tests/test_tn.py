@@ -216,3 +216,123 @@ def test_contract_edge_cases():
     t = rng.normal(size=(2, 3, 4)) + 0j
     out = Y.einsum.contract(Y.TensorNetwork([[7, 8, 9]], [9, 7, 8], [t], {7: 2, 8: 3, 9: 4}))
     assert np.array_equal(out, np.transpose(t, (2, 0, 1)))
+
+
+# ------------------------------------------ explicit contraction order
+def test_tree_to_path_post_order_pairs():
+    from yao_rs.einsum import tree_to_path
+    assert tree_to_path(((0, 1), (2, 3)), 4) == [(0, 1), (2, 3), (4, 5)]
+    # a node of more than two subtrees contracts left to right
+    assert tree_to_path([0, 1, 2, 3], 4) == [(0, 1), (4, 2), (5, 3)]
+    assert tree_to_path([[3, 1], 0, 2], 4) == [(3, 1), (4, 0), (5, 2)]
+    assert tree_to_path(0, 1) == [] and tree_to_path((), 0) == []
+    for bad, t in (([0, 0], 2), ([0, 1], 3), ([0, [1]], 2), ((0, 5), 3), ([0, True], 2)):
+        with pytest.raises(ValueError):
+            tree_to_path(bad, t)
+
+
+def _range_tree(rng, lo, hi):
+    """A binary tree over tensors lo..hi-1 whose every subtree is a contiguous
+    range, split at a random point (rng) or in the middle (rng None).  Over a
+    circuit's network in gate order such a subtree is an operator on at most
+    every wire, so its result keeps few legs."""
+    if hi - lo == 1:
+        return lo
+    m = (lo + hi) // 2 if rng is None else int(rng.integers(lo + 1, hi))
+    return (_range_tree(rng, lo, m), _range_tree(rng, m, hi))
+
+
+def _largest_intermediate(net, tree):
+    """Elements of the largest tensor a contraction in the order of `tree`
+    makes: a label stays while the output or another remaining tensor has it."""
+    from yao_rs.einsum import tree_to_path
+    legs = [set(x) for x in net.ixs]
+    alive = set(range(len(legs)))
+    big = 1
+    for a, b in tree_to_path(tree, len(legs)):
+        alive -= {a, b}
+        rest = set(net.iy).union(*(legs[t] for t in alive)) if alive else set(net.iy)
+        legs.append((legs[a] | legs[b]) & rest)
+        alive.add(len(legs) - 1)
+        big = max(big, math.prod(net.size_dict[l] for l in legs[-1]))
+    return big
+
+
+def _trees(rng, net):
+    T = len(net.tensors)
+    out = [list(range(T)), list(range(T))[::-1], _range_tree(None, 0, T), _range_tree(rng, 0, T)]
+    for t in out:
+        assert _largest_intermediate(net, t) <= 1 << 20
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [2, 5, 8])
+def test_contract_with_tree_matches_greedy_oracle_and_state_vector(n):
+    rng = np.random.default_rng(90 + n)
+    c = random_circuit(rng, n, 30, max_ctrl=min(2, n - 1))
+    net = Y.circuit_to_einsum_with_boundary(c)
+    z = np.zeros(1 << n, complex)
+    z[0] = 1
+    psi = O.apply_circuit(as_tensor_export_reads(c), z)
+    greedy = Y.contract_tn(net).reshape(-1)
+    # in gate order (one growing state), backwards (one growing operator),
+    # balanced and random trees of contiguous ranges
+    for tree in _trees(rng, net):
+        out = Y.contract_with_tree(net, tree).reshape(-1)
+        assert np.max(np.abs(out - psi)) < 1e-12
+        assert np.max(np.abs(out - greedy)) < 1e-12
+    op = one_term(rng, n)
+    enet = Y.circuit_to_expectation(c, op)
+    want = OT.contract(OT.circuit_to_expectation(c, op))
+    for tree in _trees(rng, enet):
+        e = Y.contract_with_tree(enet, tree)
+        assert e.shape == () and abs(e - want) < 1e-12
+
+
+@pytest.mark.gpu
+def test_contract_dm_with_tree_matches_the_density_matrix():
+    rng = np.random.default_rng(95)
+    n = 3
+    c = noisy_circuit(rng, n, 15)
+    net = Y.circuit_to_einsum_dm(c)
+    z = np.zeros(1 << n, complex)
+    z[0] = 1
+    ref = O.dm_apply_circuit(as_tensor_export_reads(c), O.dm_from_reg(z, n)).reshape(1 << n, 1 << n)
+    for tree in _trees(rng, net):
+        rho = Y.contract_dm_with_tree(net, tree).reshape(1 << n, 1 << n)
+        assert np.max(np.abs(rho - ref)) < 1e-12
+    assert np.max(np.abs(rho - Y.contract_dm(net).reshape(1 << n, 1 << n))) < 1e-12
+
+
+@pytest.mark.gpu
+def test_contract_path_outer_products_and_rejected_paths():
+    rng = np.random.default_rng(6)
+    a, b, d = rng.normal(size=(2, 3)) + 1j, rng.normal(size=(3,)) + 0j, rng.normal(size=(3, 2)) - 1j
+    e, f = rng.normal(size=(4,)) + 2j, rng.normal(size=(2, 5)) + 0j
+    net = Y.TensorNetwork([[0, 1], [1], [1, 2], [3], [4, 5]], [0, 2, 3],
+                          [a, b, d, e, f], {0: 2, 1: 3, 2: 2, 3: 4, 4: 2, 5: 5})
+    want = np.einsum("ij,j,jk,l,mn->ikl", a, b, d, e, f)
+    # pairs without a shared label first (outer products), then the rest
+    for tree in (((3, 4), ((0, 1), 2)), ((0, 3), (4, (2, 1))), [4, 3, 2, 1, 0]):
+        assert np.max(np.abs(Y.contract_with_tree(net, tree) - want)) < 1e-12
+    # paths that break the rules fail before reaching the GPU, with a message
+    h = net._handle()
+    try:
+        n = C.c_size_t()
+        A = Y._abi
+        A.check(A.lib().yao_tn_output_len(h, C.byref(n)))
+        out = np.zeros(2 * n.value)
+        for path, msg in (([0, 1, 5, 2, 6, 3], "T - 1 pairs"),
+                          ([0, 1, 5, 2, 6, 3, 7, 7], "distinct"),
+                          ([0, 1, 5, 2, 6, 3, 7, 9], "distinct earlier"),
+                          ([0, 1, 1, 2, 6, 3, 7, 4], "already contracted")):
+            p = np.asarray(path, dtype=np.uint32)
+            st = A.lib().yao_tn_contract_path(A.context(None), h, p.ctypes.data_as(A.u32p), len(path) // 2,
+                                              out.ctypes.data_as(A.dptr), n.value)
+            assert st == A.YAO_ERR_INVALID_ARGUMENT, path
+            assert msg in A.lib().yao_last_error().decode(), (path, A.lib().yao_last_error())
+    finally:
+        Y._abi.lib().yao_tn_free(h)
+    # the library still contracts after the refusals
+    assert np.max(np.abs(Y.contract_with_tree(net, [0, 1, 2, 3, 4]) - want)) < 1e-12

@@ -616,15 +616,43 @@ static int contract_pair(Ctx* ctx, const DevTensor& A, const DevTensor& B, const
     return YAO_OK;
 }
 
+// Checks an explicit contraction order over T tensors: T - 1 pairs (none
+// for T <= 1), pair s naming two distinct tensors among the network's
+// 0..T-1 and the results T..T+s-1 of the pairs before it, each used once.
+static int path_validate(size_t T, const uint32_t* path, size_t npairs) {
+    if (npairs != (T > 0 ? T - 1 : 0))
+        return fail(YAO_ERR_INVALID_ARGUMENT, "contraction path: a network of T tensors takes exactly T - 1 pairs");
+    if (npairs && !path) return fail(YAO_ERR_INVALID_ARGUMENT, "contraction path: null pair list");
+    std::vector<bool> used(T + npairs, false);
+    for (size_t p = 0; p < npairs; p++) {
+        const uint32_t a = path[2 * p], b = path[2 * p + 1];
+        if (a == b || a >= T + p || b >= T + p)
+            return fail(YAO_ERR_INVALID_ARGUMENT,
+                        "contraction path: pair " + std::to_string(p) + " must name two distinct earlier tensors");
+        if (used[a] || used[b])
+            return fail(YAO_ERR_INVALID_ARGUMENT,
+                        "contraction path: pair " + std::to_string(p) + " names a tensor already contracted");
+        used[a] = used[b] = true;
+    }
+    return YAO_OK;
+}
+
 // Contracts the whole network on the device and copies the result (legs in
 // the order of tn.iy, row-major) to `out` (2 * prod(sizes of iy) doubles).
-// Order: repeatedly the pair of tensors that share a label (or, when none
-// do, the two smallest) whose result minus its inputs is smallest (sizes
-// as log2 to avoid overflow), ties to the lowest indices.  A label is kept
-// in a result while the output or another remaining tensor has it.
-int tn_contract(Ctx* ctx, const TNet& tn, double* out) {
+// Order: `path` when given (pair s contracts path[2s] and path[2s+1], the
+// indices counting the network's tensors and then each pair's result, as
+// checked by path_validate); otherwise repeatedly the pair of tensors that
+// share a label (or, when none do, the two smallest) whose result minus its
+// inputs is smallest (sizes as log2 to avoid overflow), ties to the lowest
+// indices.  A label is kept in a result while the output or another
+// remaining tensor has it.
+int tn_contract(Ctx* ctx, const TNet& tn, double* out, const uint32_t* path, size_t npairs, bool by_path) {
     int s = tn_validate(tn);
     if (s) return s;
+    if (by_path) {
+        s = path_validate(tn.tensors.size(), path, npairs);
+        if (s) return s;
+    }
     const std::map<int64_t, uint32_t>& size = tn.size;
     std::vector<DevTensor> live;
     std::vector<bool> alive;
@@ -711,10 +739,14 @@ int tn_contract(Ctx* ctx, const TNet& tn, double* out) {
         }
         partner.erase(t);
     };
-    for (size_t t = 0; t < live.size(); t++) add_pairs_of(t);
-    while (nlive > 1) {
+    if (!by_path)
+        for (size_t t = 0; t < live.size(); t++) add_pairs_of(t);
+    for (size_t step = 0; nlive > 1; step++) {
         size_t ba = 0, bb = 0;
-        if (!cand.empty()) {
+        if (by_path) {
+            ba = path[2 * step];
+            bb = path[2 * step + 1];
+        } else if (!cand.empty()) {
             ba = std::get<1>(*cand.begin());
             bb = std::get<2>(*cand.begin());
         } else {  // no shared label: the two smallest (an outer product)
@@ -744,7 +776,7 @@ int tn_contract(Ctx* ctx, const TNet& tn, double* out) {
         live.push_back(c);
         alive.push_back(true);
         for (int64_t l : c.legs) holders[l].insert(live.size() - 1);
-        add_pairs_of(live.size() - 1);
+        if (!by_path) add_pairs_of(live.size() - 1);
         nlive--;
     }
     size_t last = 0;
@@ -901,7 +933,21 @@ int yao_tn_contract(yao_ctx* ctx, const yao_tn* tn, double* out, size_t out_len)
     if (s) return s;
     if (out_len < need) return fail(YAO_ERR_INVALID_ARGUMENT, "output buffer too small for the contraction result");
     YAO_CUDA(cudaSetDevice(ctx->device));
-    return tn_contract(ctx, *tn, out);
+    return tn_contract(ctx, *tn, out, nullptr, 0, false);
+}
+
+int yao_tn_contract_path(yao_ctx* ctx, const yao_tn* tn, const uint32_t* path, size_t npairs, double* out,
+                         size_t out_len) {
+    if (!ctx || !tn || !out) return fail(YAO_ERR_INVALID_ARGUMENT, "null argument");
+    clear_error();
+    size_t need = 0;
+    int s = yao_tn_output_len(tn, &need);
+    if (s) return s;
+    if (out_len < need) return fail(YAO_ERR_INVALID_ARGUMENT, "output buffer too small for the contraction result");
+    s = path_validate(tn->tensors.size(), path, npairs);
+    if (s) return s;
+    YAO_CUDA(cudaSetDevice(ctx->device));
+    return tn_contract(ctx, *tn, out, path, npairs, true);
 }
 
 }  // extern "C"

@@ -16,7 +16,9 @@ from .operator import Op, OperatorPolynomial, OperatorString, op_matrix
 from .ops import (MeasureResult, PostProcess, apply, apply_inplace, autotune, batch_apply, expect_arrayreg, expect_dm, expect_grad_batch,
                   expect_grad, grad_plan_info, measure_with_postprocess, plan_info, probs)
 from .einsum import (TensorNetwork, circuit_to_einsum, circuit_to_einsum_dm, circuit_to_einsum_with_boundary,
-                     circuit_to_expectation, circuit_to_expectation_dm, circuit_to_overlap)
+                     circuit_to_expectation, circuit_to_expectation_dm, circuit_to_overlap, contract, contract_dm,
+                     contract_dm_with_tree, contract_with_tree)
+from .einsum import contract as contract_tn
 from .register import ArrayReg, DensityMatrix, Register, density_matrix_from_reg
 
 __all__ = [
@@ -27,5 +29,6 @@ __all__ = [
     "elements_array", "expect_arrayreg", "expect_dm", "expect_grad", "expect_grad_batch", "grad_plan_info", "label", "launch_count",
     "measure_with_postprocess", "op_matrix", "plan_info", "probs", "put", "TensorNetwork", "circuit_to_einsum",
     "circuit_to_einsum_dm", "circuit_to_einsum_with_boundary", "circuit_to_expectation", "circuit_to_expectation_dm",
-    "circuit_to_overlap", "einsum",
+    "circuit_to_overlap", "contract", "contract_dm", "contract_dm_with_tree", "contract_tn", "contract_with_tree",
+    "einsum",
 ]

@@ -160,6 +160,7 @@ SIGNATURES = {
                                 u32p]),
     "yao_tn_output_len": (C.c_int, [vp, C.POINTER(sz)]),
     "yao_tn_contract": (C.c_int, [vp, vp, dptr, sz]),
+    "yao_tn_contract_path": (C.c_int, [vp, vp, u32p, sz, dptr, sz]),
 }
 
 # enum yao_tn_kind

@@ -124,12 +124,65 @@ def circuit_to_expectation_dm(circuit, operator):
 def contract(tn: TensorNetwork, device: int | None = None) -> np.ndarray:
     """Contract the network on the GPU (pairwise, greedy order, complex128);
     the result has one axis per output label, in the order of tn.iy."""
+    return _contract(tn, device, None)
+
+
+def tree_to_path(tree, ntensors: int) -> list[tuple[int, int]]:
+    """The pair list of a contraction tree, in post order: a leaf is a tensor
+    index, a node a list or tuple of two or more subtrees (contracted left to
+    right, like a NestedEinsum node's args).  Pair s names two of the
+    network's tensors 0..ntensors-1 or the results ntensors + r of pairs
+    r < s.  Raises ValueError unless every tensor is a leaf exactly once."""
+    pairs: list[tuple[int, int]] = []
+    seen: set[int] = set()
+
+    def walk(t):
+        if isinstance(t, (int, np.integer)) and not isinstance(t, bool):
+            t = int(t)
+            if not 0 <= t < ntensors or t in seen:
+                raise ValueError(f"contraction tree: leaf {t} is not a tensor of the network or appears twice")
+            seen.add(t)
+            return t
+        if not isinstance(t, (list, tuple)) or len(t) < 2:
+            raise ValueError("contraction tree: a node has two or more subtrees")
+        acc = walk(t[0])
+        for sub in t[1:]:
+            pairs.append((acc, walk(sub)))
+            acc = ntensors + len(pairs) - 1
+        return acc
+
+    if ntensors == 0:
+        return []
+    walk(tree)
+    if len(seen) != ntensors:
+        raise ValueError(f"contraction tree covers {len(seen)} of the network's {ntensors} tensors")
+    return pairs
+
+
+def contract_with_tree(tn: TensorNetwork, tree, device: int | None = None) -> np.ndarray:
+    """contract_with_tree / contract_dm_with_tree (src/contractor.rs:20-32):
+    contract on the GPU in the order of `tree` (see tree_to_path), complex128;
+    the result as from contract()."""
+    return _contract(tn, device, tree_to_path(tree, len(tn.tensors)))
+
+
+# yao-rs's density-matrix forms take the same networks here
+contract_dm = contract
+contract_dm_with_tree = contract_with_tree
+
+
+def _contract(tn, device, path):
     h = tn._handle()
     try:
         n = C.c_size_t()
         A.check(A.lib().yao_tn_output_len(h, C.byref(n)))
         out = np.zeros(2 * max(1, n.value))
-        A.check(A.lib().yao_tn_contract(A.context(device), h, out.ctypes.data_as(A.dptr), n.value))
+        if path is None:
+            A.check(A.lib().yao_tn_contract(A.context(device), h, out.ctypes.data_as(A.dptr), n.value))
+        else:
+            flat = np.ascontiguousarray(np.asarray(path, dtype=np.uint32).reshape(-1))
+            A.check(A.lib().yao_tn_contract_path(A.context(device), h, flat.ctypes.data_as(A.u32p), len(path),
+                                                 out.ctypes.data_as(A.dptr), n.value))
     finally:
         A.lib().yao_tn_free(h)
     res = out[:2 * n.value].view(np.complex128)
