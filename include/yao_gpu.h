@@ -184,6 +184,12 @@ int yao_circuit_dagger(const yao_circuit* c, yao_circuit** out);
 /* Gate::matrix (src/gate.rs:63-68) for a named gate; out holds dim*dim
  * interleaved complex (dim <= 4). */
 int yao_gate_matrix(int32_t gate, const double* params, double* out, uint32_t* dim);
+/* Gate::generator_matrix (src/gate.rs:153-193): the constant generator
+ * G = (dU/dtheta_i) U^-1 of parameter i of a named parametric gate (Rx, Ry,
+ * Rz, Phase: i = 0; FSim: i = 0 theta, 1 phi); out holds dim*dim interleaved
+ * complex (dim <= 4).  i >= num_params (every non-parametric gate) is
+ * YAO_ERR_INVALID_ARGUMENT with yao-rs's panic message. */
+int yao_gate_generator_matrix(int32_t gate, uint32_t i, double* out, uint32_t* dim);
 /* NoiseChannel::kraus_operators / superop (src/noise.rs:183-379).
  * kraus_out holds up to max_kraus matrices of dim x dim. */
 int yao_noise_kraus(const yao_element* channel, double* kraus_out, uint32_t max_kraus,

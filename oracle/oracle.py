@@ -131,6 +131,16 @@ def gate_matrix(kind, params=()):
     return out[: d * d].reshape(d, d)
 
 
+def gate_generator(kind, i):
+    """gate.rs:153-193 (generator_matrix) through orc_gate_generator."""
+    out = np.zeros(16, np.complex128)
+    dim = C.c_uint32()
+    if lib().orc_gate_generator(kind, i, _p(out), C.byref(dim)) != 0:
+        raise ValueError("not a parametric gate")
+    d = dim.value
+    return out[: d * d].reshape(d, d)
+
+
 def noise_kraus(element):
     out = np.zeros(256 * 256, np.complex128)
     nk, dim = C.c_uint32(), C.c_uint32()

@@ -219,3 +219,27 @@ def test_grad_plan_reorders_commuting_steps(monkeypatch):
     wide = Y.Circuit.qubits(4, [Y.put([0, 1, 2], Gate.Custom(np.eye(8), False, "I3"))])
     with pytest.raises(Y.YaoError):
         Y.grad_plan_info(wide)
+
+
+def test_gate_generator_matrices():
+    """Gate::generator_matrix (src/gate.rs:153-193): the oracle's entries
+    bit for bit, the definition G = (dU/dtheta_i) U^-1 by central differences,
+    and the assert on i as an error with yao-rs's message."""
+    cases = [(Gate.Rx(0.7), 0), (Gate.Ry(-1.3), 0), (Gate.Rz(2.1), 0), (Gate.Phase(0.4), 0),
+             (Gate.FSim(0.3, 1.1), 0), (Gate.FSim(0.3, 1.1), 1)]
+    h = 1e-6
+    for g, i in cases:
+        G = g.generator_matrix(i)
+        assert np.array_equal(G, O.gate_generator(g.kind, i)), (g, i)
+        hi, lo = list(g.params), list(g.params)
+        hi[i] += h
+        lo[i] -= h
+        dU = (Gate(g.kind, hi).matrix() - Gate(g.kind, lo).matrix()) / (2 * h)
+        assert np.max(np.abs(dU @ np.linalg.inv(g.matrix()) - G)) < 1e-8, (g, i)
+    for g, i, np_ in ((Gate.Rx(0.1), 1, 1), (Gate.FSim(0.1, 0.2), 2, 2), (Gate.H, 0, 0),
+                      (Gate.Custom(np.eye(2)), 0, 0)):
+        with pytest.raises(Y.YaoError) as e:
+            g.generator_matrix(i)
+        assert f"generator_matrix index {i} out of range (num_params={np_})" in str(e.value)
+    with pytest.raises(ValueError):
+        Gate.Rx(0.1).generator_matrix(-1)

@@ -538,6 +538,24 @@ int yao_gate_matrix(int32_t gate, const double* params, double* out, uint32_t* d
     return YAO_OK;
 }
 
+// Gate::generator_matrix (src/gate.rs:153-193): G = (dU/dtheta_i) U^-1, a
+// constant matrix; its assert on i (:155-159) is an error with its message.
+int yao_gate_generator_matrix(int32_t gate, uint32_t i, double* out, uint32_t* dim) {
+    CHECK_NULL(out);
+    CHECK_NULL(dim);
+    clear_error();
+    const int np = gate_num_params(gate);
+    if ((int64_t)i >= np)
+        return fail(YAO_ERR_INVALID_ARGUMENT, "generator_matrix index " + std::to_string(i) +
+                                                  " out of range (num_params=" + std::to_string(np) + ")");
+    GateElem g;
+    g.type = gate;
+    std::vector<Cx> m;
+    gate_generator(g, (int)i, m, *dim);
+    memcpy(out, m.data(), sizeof(Cx) * m.size());
+    return YAO_OK;
+}
+
 int yao_noise_kraus(const yao_element* ch, double* out, uint32_t max_kraus, uint32_t* nkraus, uint32_t* dim) {
     CHECK_NULL(ch);
     CHECK_NULL(nkraus);

@@ -102,6 +102,7 @@ SIGNATURES = {
     "yao_circuit_dispatch": (C.c_int, [vp, dptr, sz]),
     "yao_circuit_dagger": (C.c_int, [vp, pp]),
     "yao_gate_matrix": (C.c_int, [i32, dptr, dptr, u32p]),
+    "yao_gate_generator_matrix": (C.c_int, [i32, u32, dptr, u32p]),
     "yao_noise_kraus": (C.c_int, [C.POINTER(yao_element), dptr, u32, u32p, u32p]),
     "yao_noise_superop": (C.c_int, [C.POINTER(yao_element), dptr, u32p]),
     "yao_reg_zero_state": (C.c_int, [vp, u32, i32, pp]),

@@ -72,6 +72,18 @@ class Gate:
         d = dim.value
         return out[: d * d].reshape(d, d)
 
+    # -- gate.rs:153-193
+    def generator_matrix(self, i: int) -> np.ndarray:
+        """G = (dU/dtheta_i) U^-1 of parameter i (constant for every
+        parametric gate); raises YaoError for i >= num_params()."""
+        if i < 0:
+            raise ValueError(f"generator_matrix index {i} is negative")
+        out = np.zeros(16, dtype=np.complex128)
+        dim = C.c_uint32()
+        A.check(A.lib().yao_gate_generator_matrix(self.kind, i, out.ctypes.data_as(A.dptr), C.byref(dim)))
+        d = dim.value
+        return out[: d * d].reshape(d, d)
+
     def num_sites(self) -> int:
         if self.kind in (A.GATE_SWAP, A.GATE_ISWAP, A.GATE_FSIM):
             return 2
