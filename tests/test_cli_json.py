@@ -1,5 +1,6 @@
 """Circuit JSON (src/json.rs), the yao-state-v1 file format
-(yao-cli/src/state_io.rs) and the CLI commands simulate / probs / expect,
+(yao-cli/src/state_io.rs) and the CLI commands simulate / probs / expect /
+measure,
 checked against the outputs yao-rs generated for its documentation examples
 (docs/src/examples/generated/results/*.json)."""
 import io
@@ -129,3 +130,55 @@ def test_cli_examples_on_gpu(golden, tmp_path):
     e = json.loads(_cli("expect", str(spath), "X(0) + 0.5*Z(1)Z(3)", "--json").stdout)
     ref = O.expect_arrayreg(st, 4, parse_operator("X(0) + 0.5*Z(1)Z(3)"))
     assert abs(e["expectation_value"]["re"] - ref.real) < 1e-12
+
+
+def test_measure_sampling_rule_and_format():
+    """sample_outcomes follows sample_from_probs / decode_outcome_bits
+    (src/measure.rs:140-156) draw by draw, and format_measurement lays out
+    counts as yao-cli does (yao-cli/src/commands/mod.rs:54-100)."""
+    from yao_rs.cli import format_measurement, sample_outcomes
+
+    def one(p, r):
+        acc = 0.0
+        for i, x in enumerate(p):
+            acc += x
+            if r < acc:
+                return i
+        return len(p) - 1
+
+    rng = np.random.default_rng(11)
+    for m in (1, 2, 3, 5):
+        p = rng.random(1 << m)
+        p[rng.random(1 << m) < 0.3] = 0.0
+        p /= p.sum()
+        draws = np.concatenate([rng.random(500), [0.0, np.nextafter(1.0, 0.0)], np.cumsum(p)[:-1]])
+        got = sample_outcomes(p, m, draws)
+        for r, o in zip(draws, got):
+            i = one(p, float(r))
+            assert o == [(i >> (m - 1 - b)) & 1 for b in range(m)]
+    human, obj = format_measurement([[1, 0], [0, 1], [1, 0]], 3, [2, 0], 4)
+    assert human.splitlines() == ["Measurement results (3 shots):", "  |01> : 1 (33.3%)", "  |10> : 2 (66.7%)"]
+    assert obj == {"num_qubits": 4, "shots": 3, "locs": [2, 0], "counts": {"01": 1, "10": 2},
+                   "outcomes": [[1, 0], [0, 1], [1, 0]]}
+
+
+@pytest.mark.gpu
+def test_cli_measure_on_gpu(tmp_path):
+    """measure over a state file: the outcomes are those the oracle's
+    marginal probabilities give for the same seeded draws."""
+    from yao_rs.cli import sample_outcomes
+
+    rng = np.random.default_rng(5)
+    n = 6
+    st = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    st /= np.linalg.norm(st)
+    spath = tmp_path / "s.state"
+    with open(spath, "wb") as f:
+        write_state(st, f)
+    for locs, arg in (([3, 0, 5], ["--locs", "3,0,5"]), (list(range(n)), [])):
+        out = json.loads(_cli("measure", str(spath), "--shots", "300", "--seed", "17", *arg, "--json").stdout)
+        draws = np.random.default_rng(17).random(300)
+        want = sample_outcomes(O.probs(st, n, locs), len(locs), draws)
+        assert out["outcomes"] == want
+        assert out["shots"] == 300 and sum(out["counts"].values()) == 300
+        assert out["locs"] == (locs if arg else None)

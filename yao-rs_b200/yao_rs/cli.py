@@ -1,9 +1,11 @@
-"""Command line front end over the GPU path (the simulate / probs / expect
-commands of yao-cli, yao-cli/src/commands/{simulate,probs,expect}.rs).
+"""Command line front end over the GPU path (the simulate / probs / expect /
+measure commands of yao-cli, yao-cli/src/commands/{simulate,probs,expect,
+measure}.rs).
 
     python -m yao_rs.cli simulate circuit.json [--input state] [--output out.state]
     python -m yao_rs.cli probs state|- [--locs 0,1] [--json]
     python -m yao_rs.cli expect state|- "Z(0)Z(1) + 0.5*X(2)" [--json]
+    python -m yao_rs.cli measure state|- [--shots 1024] [--locs 0,1] [--seed S] [--json]
     python -m yao_rs.cli run circuit.json [--probs] [--op "Z(0)"] [--json]
 
 States use the yao-state-v1 file format; `-` reads standard input.  The
@@ -99,6 +101,31 @@ def _expect_report(op_str, v, as_json):
     _emit(human, {"operator": op_str, "expectation_value": {"re": v.real, "im": v.imag}}, as_json)
 
 
+def sample_outcomes(p, nlocs, draws):
+    """One outcome per uniform draw r, by sample_from_probs and
+    decode_outcome_bits (src/measure.rs:140-156): the first index whose
+    running sum of p exceeds r (the last index if none does), as nlocs bits,
+    most significant first."""
+    cum = np.add.accumulate(np.asarray(p, dtype=np.float64))
+    idx = np.minimum(np.searchsorted(cum, np.asarray(draws, dtype=np.float64), side="right"), len(cum) - 1)
+    return [[(int(i) >> (nlocs - 1 - b)) & 1 for b in range(nlocs)] for i in idx]
+
+
+def format_measurement(outcomes, shots, locs, n):
+    """yao-cli/src/commands/mod.rs:54-100 (format_measurement): counts per
+    outcome in outcome order, the human table and the JSON object."""
+    counts = {}
+    for o in outcomes:
+        counts[tuple(o)] = counts.get(tuple(o), 0) + 1
+    ordered = sorted(counts.items())
+    human = [f"Measurement results ({shots} shots):"]
+    for o, cnt in ordered:
+        human.append(f"  |{''.join(map(str, o))}> : {cnt} ({cnt / shots * 100:.1f}%)")
+    obj = {"num_qubits": n, "shots": shots, "locs": locs,
+           "counts": {"".join(map(str, o)): cnt for o, cnt in ordered}, "outcomes": outcomes}
+    return "\n".join(human), obj
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="yao_rs.cli")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -114,6 +141,12 @@ def main(argv=None):
     e.add_argument("input")
     e.add_argument("op")
     e.add_argument("--json", action="store_true")
+    ms = sub.add_parser("measure")
+    ms.add_argument("input")
+    ms.add_argument("--shots", type=int, default=1024)
+    ms.add_argument("--locs")
+    ms.add_argument("--seed", type=int)
+    ms.add_argument("--json", action="store_true")
     r = sub.add_parser("run")
     r.add_argument("circuit")
     r.add_argument("--input")
@@ -142,6 +175,19 @@ def main(argv=None):
         st = load_state(a.input)
         n = int(st.size).bit_length() - 1
         _expect_report(a.op, expect_arrayreg(ArrayReg.from_vec(n, st), parse_operator(a.op)), a.json)
+    elif a.cmd == "measure":
+        # yao-cli/src/commands/measure.rs: `shots` draws without post-processing
+        # (the state is never collapsed), so the marginal probabilities are
+        # computed once on the GPU and every shot samples them
+        st = load_state(a.input)
+        n = int(st.size).bit_length() - 1
+        locs = [int(x) for x in a.locs.split(",")] if a.locs else None
+        mlocs = locs if locs is not None else list(range(n))
+        p = probs(ArrayReg.from_vec(n, st), mlocs)
+        rng = np.random.default_rng(a.seed)
+        outcomes = sample_outcomes(p, len(mlocs), rng.random(a.shots))
+        human, obj = format_measurement(outcomes, a.shots, locs, n)
+        _emit(human, obj, a.json)
     else:
         c = load_circuit(a.circuit)
         reg = ArrayReg.from_vec(c.nbits, load_state(a.input)) if a.input else ArrayReg.zero_state(c.nbits)
